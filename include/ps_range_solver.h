@@ -1,0 +1,168 @@
+/*
+ * ps_range_solver.h - C ABI of the B200 range solver (drop-in for the game /
+ * solve path of tjennings/poker_solver_rust `crates/range-solver`).
+ *
+ * Every entry point replaces one reference function; the comment beside it
+ * names the reference item (paths relative to crates/range-solver/src).
+ * Conventions: plain pointers and sizes, host memory unless a name says
+ * "device"; every function returns PS_OK (0) or a negative PS_ERR_* code and
+ * never aborts the caller - the reference's panics ("Game is already solved",
+ * "Game is not ready") become PS_ERR_STATE; the message of the last error on
+ * the calling thread is ps_last_error().  A game owns one CUDA stream; calls
+ * on one game must not overlap, different games may be used from different
+ * threads.  The library requires an sm_100 GPU; there is no CPU fallback.
+ */
+#ifndef PS_RANGE_SOLVER_H
+#define PS_RANGE_SOLVER_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PS_OK 0
+#define PS_ERR_INVALID (-1)     /* invalid configuration or argument */
+#define PS_ERR_STATE (-2)       /* call not allowed in the game's state */
+#define PS_ERR_CUDA (-3)        /* CUDA runtime error or no usable GPU */
+#define PS_ERR_UNSUPPORTED (-4) /* feature outside this build */
+#define PS_ERR_DEVICE (-5)      /* a kernel reported an error flag */
+
+/* action_tree.rs:130-192 TreeConfig; bet sizes are the reference's strings
+ * (bet_size.rs:82-112, e.g. "50%, 100%, a" / "2.5x" / "20c3r" / "2e"). */
+typedef struct ps_tree_config {
+  int32_t initial_state; /* BoardState: 0 flop, 1 turn, 2 river */
+  int32_t starting_pot;
+  int32_t effective_stack;
+  int32_t depth_limit; /* -1 = None */
+  double rake_rate;
+  double rake_cap;
+  double add_allin_threshold;
+  double force_allin_threshold;
+  double merging_threshold;
+  const char* bet_sizes[3][2][2]; /* [flop, turn, river][oop, ip][bet, raise]; NULL = "" */
+  const char* donk_sizes[2];      /* turn, river; NULL = None */
+  int32_t max_bets;               /* extension, not in the reference: cap on bets + raises
+                                     per street (0 = no cap, the reference behaviour) */
+  int32_t reserved;
+} ps_tree_config;
+
+/* card.rs:19-32 CardConfig; ranges as range.rs:38-39 raw data (1326 weights in
+ * card_pair_to_index order, each in [0, 1]); 255 = card not dealt. */
+typedef struct ps_card_config {
+  const float* range[2];
+  uint8_t flop[3];
+  uint8_t turn;
+  uint8_t river;
+  uint8_t reserved[3];
+} ps_card_config;
+
+typedef struct ps_game ps_game;
+
+/* ---- game lifecycle (game/interpreter.rs) ---- */
+/* ActionTree::new + PostFlopGame::with_config (action_tree.rs:326, interpreter.rs:128) */
+int ps_game_new(const ps_card_config* cards, const ps_tree_config* tree, ps_game** out);
+void ps_game_free(ps_game* g);
+/* PostFlopGame::memory_usage (interpreter.rs:188): bytes of f32 state on the device */
+int ps_game_memory_usage(ps_game* g, uint64_t* bytes);
+/* PostFlopGame::allocate_memory (interpreter.rs:212); compression -> PS_ERR_UNSUPPORTED */
+int ps_game_allocate_memory(ps_game* g, int enable_compression);
+
+/* ---- solver (solver.rs, utility.rs) ---- */
+/* solve (solver.rs:108): DCFR until max_iter or exploitability <= target (chips) */
+int ps_solve(ps_game* g, uint32_t max_iter, float target, int print_progress, float* out_exploitability);
+/* number of iterations the last ps_solve ran */
+int ps_last_iterations(ps_game* g, uint32_t* out);
+/* solve_step (solver.rs:184) */
+int ps_solve_step(ps_game* g, uint32_t current_iteration);
+/* compute_exploitability (utility.rs:380), chips */
+int ps_compute_exploitability(ps_game* g, float* out);
+/* finalize (utility.rs:348) */
+int ps_finalize(ps_game* g);
+/* root_cfvalues_with_reach (utility.rs:422); opp_reach NULL = initial weights (root_cfvalues, :407) */
+int ps_root_cfvalues_with_reach(ps_game* g, int player, const float* opp_reach, float* out);
+
+/* ---- game data (game/mod.rs, interpreter.rs) ---- */
+int ps_num_private_hands(ps_game* g, int player);
+int ps_private_cards(ps_game* g, int player, uint8_t* out_pairs);  /* private_cards(): [H][2] */
+int ps_initial_weights(ps_game* g, int player, float* out);
+double ps_num_combinations(ps_game* g);
+int64_t ps_num_nodes(ps_game* g);
+/* node fields: player, amount, turn, river, num_children, children_offset, prev kind, prev amount */
+int ps_node_info(ps_game* g, int64_t node, int32_t out[8]);
+int ps_child_indices(ps_game* g, int64_t node, int64_t* out, int cap); /* query.rs:475 */
+int ps_strategy_at_index(ps_game* g, int64_t node, float* out);     /* query.rs:386 */
+/* raw per-node storage: 1 cumulative strategy, 2 regrets (cfvalues after finalize),
+ * 3 IP cfvalues, 4 chance cfvalues; returns the element count */
+int64_t ps_node_storage(ps_game* g, int64_t node, int which, float* out);
+int ps_same_hand_index(ps_game* g, int player, uint16_t* out);      /* game/mod.rs:288 */
+/* hand strength order for board (turn, river) as computed on the device:
+ * ascending (strength, index) items incl. the (0,0) / (65535,65535) sentinels
+ * (card.rs:163-226); returns the item count */
+int ps_hand_strength(ps_game* g, int turn, int river, int player, uint16_t* strength, uint16_t* index);
+/* valid_indices for a board (card.rs:81-156); returns the count */
+int ps_valid_indices(ps_game* g, int turn, int river, int player, uint16_t* out);
+
+/* ---- depth boundary (interpreter.rs:307-534) ---- */
+int64_t ps_num_boundary_nodes(ps_game* g);
+int ps_boundary_node_indices(ps_game* g, int64_t* out);
+int ps_set_boundary_cfvs(ps_game* g, int64_t ordinal, int player, const float* cfvs, int64_t n);
+
+/* ---- navigation and queries (game/query.rs) ---- */
+int ps_back_to_root(ps_game* g);
+int ps_play(ps_game* g, int64_t action); /* action = -1: first possible card */
+int ps_available_actions(ps_game* g, int32_t* kinds, int32_t* amounts, int cap);
+int ps_is_terminal_node(ps_game* g);
+int ps_is_chance_node(ps_game* g);
+int ps_current_player(ps_game* g);
+int64_t ps_current_node_index(ps_game* g);
+uint64_t ps_possible_cards(ps_game* g);
+int ps_strategy(ps_game* g, float* out); /* returns the element count */
+int ps_cache_normalized_weights(ps_game* g);
+int ps_weights(ps_game* g, int player, int normalized, float* out);
+int ps_expected_values(ps_game* g, int player, int detail, float* out); /* returns count */
+int ps_total_bet_amount(ps_game* g, int32_t out[2]);
+
+/* ---- checkpoint (storage_buffers / set_storage_buffers, interpreter.rs:265-300) ---- */
+int ps_state_export(ps_game* g, void* buf, uint64_t cap, uint64_t* needed);
+int ps_state_import(ps_game* g, const void* buf, uint64_t size);
+
+/* ---- batched solve (replaces per-spot GpuBatchSolver launches,
+ *      crates/gpu-range-solver/src/batch.rs:79-610) ---- */
+typedef struct ps_batch ps_batch;
+typedef struct ps_batch_opts {
+  int32_t block_threads;  /* 0 = autotuned */
+  int32_t ctas_per_sm;    /* 0 = autotuned */
+  int32_t sort_by_cost;   /* 1 = hand out the largest spots first */
+  int32_t reserved;
+} ps_batch_opts;
+int ps_batch_new(const ps_card_config* cards, const ps_tree_config* trees, int32_t n,
+                 const ps_batch_opts* opts, ps_batch** out);
+void ps_batch_free(ps_batch* b);
+/* one persistent launch: every spot runs solve() to max_iter or target[i] chips */
+int ps_batch_solve(ps_batch* b, uint32_t max_iter, const float* target_chips);
+int ps_batch_results(ps_batch* b, float* exploitability, int32_t* iterations);
+int ps_batch_root_strategy(ps_batch* b, int32_t spot, float* out); /* returns count */
+/* device time in ms of the last ps_batch_solve (setup excluded / included) */
+int ps_batch_last_timing(ps_batch* b, float* solve_ms, float* setup_ms);
+/* algorithmic bytes of one DCFR iteration of spot i: 20 * sum_edges H_actor */
+double ps_batch_iteration_bytes(ps_batch* b, int32_t spot);
+int ps_batch_config(ps_batch* b, int32_t* block_threads, int32_t* grid, int32_t* ctas_per_sm);
+/* bytes copied host->device by ps_batch_new and device->host by ps_batch_results */
+int ps_batch_io_bytes(ps_batch* b, uint64_t* h2d, uint64_t* d2h);
+
+/* ---- misc ---- */
+/* BetSizeOptions::try_from one list (bet_size.rs:82-112): per entry the kind
+ * (0 PotRelative, 1 PrevBetRelative, 2 Additive, 3 Geometric, 4 AllIn), its
+ * float (ratio / max ratio), int (adder / streets) and raise cap; returns the
+ * count */
+int ps_parse_bet_sizes(const char* sizes, int is_raise, int32_t* kinds, double* values, int32_t* ints,
+                       int32_t* caps, int cap);
+const char* ps_last_error(void);
+int ps_hand_table(int32_t* out, int cap); /* hand_table.rs values as built here */
+int ps_discount_params(uint32_t t, float out[3]); /* solver.rs:26-44 */
+
+#ifdef __cplusplus
+}
+#endif
+#endif

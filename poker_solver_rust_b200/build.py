@@ -1,0 +1,56 @@
+"""Builds the in-tree CUDA library ``_lib/libps_b200.so`` for sm_100a.
+
+nvcc compiles the kernels and the C++ host side; the result is a plain C-ABI
+shared library (include/ps_range_solver.h) loaded by ``poker_solver_rust_b200``
+through ctypes.  Rebuilds only when a source is newer than the library.
+"""
+
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT_DIR = os.path.join(HERE, "_lib")
+LIB = os.path.join(OUT_DIR, "libps_b200.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+SOURCES = ["ps_kernels.cu", "ps_host.cpp", "ps_capi.cpp"]
+HEADERS = ["ps_device.hpp", "ps_handeval.hpp", "ps_host.hpp", "ps_launch.hpp"]
+
+
+def _stale() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
+    deps.append(os.path.join(HERE, "..", "include", "ps_range_solver.h"))
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and not _stale():
+        return LIB
+    os.makedirs(OUT_DIR, exist_ok=True)
+    objs = []
+    for src in SOURCES:
+        obj = os.path.join(OUT_DIR, src.replace(".", "_") + ".o")
+        cmd = [NVCC, *ARCH, "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
+               "-Xcompiler", "-ffp-contract=off", "-c", os.path.join(CSRC, src), "-o", obj]
+        if src.endswith(".cu"):
+            cmd[1:1] = ["-Xptxas", "-v"] if verbose else []
+        else:
+            cmd += ["-x", "cu"] if False else []
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        objs.append(obj)
+    cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-lpthread"]
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

@@ -1,0 +1,1277 @@
+// extern "C" boundary of the B200 range solver (include/ps_range_solver.h).
+//
+// A ps_batch owns N games packed into one device pool; a ps_game is a batch
+// of one plus the navigation state of game/query.rs.  Host code here builds
+// trees (ps_host.cpp), uploads them, launches the kernels of ps_kernels.cu and
+// implements the query logic over the downloaded strategy / cfvalue arrays.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/ps_range_solver.h"
+#include "ps_handeval.hpp"
+#include "ps_host.hpp"
+#include "ps_launch.hpp"
+
+using namespace ps;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CU(x)                                                                           \
+  do {                                                                                  \
+    cudaError_t e_ = (x);                                                               \
+    if (e_ != cudaSuccess) return fail(PS_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// ---- per-device constants: hand table ----
+struct DeviceConsts {
+  int device = -1;
+  int32_t* table = nullptr;
+  int nsm = 0;
+};
+std::mutex g_dev_mu;
+DeviceConsts g_dev[16];
+
+int device_consts(DeviceConsts** out) {
+  int dev = 0;
+  CU(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 16) return fail(PS_ERR_CUDA, "device index out of range");
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  DeviceConsts& d = g_dev[dev];
+  if (!d.table) {
+    cudaDeviceProp prop;
+    CU(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major != 10) return fail(PS_ERR_CUDA, "this build targets sm_100a (B200); found sm_" +
+                                                       std::to_string(prop.major) + std::to_string(prop.minor));
+    std::vector<int32_t> t(kHandTableSize + 64);
+    int n = build_hand_table(t.data(), (int)t.size());
+    if (n != kHandTableSize) return fail(PS_ERR_INVALID, "hand table size mismatch");
+    CU(cudaMalloc(&d.table, sizeof(int32_t) * kHandTableSize));
+    CU(cudaMemcpy(d.table, t.data(), sizeof(int32_t) * kHandTableSize, cudaMemcpyHostToDevice));
+    d.nsm = prop.multiProcessorCount;
+    d.device = dev;
+  }
+  *out = &d;
+  return PS_OK;
+}
+
+bool parse_tree_config(const ps_tree_config* c, TreeCfg& t, std::string& err) {
+  t.initial_state = c->initial_state;
+  if (t.initial_state < 0 || t.initial_state > 2) {
+    err = "initial_state must be 0 (flop), 1 (turn) or 2 (river)";
+    return false;
+  }
+  t.starting_pot = c->starting_pot;
+  t.effective_stack = c->effective_stack;
+  t.rake_rate = c->rake_rate;
+  t.rake_cap = c->rake_cap;
+  t.add_allin_threshold = c->add_allin_threshold;
+  t.force_allin_threshold = c->force_allin_threshold;
+  t.merging_threshold = c->merging_threshold;
+  t.depth_limit = c->depth_limit;
+  t.max_bets = c->max_bets;
+  for (int s = 0; s < 3; ++s)
+    for (int p = 0; p < 2; ++p) {
+      const char* b = c->bet_sizes[s][p][0];
+      const char* r = c->bet_sizes[s][p][1];
+      if (!parse_menu(b ? b : "", false, t.menu[s][p].bet, err)) return false;
+      if (!parse_menu(r ? r : "", true, t.menu[s][p].raise, err)) return false;
+    }
+  for (int k = 0; k < 2; ++k) {
+    t.has_donk[k] = c->donk_sizes[k] != nullptr;
+    if (t.has_donk[k] && !parse_menu(c->donk_sizes[k], false, t.donk[k], err)) return false;
+  }
+  return true;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct Layout {  // byte offsets inside the pool
+  size_t cards[2], w[2], same[2], ops[2], steps[2], nodes, board_cards, iso_perm[2], iso_off, iso_ent;  // static
+  size_t gidx[2], coff[2], thr[2], nvalid[2];                                                         // setup
+  size_t R, S, ipcfv, chcfv, bcfv;                                                                    // state
+};
+
+// ---------------------------------------------------------------------------
+// Batch: N games in one device pool
+// ---------------------------------------------------------------------------
+struct Batch {
+  std::vector<std::unique_ptr<Game>> games;
+  std::vector<Layout> lay;
+  DeviceConsts* dc = nullptr;
+  cudaStream_t stream = nullptr;
+  char* pool = nullptr;
+  size_t static_bytes = 0, setup_bytes = 0, state_bytes = 0;
+  char* h_static = nullptr;  // pinned staging of the static region
+  SpotDev* d_spots = nullptr;
+  std::vector<SpotDev> h_spots;
+  int2* d_work = nullptr;
+  int nwork = 0;
+  float* d_scratch = nullptr;
+  size_t scratch_floats = 0;
+  int scratch_ctas = 0;
+  Discount* d_disc = nullptr;
+  int disc_cap = 0;
+  float* d_target = nullptr;
+  float* d_expl = nullptr;
+  int* d_iters = nullptr;
+  int* d_counter = nullptr;
+  int* d_err = nullptr;
+  int* d_order = nullptr;
+  int block = 256, grid = 1, ctas_per_sm = 0;
+  int max_vstride = 32;
+  size_t smem = 0;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  float last_solve_ms = 0, last_setup_ms = 0;
+  std::vector<float> h_expl;
+  std::vector<int> h_iters;
+
+  ~Batch() {
+    if (stream) cudaStreamSynchronize(stream);
+    cudaFree(pool);
+    cudaFreeHost(h_static);
+    cudaFree(d_spots);
+    cudaFree(d_work);
+    cudaFree(d_scratch);
+    cudaFree(d_disc);
+    cudaFree(d_target);
+    cudaFree(d_expl);
+    cudaFree(d_iters);
+    cudaFree(d_counter);
+    cudaFree(d_err);
+    cudaFree(d_order);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  int build(const ps_batch_opts* opts) {
+    int rc = device_consts(&dc);
+    if (rc) return rc;
+    CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    for (auto& e : ev) CU(cudaEventCreate(&e));
+    const int n = (int)games.size();
+    lay.resize(n);
+    // ---- layout ----
+    size_t so = 0, su = 0, st = 0;
+    auto take = [](size_t& off, size_t bytes) {
+      size_t r = off;
+      off += align256(bytes);
+      return r;
+    };
+    for (int i = 0; i < n; ++i) {
+      Game& g = *games[i];
+      Layout& L = lay[i];
+      const size_t nb = g.boards.size();
+      for (int p = 0; p < 2; ++p) {
+        L.cards[p] = take(so, (size_t)g.H[p] * 2 + 16);
+        L.w[p] = take(so, (size_t)g.hs[p] * 4);
+        L.same[p] = take(so, (size_t)g.hs[p] * 2);
+        L.ops[p] = take(so, g.prog[p].ops.size() * sizeof(Op));
+        L.steps[p] = take(so, g.prog[p].steps.size() * sizeof(Step));
+        L.iso_perm[p] = take(so, g.iso_perm[p].size() * (size_t)g.hs[p] * 2 + 16);
+        L.gidx[p] = take(su, nb * 3 * g.hs[p] * 2);
+        L.coff[p] = take(su, nb * 56 * 2);
+        L.thr[p] = take(su, nb * g.hs[p] * kThrWords * 2);
+        L.nvalid[p] = take(su, nb * 4);
+      }
+      L.nodes = take(so, g.arena.size() * sizeof(NodeDev));
+      L.board_cards = take(so, nb * 5);
+      L.iso_off = take(so, g.iso_list_off.size() * 4 + 16);
+      L.iso_ent = take(so, g.iso_list.size() * 8 + 16);
+      L.R = take(st, g.num_storage * 4 + 16);
+      L.S = take(st, g.num_storage * 4 + 16);
+      L.ipcfv = take(st, g.num_storage_ip * 4 + 16);
+      L.chcfv = take(st, g.num_storage_chance * 4 + 16);
+      L.bcfv = take(st, (size_t)g.num_boundary * 2 * g.vstride * 4 + 16);
+      max_vstride = std::max(max_vstride, g.vstride);
+    }
+    static_bytes = so;
+    setup_bytes = su;
+    state_bytes = st;
+    CU(cudaMalloc(&pool, static_bytes + setup_bytes + state_bytes));
+    CU(cudaMallocHost(&h_static, std::max<size_t>(static_bytes, 16)));
+    // ---- fill static ----
+    h_spots.resize(n);
+    std::vector<int2> work;
+    char* dS = pool;
+    char* dU = pool + static_bytes;
+    char* dT = pool + static_bytes + setup_bytes;
+    for (int i = 0; i < n; ++i) {
+      Game& g = *games[i];
+      Layout& L = lay[i];
+      SpotDev& s = h_spots[i];
+      std::memset(&s, 0, sizeof(s));
+      for (int p = 0; p < 2; ++p) {
+        uint8_t* cp = (uint8_t*)(h_static + L.cards[p]);
+        for (int h = 0; h < g.H[p]; ++h) {
+          cp[2 * h] = g.cards[p][h][0];
+          cp[2 * h + 1] = g.cards[p][h][1];
+        }
+        float* wp = (float*)(h_static + L.w[p]);
+        uint16_t* sp = (uint16_t*)(h_static + L.same[p]);
+        for (int h = 0; h < g.hs[p]; ++h) {
+          wp[h] = h < g.H[p] ? g.w[p][h] : 0.0f;
+          sp[h] = h < g.H[p] ? g.same[p][h] : (uint16_t)0xFFFF;
+        }
+        std::memcpy(h_static + L.ops[p], g.prog[p].ops.data(), g.prog[p].ops.size() * sizeof(Op));
+        std::memcpy(h_static + L.steps[p], g.prog[p].steps.data(), g.prog[p].steps.size() * sizeof(Step));
+        uint16_t* ip = (uint16_t*)(h_static + L.iso_perm[p]);
+        for (size_t k = 0; k < g.iso_perm[p].size(); ++k)
+          std::memcpy(ip + k * g.hs[p], g.iso_perm[p][k].data(), (size_t)g.hs[p] * 2);
+        s.H[p] = g.H[p];
+        s.hs[p] = g.hs[p];
+        s.nsteps[p] = (int)g.prog[p].steps.size();
+        s.root_slot[p] = g.prog[p].root_slot;
+        s.cards[p] = (const uint8_t*)(dS + L.cards[p]);
+        s.w[p] = (const float*)(dS + L.w[p]);
+        s.same[p] = (const uint16_t*)(dS + L.same[p]);
+        s.ops[p] = (const Op*)(dS + L.ops[p]);
+        s.steps[p] = (const Step*)(dS + L.steps[p]);
+        s.iso_perm[p] = (const uint16_t*)(dS + L.iso_perm[p]);
+        s.gidx[p] = (uint16_t*)(dU + L.gidx[p]);
+        s.coff[p] = (uint16_t*)(dU + L.coff[p]);
+        s.thr[p] = (uint16_t*)(dU + L.thr[p]);
+        s.nvalid[p] = (int32_t*)(dU + L.nvalid[p]);
+      }
+      NodeDev* nd = (NodeDev*)(h_static + L.nodes);
+      for (size_t k = 0; k < g.arena.size(); ++k) {
+        const ArenaNode& a = g.arena[k];
+        NodeDev& d = nd[k];
+        std::memset(&d, 0, sizeof(d));
+        d.amount = a.amount;
+        d.rs_off = a.rs_off;
+        d.ip_off = a.ip_off;
+        d.ch_off = a.ch_off;
+        d.chance_factor = g.chance_factor(a);
+        int sp = a.player & PL_MASK;
+        d.ch_player = (a.chance() && (sp == 0 || sp == 1)) ? (sp ^ 1) : -1;
+        d.boundary = g.bnd_ordinal[k];
+        // evaluation.rs:64-68, :430 in f64, rounded once to f32
+        double pot = (double)(g.cfg.starting_pot + 2 * a.amount);
+        double half = 0.5 * pot;
+        double rake = std::min(pot * g.cfg.rake_rate, g.cfg.rake_cap);
+        d.amount_win = (float)((half - rake) / g.num_combinations);
+        d.amount_lose = (float)(-half / g.num_combinations);
+        d.amount_tie = (float)(-0.5 * rake / g.num_combinations);
+        d.payoff_scale = (float)(half / g.num_combinations);
+      }
+      uint8_t* bc = (uint8_t*)(h_static + L.board_cards);
+      for (size_t b = 0; b < g.boards.size(); ++b) {
+        std::memcpy(bc + 5 * b, g.boards[b].data(), 5);
+        work.push_back(make_int2(i, (int)b));
+      }
+      std::memcpy(h_static + L.iso_off, g.iso_list_off.data(), g.iso_list_off.size() * 4);
+      std::memcpy(h_static + L.iso_ent, g.iso_list.data(), g.iso_list.size() * 8);
+      s.vstride = g.vstride;
+      s.num_slots = g.num_slots;
+      s.num_boards = (int)g.boards.size();
+      s.starting_pot = g.cfg.starting_pot;
+      s.raked = (g.cfg.rake_rate > 0.0 && g.cfg.rake_cap > 0.0) ? 1 : 0;
+      s.num_boundary = g.num_boundary;
+      s.num_combinations = g.num_combinations;
+      s.rake_rate = g.cfg.rake_rate;
+      s.rake_cap = g.cfg.rake_cap;
+      s.nodes = (const NodeDev*)(dS + L.nodes);
+      s.board_cards = (const uint8_t*)(dS + L.board_cards);
+      s.iso_off = (const int32_t*)(dS + L.iso_off);
+      s.iso_ent = (const int32_t*)(dS + L.iso_ent);
+      s.bcfv = (const float*)(dT + L.bcfv);
+      s.R = (float*)(dT + L.R);
+      s.S = (float*)(dT + L.S);
+      s.ipcfv = (float*)(dT + L.ipcfv);
+      s.chcfv = (float*)(dT + L.chcfv);
+    }
+    nwork = (int)work.size();
+    CU(cudaMalloc(&d_spots, sizeof(SpotDev) * n));
+    CU(cudaMalloc(&d_work, sizeof(int2) * std::max(1, nwork)));
+    CU(cudaMalloc(&d_target, sizeof(float) * n));
+    CU(cudaMalloc(&d_expl, sizeof(float) * n));
+    CU(cudaMalloc(&d_iters, sizeof(int) * n));
+    CU(cudaMalloc(&d_counter, sizeof(int)));
+    CU(cudaMalloc(&d_err, sizeof(int)));
+    CU(cudaMalloc(&d_order, sizeof(int) * n));
+    // launch configuration
+    block = opts && opts->block_threads > 0 ? opts->block_threads : 256;
+    smem = solve_smem(max_vstride);
+    int occ = solve_occupancy(block, smem);
+    ctas_per_sm = opts && opts->ctas_per_sm > 0 ? std::min(opts->ctas_per_sm, occ) : occ;
+    grid = std::max(1, std::min(n, dc->nsm * ctas_per_sm));
+    for (auto& gp : games) scratch_floats = std::max(scratch_floats, (size_t)gp->num_slots * gp->vstride);
+    scratch_floats = (scratch_floats + 63) & ~(size_t)63;
+    scratch_ctas = grid;
+    CU(cudaMalloc(&d_scratch, sizeof(float) * scratch_floats * scratch_ctas));
+    // order: largest estimated cost first (longest-processing-time first)
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    if (!opts || opts->sort_by_cost) {
+      std::vector<double> cost(n);
+      for (int i = 0; i < n; ++i) cost[i] = (double)games[i]->num_storage + 4.0 * games[i]->arena.size() * games[i]->vstride;
+      std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    }
+    // ---- upload ----
+    CU(cudaMemcpyAsync(pool, h_static, static_bytes, cudaMemcpyHostToDevice, stream));
+    CU(cudaMemcpyAsync(d_spots, h_spots.data(), sizeof(SpotDev) * n, cudaMemcpyHostToDevice, stream));
+    CU(cudaMemcpyAsync(d_work, work.data(), sizeof(int2) * nwork, cudaMemcpyHostToDevice, stream));
+    CU(cudaMemcpyAsync(d_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
+    CU(cudaStreamSynchronize(stream));
+    return PS_OK;
+  }
+
+  // Zeroes the solver state and rebuilds the per-board tables on the device.
+  int enqueue_setup() {
+    CU(cudaMemsetAsync(pool + static_bytes + setup_bytes, 0, state_bytes, stream));
+    CU(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
+    CU(launch_setup(d_spots, d_work, nwork, dc->table, d_err, std::max(1, std::min(nwork, dc->nsm * 4)), stream));
+    return PS_OK;
+  }
+
+  int run_setup() {
+    int rc = enqueue_setup();
+    if (rc) return rc;
+    CU(cudaStreamSynchronize(stream));
+    return check_err();
+  }
+
+  int check_err() {
+    int e = 0;
+    CU(cudaMemcpyAsync(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
+    if (e) return fail(PS_ERR_DEVICE, "kernel error flag " + std::to_string(e));
+    return PS_OK;
+  }
+
+  int ensure_disc(uint32_t upto) {
+    if ((int)upto <= disc_cap) return PS_OK;
+    int cap = std::max<int>(upto, std::max(1024, 2 * disc_cap));
+    std::vector<Discount> h(cap);
+    for (int t = 0; t < cap; ++t) h[t] = discount_params((uint32_t)t);
+    cudaFree(d_disc);
+    d_disc = nullptr;
+    CU(cudaMalloc(&d_disc, sizeof(Discount) * cap));
+    CU(cudaMemcpy(d_disc, h.data(), sizeof(Discount) * cap, cudaMemcpyHostToDevice));
+    disc_cap = cap;
+    return PS_OK;
+  }
+
+  // fresh = true: a complete job (state reset + board setup + solve), timed
+  // as setup_ms + solve_ms; fresh = false continues from the current state.
+  int solve(uint32_t max_iter, const float* target, bool fresh) {
+    const int n = (int)games.size();
+    int rc = ensure_disc(max_iter + 1);
+    if (rc) return rc;
+    CU(cudaMemcpyAsync(d_target, target, sizeof(float) * n, cudaMemcpyHostToDevice, stream));
+    CU(cudaMemsetAsync(d_counter, 0, sizeof(int), stream));
+    CU(cudaEventRecord(ev[1], stream));
+    if (fresh && (rc = enqueue_setup())) return rc;
+    if (!fresh) CU(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
+    CU(cudaEventRecord(ev[2], stream));
+    CU(launch_solve(d_spots, n, d_order, d_counter, d_disc, (int)max_iter, d_target, d_scratch, scratch_floats,
+                    d_expl, d_iters, d_err, grid, block, smem, stream));
+    CU(cudaEventRecord(ev[3], stream));
+    h_expl.resize(n);
+    h_iters.resize(n);
+    CU(cudaMemcpyAsync(h_expl.data(), d_expl, sizeof(float) * n, cudaMemcpyDeviceToHost, stream));
+    CU(cudaMemcpyAsync(h_iters.data(), d_iters, sizeof(int) * n, cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
+    CU(cudaEventElapsedTime(&last_solve_ms, ev[2], ev[3]));
+    CU(cudaEventElapsedTime(&last_setup_ms, ev[1], ev[2]));
+    return check_err();
+  }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// ps_game: a batch of one plus query state
+// ---------------------------------------------------------------------------
+enum class GState { TreeBuilt = 2, MemoryAllocated = 3, Solved = 4 };
+
+struct ps_game {
+  std::unique_ptr<Batch> b;
+  Game* g = nullptr;
+  GState state = GState::TreeBuilt;
+  uint32_t last_iters = 0;
+  bool host_dirty = true;
+  std::vector<float> hS, hR, hIP, hCH;
+  // navigation (query.rs)
+  std::vector<size_t> action_history, node_history;
+  bool normalized_cached = false;
+  uint8_t turn = NOT_DEALT, river = NOT_DEALT;
+  int turn_swap = -1, river_swap[2] = {-1, -1}, turn_swapped[2] = {-1, -1};
+  int32_t total_bet[2] = {0, 0};
+  std::vector<float> weights[2], normalized[2], cfv_cache[2];
+  std::vector<std::vector<float>> bcfv_host;  // [ordinal*2+player]
+};
+
+namespace {
+int sync_host(ps_game* G) {
+  if (!G->host_dirty) return PS_OK;
+  Game& g = *G->g;
+  const SpotDev& s = G->b->h_spots[0];
+  G->hS.resize(g.num_storage);
+  G->hR.resize(g.num_storage);
+  G->hIP.resize(g.num_storage_ip);
+  G->hCH.resize(g.num_storage_chance);
+  CU(cudaMemcpy(G->hS.data(), s.S, 4 * g.num_storage, cudaMemcpyDeviceToHost));
+  CU(cudaMemcpy(G->hR.data(), s.R, 4 * g.num_storage, cudaMemcpyDeviceToHost));
+  if (g.num_storage_ip) CU(cudaMemcpy(G->hIP.data(), s.ipcfv, 4 * g.num_storage_ip, cudaMemcpyDeviceToHost));
+  if (g.num_storage_chance) CU(cudaMemcpy(G->hCH.data(), s.chcfv, 4 * g.num_storage_chance, cudaMemcpyDeviceToHost));
+  G->host_dirty = false;
+  return PS_OK;
+}
+
+int need_ready(ps_game* G) {
+  if (!G) return fail(PS_ERR_INVALID, "null game");
+  if (G->state == GState::Solved) return fail(PS_ERR_STATE, "Game is already solved");
+  if (G->state != GState::MemoryAllocated) return fail(PS_ERR_STATE, "Game is not ready");
+  return PS_OK;
+}
+
+int need_boundaries(ps_game* G) {
+  for (int k = 0; k < G->g->num_boundary * 2; ++k)
+    if (G->bcfv_host[k].empty())
+      return fail(PS_ERR_STATE, "boundary cfvs empty at ordinal " + std::to_string(k / 2) + ", player " +
+                                    std::to_string(k % 2) + " (set_boundary_cfvs not called)");
+  return PS_OK;
+}
+
+float expl_run(ps_game* G, int* rc) {
+  Batch& B = *G->b;
+  float e = 0;
+  cudaError_t ce = cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream);
+  if (ce == cudaSuccess)
+    ce = launch_exploitability(B.d_spots, 1, B.d_scratch, B.scratch_floats, B.d_expl, B.d_err, 1, B.block, B.smem,
+                               B.stream);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(&e, B.d_expl, 4, cudaMemcpyDeviceToHost, B.stream);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(B.stream);
+  if (ce != cudaSuccess) {
+    *rc = fail(PS_ERR_CUDA, std::string("exploitability: ") + cudaGetErrorString(ce));
+    return 0;
+  }
+  *rc = B.check_err();
+  return e;
+}
+
+void assign_zero_weights(ps_game* G) {  // query.rs:886-920
+  Game& g = *G->g;
+  uint64_t board = 0;
+  if (G->turn != NOT_DEALT) board |= 1ull << G->turn;
+  if (G->river != NOT_DEALT) board |= 1ull << G->river;
+  for (int p = 0; p < 2; ++p) {
+    uint64_t dead = (1ull << 52) - 1;
+    for (int i = 0; i < g.H[p ^ 1]; ++i) {
+      uint64_t m = (1ull << g.cards[p ^ 1][i][0]) | (1ull << g.cards[p ^ 1][i][1]);
+      if ((m & board) == 0) dead &= m;
+      if (!dead) break;
+    }
+    dead |= board;
+    for (int i = 0; i < g.H[p]; ++i) {
+      uint64_t m = (1ull << g.cards[p][i][0]) | (1ull << g.cards[p][i][1]);
+      if (m & dead) G->weights[p][i] = 0.f;
+    }
+  }
+}
+
+const ArenaNode& cur(ps_game* G) { return G->g->arena[G->node_history.empty() ? 0 : G->node_history.back()]; }
+size_t cur_index(ps_game* G) { return G->node_history.empty() ? 0 : G->node_history.back(); }
+
+bool is_terminal(ps_game* G) {
+  const ArenaNode& n = cur(G);
+  return n.terminal() || n.amount == G->g->cfg.effective_stack;
+}
+bool is_chance(ps_game* G) { return cur(G).chance() && !is_terminal(G); }
+
+void apply_swap(ps_game* G, float* v, int p, bool reverse) {  // query.rs:863-883
+  Game& g = *G->g;
+  int ids[2] = {G->turn_swap >= 0 ? g.iso_perm_turn[G->turn_swap] : -1,
+                G->river_swap[0] >= 0 ? g.iso_perm_river[G->river_swap[0]][G->river_swap[1]] : -1};
+  if (reverse) std::swap(ids[0], ids[1]);
+  for (int id : ids) {
+    if (id < 0) continue;
+    const auto& perm = g.iso_perm[p][id];
+    for (int h = 0; h < g.H[p]; ++h)
+      if ((int)perm[h] > h) std::swap(v[h], v[perm[h]]);
+  }
+}
+
+std::vector<float> normalized_strategy(ps_game* G, const ArenaNode& n) {  // utility.rs:227-250
+  Game& g = *G->g;
+  int p = n.player, H = g.H[p], hs = g.hs[p], na = n.nch;
+  std::vector<float> out((size_t)na * H);
+  const float* S = G->hS.data() + n.rs_off;
+  float def = 1.0f / (float)na;
+  for (int h = 0; h < H; ++h) {
+    float d = S[h];
+    for (int a = 1; a < na; ++a) d += S[a * hs + h];
+    for (int a = 0; a < na; ++a) out[(size_t)a * H + h] = d == 0.0f ? def : S[a * hs + h] / d;
+  }
+  return out;
+}
+}  // namespace
+
+extern "C" {
+
+const char* ps_last_error(void) { return g_err.c_str(); }
+
+int ps_hand_table(int32_t* out, int cap) { return build_hand_table(out, cap); }
+
+int ps_parse_bet_sizes(const char* sizes, int is_raise, int32_t* kinds, double* values, int32_t* ints,
+                       int32_t* caps, int cap) {
+  std::vector<BetSize> v;
+  std::string err;
+  if (!parse_menu(sizes ? sizes : "", is_raise != 0, v, err)) return fail(PS_ERR_INVALID, err);
+  for (size_t k = 0; k < v.size() && (int)k < cap; ++k) {
+    kinds[k] = (int32_t)v[k].kind;
+    values[k] = v[k].ratio;
+    ints[k] = v[k].n;
+    caps[k] = v[k].cap;
+  }
+  return (int)v.size();
+}
+
+int ps_discount_params(uint32_t t, float out[3]) {
+  Discount d = discount_params(t);
+  out[0] = d.alpha;
+  out[1] = d.beta;
+  out[2] = d.gamma;
+  return PS_OK;
+}
+
+int ps_game_new(const ps_card_config* cc, const ps_tree_config* tc, ps_game** out) {
+  if (!cc || !tc || !out || !cc->range[0] || !cc->range[1]) return fail(PS_ERR_INVALID, "null argument");
+  *out = nullptr;
+  TreeCfg t;
+  std::string err;
+  if (!parse_tree_config(tc, t, err)) return fail(PS_ERR_INVALID, err);
+  auto g = std::make_unique<Game>();
+  uint8_t board[5] = {cc->flop[0], cc->flop[1], cc->flop[2], cc->turn, cc->river};
+  if (!g->init(cc->range[0], cc->range[1], board, t, err)) return fail(PS_ERR_INVALID, err);
+  auto* G = new ps_game();
+  G->b = std::make_unique<Batch>();
+  G->g = g.get();
+  G->b->games.push_back(std::move(g));
+  G->bcfv_host.assign((size_t)G->g->num_boundary * 2, {});
+  for (int p = 0; p < 2; ++p) {
+    G->weights[p].assign(G->g->H[p], 0.f);
+    G->normalized[p].assign(G->g->H[p], 0.f);
+    G->cfv_cache[p].assign(G->g->H[p], 0.f);
+  }
+  *out = G;
+  return PS_OK;
+}
+
+void ps_game_free(ps_game* G) { delete G; }
+
+int ps_game_memory_usage(ps_game* G, uint64_t* bytes) {
+  if (!G || !bytes) return fail(PS_ERR_INVALID, "null argument");
+  Game& g = *G->g;
+  *bytes = 4 * (2 * g.num_storage + g.num_storage_ip + g.num_storage_chance);
+  return PS_OK;
+}
+
+int ps_game_allocate_memory(ps_game* G, int enable_compression) {
+  if (!G) return fail(PS_ERR_INVALID, "null game");
+  if (enable_compression) return fail(PS_ERR_UNSUPPORTED, "compressed (16-bit) storage is not supported: state is FP32");
+  if (G->state != GState::TreeBuilt) return PS_OK;
+  int rc = G->b->build(nullptr);
+  if (!rc) rc = G->b->run_setup();
+  if (rc) return rc;
+  G->state = GState::MemoryAllocated;
+  ps_back_to_root(G);
+  return PS_OK;
+}
+
+int ps_solve(ps_game* G, uint32_t max_iter, float target, int print, float* out) {
+  int rc = need_ready(G);
+  if (rc) return rc;
+  if ((rc = need_boundaries(G))) return rc;
+  rc = G->b->solve(max_iter, &target, false);
+  if (rc) return rc;
+  float e = G->b->h_expl[0];
+  G->last_iters = (uint32_t)G->b->h_iters[0];
+  if (print) printf("iteration: %u / %u (exploitability = %.4e)\n", G->last_iters, max_iter, e);
+  G->host_dirty = true;
+  if ((rc = ps_finalize(G))) return rc;
+  if (out) *out = e;
+  return PS_OK;
+}
+
+int ps_last_iterations(ps_game* G, uint32_t* out) {
+  if (!G || !out) return fail(PS_ERR_INVALID, "null argument");
+  *out = G->last_iters;
+  return PS_OK;
+}
+
+int ps_solve_step(ps_game* G, uint32_t t) {
+  int rc = need_ready(G);
+  if (rc) return rc;
+  if ((rc = need_boundaries(G))) return rc;
+  Batch& B = *G->b;
+  if ((rc = B.ensure_disc(t + 1))) return rc;
+  CU(cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream));
+  CU(launch_iterate(B.d_spots, 1, B.d_disc, (int)t, (int)t + 1, B.d_scratch, B.scratch_floats, B.d_err, 1, B.block,
+                    B.smem, B.stream));
+  G->host_dirty = true;
+  return B.check_err();
+}
+
+int ps_compute_exploitability(ps_game* G, float* out) {
+  if (!G || !out) return fail(PS_ERR_INVALID, "null argument");
+  if (G->state == GState::TreeBuilt) return fail(PS_ERR_STATE, "Game is not ready");
+  int rc = need_boundaries(G);
+  if (rc) return rc;
+  float e = expl_run(G, &rc);
+  if (rc) return rc;
+  *out = e;
+  return PS_OK;
+}
+
+int ps_finalize(ps_game* G) {
+  int rc = need_ready(G);
+  if (rc) return rc;
+  if ((rc = need_boundaries(G))) return rc;
+  Batch& B = *G->b;
+  CU(cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream));
+  CU(launch_average(B.d_spots, 1, 1, 0, nullptr, B.d_scratch, B.scratch_floats, nullptr, B.d_err, 1, B.block,
+                    B.smem, B.stream));
+  if ((rc = B.check_err())) return rc;
+  G->state = GState::Solved;
+  G->host_dirty = true;
+  if ((rc = sync_host(G))) return rc;
+  auto h = G->action_history;  // set_solved re-applies the history (interpreter.rs:67-71)
+  ps_back_to_root(G);
+  for (size_t a : h) ps_play(G, (int64_t)a);
+  return PS_OK;
+}
+
+int ps_root_cfvalues_with_reach(ps_game* G, int player, const float* opp_reach, float* out) {
+  if (!G || !out || (player != 0 && player != 1)) return fail(PS_ERR_INVALID, "bad argument");
+  if (G->state == GState::TreeBuilt) return fail(PS_ERR_STATE, "Game is not ready");
+  int rc = need_boundaries(G);
+  if (rc) return rc;
+  Batch& B = *G->b;
+  Game& g = *G->g;
+  const int o = player ^ 1;
+  float* d_reach = nullptr;
+  float* d_out = nullptr;
+  std::vector<float> r(g.hs[o], 0.f);
+  for (int h = 0; h < g.H[o]; ++h) r[h] = opp_reach ? opp_reach[h] : g.w[o][h];
+  CU(cudaMalloc(&d_reach, 4 * r.size()));
+  CU(cudaMalloc(&d_out, 4 * (size_t)g.hs[player]));
+  CU(cudaMemcpyAsync(d_reach, r.data(), 4 * r.size(), cudaMemcpyHostToDevice, B.stream));
+  CU(cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream));
+  CU(launch_average(B.d_spots, 1, 0, player, d_reach, B.d_scratch, B.scratch_floats, d_out, B.d_err, 1, B.block,
+                    B.smem, B.stream));
+  CU(cudaMemcpyAsync(out, d_out, 4 * (size_t)g.H[player], cudaMemcpyDeviceToHost, B.stream));
+  CU(cudaStreamSynchronize(B.stream));
+  cudaFree(d_reach);
+  cudaFree(d_out);
+  return B.check_err();
+}
+
+int ps_num_private_hands(ps_game* G, int p) { return G ? G->g->H[p & 1] : fail(PS_ERR_INVALID, "null game"); }
+
+int ps_private_cards(ps_game* G, int p, uint8_t* out) {
+  if (!G || !out) return fail(PS_ERR_INVALID, "null argument");
+  for (int h = 0; h < G->g->H[p & 1]; ++h) {
+    out[2 * h] = G->g->cards[p & 1][h][0];
+    out[2 * h + 1] = G->g->cards[p & 1][h][1];
+  }
+  return PS_OK;
+}
+
+int ps_initial_weights(ps_game* G, int p, float* out) {
+  if (!G || !out) return fail(PS_ERR_INVALID, "null argument");
+  std::copy(G->g->w[p & 1].begin(), G->g->w[p & 1].end(), out);
+  return PS_OK;
+}
+
+double ps_num_combinations(ps_game* G) { return G ? G->g->num_combinations : 0.0; }
+int64_t ps_num_nodes(ps_game* G) { return G ? (int64_t)G->g->arena.size() : -1; }
+
+int ps_node_info(ps_game* G, int64_t idx, int32_t out[8]) {
+  if (!G || idx < 0 || idx >= (int64_t)G->g->arena.size()) return fail(PS_ERR_INVALID, "bad node index");
+  const ArenaNode& n = G->g->arena[idx];
+  out[0] = n.player;
+  out[1] = n.amount;
+  out[2] = n.turn;
+  out[3] = n.river;
+  out[4] = n.nch;
+  out[5] = (int32_t)n.child_off;
+  out[6] = n.prev.kind;
+  out[7] = n.prev.amount;
+  return PS_OK;
+}
+
+int ps_child_indices(ps_game* G, int64_t idx, int64_t* out, int cap) {
+  if (!G || idx < 0 || idx >= (int64_t)G->g->arena.size()) return fail(PS_ERR_INVALID, "bad node index");
+  const ArenaNode& n = G->g->arena[idx];
+  if (n.terminal()) return 0;
+  for (int c = 0; c < n.nch && c < cap; ++c) out[c] = idx + n.child_off + c;
+  return n.nch;
+}
+
+int ps_strategy_at_index(ps_game* G, int64_t idx, float* out) {
+  if (!G || idx < 0 || idx >= (int64_t)G->g->arena.size()) return fail(PS_ERR_INVALID, "bad node index");
+  if (G->state == GState::TreeBuilt) return fail(PS_ERR_STATE, "Memory is not allocated");
+  const ArenaNode& n = G->g->arena[idx];
+  if (n.terminal() || n.chance()) return fail(PS_ERR_INVALID, "strategy_at_index requires a decision node");
+  int rc = sync_host(G);
+  if (rc) return rc;
+  auto v = normalized_strategy(G, n);
+  std::copy(v.begin(), v.end(), out);
+  return (int)v.size();
+}
+
+int64_t ps_node_storage(ps_game* G, int64_t idx, int which, float* out) {
+  if (!G || idx < 0 || idx >= (int64_t)G->g->arena.size()) return fail(PS_ERR_INVALID, "bad node index");
+  if (G->state == GState::TreeBuilt) return fail(PS_ERR_STATE, "Memory is not allocated");
+  int rc = sync_host(G);
+  if (rc) return rc;
+  Game& g = *G->g;
+  const ArenaNode& n = g.arena[idx];
+  if (n.terminal()) return 0;
+  if (which == 4) {
+    if (!n.chance() || n.ch_off == 0xFFFFFFFFu) return 0;
+    int sp = (n.player & PL_MASK) ^ 1;
+    std::copy(G->hCH.begin() + n.ch_off, G->hCH.begin() + n.ch_off + g.H[sp], out);
+    return g.H[sp];
+  }
+  if (n.chance()) return 0;
+  if (which == 3) {
+    if (n.ip_off == 0xFFFFFFFFu) return 0;
+    std::copy(G->hIP.begin() + n.ip_off, G->hIP.begin() + n.ip_off + g.H[1], out);
+    return g.H[1];
+  }
+  const auto& src = which == 1 ? G->hS : G->hR;
+  int p = n.player, H = g.H[p], hs = g.hs[p];
+  for (int a = 0; a < n.nch; ++a)
+    for (int h = 0; h < H; ++h) out[(size_t)a * H + h] = src[n.rs_off + (size_t)a * hs + h];
+  return (int64_t)n.nch * H;
+}
+
+int ps_same_hand_index(ps_game* G, int p, uint16_t* out) {
+  if (!G || !out) return fail(PS_ERR_INVALID, "null argument");
+  std::copy(G->g->same[p & 1].begin(), G->g->same[p & 1].end(), out);
+  return PS_OK;
+}
+
+static int find_board(ps_game* G, int turn, int river) {
+  Game& g = *G->g;
+  for (size_t b = 0; b < g.boards.size(); ++b)
+    if (g.boards[b][3] == (uint8_t)turn && g.boards[b][4] == (uint8_t)river) return (int)b;
+  return -1;
+}
+
+int ps_hand_strength(ps_game* G, int turn, int river, int p, uint16_t* strength, uint16_t* index) {
+  if (!G || G->state == GState::TreeBuilt) return fail(PS_ERR_STATE, "Memory is not allocated");
+  int b = find_board(G, turn, river);
+  if (b < 0) return fail(PS_ERR_INVALID, "board not in this game");
+  Game& g = *G->g;
+  const SpotDev& s = G->b->h_spots[0];
+  int V = 0;
+  CU(cudaMemcpy(&V, s.nvalid[p] + b, 4, cudaMemcpyDeviceToHost));
+  std::vector<uint16_t> ord(V), thr((size_t)g.hs[p] * kThrWords);
+  CU(cudaMemcpy(ord.data(), s.gidx[p] + (size_t)b * 3 * g.hs[p], 2 * (size_t)V, cudaMemcpyDeviceToHost));
+  // the strength of each ordered hand: recover from the opponent's thresholds is
+  // indirect, so evaluate it on the host with the shared evaluator
+  std::vector<int32_t> table(kHandTableSize);
+  build_hand_table(table.data(), kHandTableSize);
+  strength[0] = 0;
+  index[0] = 0;
+  for (int k = 0; k < V; ++k) {
+    int h = ord[k];
+    uint16_t st = 0;
+    if (g.boards[b][4] != NOT_DEALT) {
+      int c7[7] = {g.boards[b][0], g.boards[b][1], g.boards[b][2], g.boards[b][3], g.boards[b][4],
+                   g.cards[p][h][0], g.cards[p][h][1]};
+      st = (uint16_t)(table_index(table.data(), kHandTableSize, hand_value7(c7)) + 1);
+    }
+    strength[k + 1] = st;
+    index[k + 1] = (uint16_t)h;
+  }
+  strength[V + 1] = 0xFFFF;
+  index[V + 1] = 0xFFFF;
+  return V + 2;
+}
+
+int ps_valid_indices(ps_game* G, int turn, int river, int p, uint16_t* out) {
+  if (!G || G->state == GState::TreeBuilt) return fail(PS_ERR_STATE, "Memory is not allocated");
+  int b = find_board(G, turn, river);
+  if (b < 0) return fail(PS_ERR_INVALID, "board not in this game");
+  Game& g = *G->g;
+  const SpotDev& s = G->b->h_spots[0];
+  std::vector<uint16_t> thr((size_t)g.hs[p] * kThrWords);
+  CU(cudaMemcpy(thr.data(), s.thr[p] + (size_t)b * g.hs[p] * kThrWords, 2 * thr.size(), cudaMemcpyDeviceToHost));
+  int n = 0;
+  for (int h = 0; h < g.H[p]; ++h)
+    if (thr[(size_t)h * kThrWords + 6]) out[n++] = (uint16_t)h;
+  return n;
+}
+
+int64_t ps_num_boundary_nodes(ps_game* G) { return G ? G->g->num_boundary : -1; }
+
+int ps_boundary_node_indices(ps_game* G, int64_t* out) {
+  if (!G || !out) return fail(PS_ERR_INVALID, "null argument");
+  for (size_t i = 0; i < G->g->bnd_ordinal.size(); ++i)
+    if (G->g->bnd_ordinal[i] >= 0) out[G->g->bnd_ordinal[i]] = (int64_t)i;
+  return PS_OK;
+}
+
+int ps_set_boundary_cfvs(ps_game* G, int64_t ordinal, int p, const float* cfvs, int64_t n) {
+  if (!G || !cfvs || (p != 0 && p != 1)) return fail(PS_ERR_INVALID, "bad argument");
+  Game& g = *G->g;
+  if (ordinal < 0 || ordinal >= g.num_boundary) return PS_OK;  // ignored like the reference (interpreter.rs:343-348)
+  if (n != g.H[p]) return fail(PS_ERR_INVALID, "cfvs must have one value per private hand");
+  if (G->state == GState::TreeBuilt) return fail(PS_ERR_STATE, "allocate memory before setting boundary values");
+  G->bcfv_host[ordinal * 2 + p].assign(cfvs, cfvs + n);
+  const SpotDev& s = G->b->h_spots[0];
+  CU(cudaMemcpy((float*)s.bcfv + ((size_t)ordinal * 2 + p) * g.vstride, cfvs, 4 * (size_t)n, cudaMemcpyHostToDevice));
+  return PS_OK;
+}
+
+// ---- navigation (query.rs) ----
+int ps_back_to_root(ps_game* G) {
+  if (!G) return fail(PS_ERR_INVALID, "null game");
+  Game& g = *G->g;
+  G->action_history.clear();
+  G->node_history.clear();
+  G->normalized_cached = false;
+  G->turn = g.turn;
+  G->river = g.river;
+  G->turn_swap = -1;
+  G->river_swap[0] = G->river_swap[1] = -1;
+  G->turn_swapped[0] = G->turn_swapped[1] = -1;
+  G->total_bet[0] = G->total_bet[1] = 0;
+  for (int p = 0; p < 2; ++p) G->weights[p] = g.w[p];
+  assign_zero_weights(G);
+  return PS_OK;
+}
+
+int ps_is_terminal_node(ps_game* G) { return G ? (int)is_terminal(G) : fail(PS_ERR_INVALID, "null game"); }
+int ps_is_chance_node(ps_game* G) { return G ? (int)is_chance(G) : fail(PS_ERR_INVALID, "null game"); }
+int ps_current_player(ps_game* G) { return G ? (int)cur(G).player : fail(PS_ERR_INVALID, "null game"); }
+int64_t ps_current_node_index(ps_game* G) { return G ? (int64_t)cur_index(G) : -1; }
+
+int ps_available_actions(ps_game* G, int32_t* kinds, int32_t* amounts, int cap) {
+  if (!G) return fail(PS_ERR_INVALID, "null game");
+  if (is_terminal(G)) return 0;
+  const ArenaNode& n = cur(G);
+  size_t idx = cur_index(G);
+  for (int c = 0; c < n.nch && c < cap; ++c) {
+    const ArenaNode& ch = G->g->arena[idx + n.child_off + c];
+    kinds[c] = ch.prev.kind;
+    amounts[c] = ch.prev.amount;
+  }
+  return n.nch;
+}
+
+uint64_t ps_possible_cards(ps_game* G) {  // query.rs:100-136
+  if (!G || !is_chance(G)) return 0;
+  Game& g = *G->g;
+  uint64_t board = (1ull << g.flop[0]) | (1ull << g.flop[1]) | (1ull << g.flop[2]);
+  if (G->turn != NOT_DEALT) board |= 1ull << G->turn;
+  uint64_t dead = 0;
+  for (int card = 0; card < 52; ++card) {
+    uint64_t nb = board | (1ull << card);
+    bool alive = false;
+    if (nb != board) {
+      for (int i = 0; i < g.H[0] && !alive; ++i) {
+        uint64_t om = (1ull << g.cards[0][i][0]) | (1ull << g.cards[0][i][1]);
+        if (om & nb) continue;
+        uint64_t cm = om | nb;
+        for (int j = 0; j < g.H[1]; ++j) {
+          uint64_t im = (1ull << g.cards[1][j][0]) | (1ull << g.cards[1][j][1]);
+          if (!(im & cm)) {
+            alive = true;
+            break;
+          }
+        }
+      }
+    }
+    if (!alive) dead |= 1ull << card;
+  }
+  return ((1ull << 52) - 1) ^ dead;
+}
+
+int ps_strategy(ps_game* G, float* out) {  // query.rs:346-378
+  if (!G) return fail(PS_ERR_INVALID, "null game");
+  if (G->state == GState::TreeBuilt) return fail(PS_ERR_STATE, "Memory is not allocated");
+  if (is_terminal(G)) return fail(PS_ERR_STATE, "Terminal node is not allowed");
+  if (is_chance(G)) return fail(PS_ERR_STATE, "Chance node is not allowed");
+  int rc = sync_host(G);
+  if (rc) return rc;
+  const ArenaNode& n = cur(G);
+  auto v = normalized_strategy(G, n);
+  int H = G->g->H[n.player];
+  for (int a = 0; a < n.nch; ++a) apply_swap(G, v.data() + (size_t)a * H, n.player, false);
+  std::copy(v.begin(), v.end(), out);
+  return (int)v.size();
+}
+
+int ps_play(ps_game* G, int64_t action) {  // query.rs:186-335
+  if (!G) return fail(PS_ERR_INVALID, "null game");
+  if (G->state == GState::TreeBuilt) return fail(PS_ERR_STATE, "Memory is not allocated");
+  if (is_terminal(G)) return fail(PS_ERR_STATE, "Terminal node is not allowed");
+  Game& g = *G->g;
+  size_t idx = cur_index(G);
+  const ArenaNode& n = g.arena[idx];
+  if (is_chance(G)) {
+    bool is_turn = G->turn == NOT_DEALT;
+    int actual = action < 0 ? __builtin_ctzll(ps_possible_cards(G)) : (int)action;
+    int card = actual;
+    if (G->turn_swapped[0] >= 0) {
+      int s1 = G->turn_swapped[0], s2 = G->turn_swapped[1];
+      if ((actual & 3) == s1) card = actual - s1 + s2;
+      else if ((actual & 3) == s2) card = actual + s1 - s2;
+    }
+    int ai = -1;
+    for (int c = 0; c < n.nch; ++c)
+      if (g.arena[idx + n.child_off + c].prev.amount == card) {
+        ai = c;
+        break;
+      }
+    if (ai < 0) {
+      const auto& iref = n.turn == NOT_DEALT ? g.iso_ref_turn : g.iso_ref_river[n.turn];
+      const auto& icard = n.turn == NOT_DEALT ? g.iso_card_turn : g.iso_card_river[n.turn & 3];
+      for (size_t i = 0; i < iref.size(); ++i)
+        if (card == icard[i]) {
+          ai = iref[i];
+          if (is_turn) {
+            G->turn_swapped[0] = card & 3;
+            G->turn_swapped[1] = g.arena[idx + n.child_off + ai].prev.amount & 3;
+            G->turn_swap = card & 3;
+          } else {
+            G->river_swap[0] = G->turn & 3;
+            G->river_swap[1] = icard[i] & 3;
+          }
+          break;
+        }
+    }
+    if (ai < 0) return fail(PS_ERR_INVALID, "Invalid action");
+    G->node_history.push_back(idx + n.child_off + ai);
+    if (is_turn) G->turn = (uint8_t)actual;
+    else G->river = (uint8_t)actual;
+    assign_zero_weights(G);
+  } else {
+    if (action < 0 || action >= n.nch) return fail(PS_ERR_INVALID, "Invalid action");
+    int rc = sync_host(G);
+    if (rc) return rc;
+    int p = n.player, H = g.H[p];
+    if (n.nch > 1) {
+      std::vector<float> st((size_t)n.nch * H);
+      rc = ps_strategy(G, st.data());
+      if (rc < 0) return rc;
+      for (int h = 0; h < H; ++h) G->weights[p][h] *= st[(size_t)action * H + h];
+    }
+    for (int h = 0; h < H; ++h) G->cfv_cache[p][h] = G->hR[n.rs_off + (size_t)action * g.hs[p] + h];
+    const Act& pa = g.arena[idx + n.child_off + action].prev;
+    if (pa.kind == ACT_CALL) {
+      G->total_bet[p] = G->total_bet[p ^ 1];
+    } else if (pa.kind == ACT_BET || pa.kind == ACT_RAISE || pa.kind == ACT_ALLIN) {
+      int prev = (n.prev.kind == ACT_BET || n.prev.kind == ACT_RAISE || n.prev.kind == ACT_ALLIN) ? n.prev.amount : 0;
+      int to_call = G->total_bet[p ^ 1] - G->total_bet[p];
+      G->total_bet[p] += pa.amount - prev + to_call;
+    }
+    G->node_history.push_back(idx + n.child_off + action);
+  }
+  G->action_history.push_back((size_t)action);
+  G->normalized_cached = false;
+  return PS_OK;
+}
+
+int ps_cache_normalized_weights(ps_game* G) {  // query.rs:498-567
+  if (!G) return fail(PS_ERR_INVALID, "null game");
+  if (G->normalized_cached) return PS_OK;
+  Game& g = *G->g;
+  uint64_t board = 0;
+  if (G->turn != NOT_DEALT) board |= 1ull << G->turn;
+  if (G->river != NOT_DEALT) board |= 1ull << G->river;
+  double ws[2] = {0, 0}, wm[2][52];
+  for (int p = 0; p < 2; ++p) {
+    for (int c = 0; c < 52; ++c) wm[p][c] = 0;
+    for (int i = 0; i < g.H[p]; ++i) {
+      int c1 = g.cards[p][i][0], c2 = g.cards[p][i][1];
+      if (((1ull << c1) | (1ull << c2)) & board) continue;
+      double w = G->weights[p][i];
+      ws[p] += w;
+      wm[p][c1] += w;
+      wm[p][c2] += w;
+    }
+  }
+  for (int p = 0; p < 2; ++p)
+    for (int i = 0; i < g.H[p]; ++i) {
+      int c1 = g.cards[p][i][0], c2 = g.cards[p][i][1];
+      if (((1ull << c1) | (1ull << c2)) & board) {
+        G->normalized[p][i] = 0.f;
+        continue;
+      }
+      uint16_t si = g.same[p][i];
+      double osame = si == 0xFFFF ? 0.0 : (double)G->weights[p ^ 1][si];
+      double ow = ws[p ^ 1] + osame - wm[p ^ 1][c1] - wm[p ^ 1][c2];
+      G->normalized[p][i] = G->weights[p][i] * (float)ow;
+    }
+  G->normalized_cached = true;
+  return PS_OK;
+}
+
+int ps_weights(ps_game* G, int p, int normalized, float* out) {
+  if (!G || !out) return fail(PS_ERR_INVALID, "null argument");
+  const auto& v = normalized ? G->normalized[p & 1] : G->weights[p & 1];
+  std::copy(v.begin(), v.end(), out);
+  return PS_OK;
+}
+
+int ps_total_bet_amount(ps_game* G, int32_t out[2]) {
+  if (!G) return fail(PS_ERR_INVALID, "null game");
+  out[0] = G->total_bet[0];
+  out[1] = G->total_bet[1];
+  return PS_OK;
+}
+
+int ps_expected_values(ps_game* G, int player, int detail, float* out) {  // query.rs:639-760
+  if (!G || !out || (player != 0 && player != 1)) return fail(PS_ERR_INVALID, "bad argument");
+  if (G->state != GState::Solved) return fail(PS_ERR_STATE, "Game is not solved");
+  if (!G->normalized_cached) return fail(PS_ERR_STATE, "Normalized weights are not cached");
+  Game& g = *G->g;
+  int rc = sync_host(G);
+  if (rc) return rc;
+  size_t idx = cur_index(G);
+  const ArenaNode& n = g.arena[idx];
+  const int H = g.H[player];
+  int cf = 1;
+  if (g.turn == NOT_DEALT && G->turn != NOT_DEALT) cf *= 45;
+  if (g.river == NOT_DEALT && G->river != NOT_DEALT) cf *= 44;
+  bool have_actions = false;
+  float normalizer = (float)(g.num_combinations * (double)cf);
+  std::vector<float> ret;
+  if (n.terminal()) {
+    normalizer = (float)g.num_combinations;
+    Batch& B = *G->b;
+    const int o = player ^ 1;
+    std::vector<float> reach(g.hs[o], 0.f);
+    std::copy(G->weights[o].begin(), G->weights[o].end(), reach.begin());
+    CU(cudaMemcpyAsync(B.d_scratch, reach.data(), 4 * reach.size(), cudaMemcpyHostToDevice, B.stream));
+    Op op{};
+    op.type = OP_TERM;
+    op.node = (uint32_t)idx;
+    op.src = 0;
+    op.dst = 1;
+    op.board = (uint16_t)g.node_board[idx];
+    op.term = n.boundary() ? TERM_BOUNDARY : n.fold() ? TERM_FOLD : TERM_SHOWDOWN;
+    op.fold_pl = n.player & PL_MASK;
+    if (n.boundary() && (rc = need_boundaries(G))) return rc;
+    CU(cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream));
+    CU(launch_eval_terminal(B.d_spots, op, player, B.d_scratch, B.scratch_floats, B.d_err, B.block, B.smem, B.stream));
+    ret.resize(H);
+    CU(cudaMemcpyAsync(ret.data(), B.d_scratch + g.vstride, 4 * (size_t)H, cudaMemcpyDeviceToHost, B.stream));
+    CU(cudaStreamSynchronize(B.stream));
+    if ((rc = B.check_err())) return rc;
+  } else if (n.chance() && n.ch_off != 0xFFFFFFFFu && ((n.player & PL_MASK) ^ 1) == player) {
+    ret.assign(G->hCH.begin() + n.ch_off, G->hCH.begin() + n.ch_off + H);
+  } else if (!n.chance() && n.ip_off != 0xFFFFFFFFu && player == 1) {
+    ret.assign(G->hIP.begin() + n.ip_off, G->hIP.begin() + n.ip_off + H);
+  } else if (!n.chance() && player == n.player) {
+    have_actions = true;
+    ret.resize((size_t)n.nch * H);
+    for (int a = 0; a < n.nch; ++a)
+      for (int h = 0; h < H; ++h) ret[(size_t)a * H + h] = G->hR[n.rs_off + (size_t)a * g.hs[player] + h];
+  } else {
+    ret = G->cfv_cache[player];
+  }
+  int bias = std::max(G->total_bet[player] - G->total_bet[player ^ 1], 0);
+  for (size_t a = 0; a * H < ret.size(); ++a) {
+    bool is_fold = have_actions && g.arena[idx + n.child_off + a].prev.kind == ACT_FOLD;
+    apply_swap(G, ret.data() + a * H, player, false);
+    for (int h = 0; h < H; ++h) {
+      float& v = ret[a * H + h];
+      float wr = G->weights[player][h], wn = G->normalized[player][h];
+      if (is_fold || wn == 0.0f) {
+        v = 0.0f;
+      } else {
+        v *= normalizer * (wr / wn);
+        v += (float)g.cfg.starting_pot * 0.5f + (float)(n.amount + bias);
+      }
+    }
+  }
+  if (!detail && !is_terminal(G) && !is_chance(G) && (int)n.player == player) {
+    std::vector<float> st((size_t)n.nch * H);
+    rc = ps_strategy(G, st.data());
+    if (rc < 0) return rc;
+    for (int h = 0; h < H; ++h) {
+      float ev = 0.f;
+      for (int a = 0; a < n.nch; ++a) ev += ret[h + (size_t)a * H] * st[h + (size_t)a * H];
+      out[h] = ev;
+    }
+    return H;
+  }
+  std::copy(ret.begin(), ret.end(), out);
+  return (int)ret.size();
+}
+
+// ---- checkpoint ----
+int ps_state_export(ps_game* G, void* buf, uint64_t cap, uint64_t* needed) {
+  if (!G || !needed) return fail(PS_ERR_INVALID, "null argument");
+  if (G->state == GState::TreeBuilt) return fail(PS_ERR_STATE, "Memory is not allocated");
+  Game& g = *G->g;
+  uint64_t n = 16 + 8 * g.num_storage;
+  *needed = n;
+  if (!buf) return PS_OK;
+  if (cap < n) return fail(PS_ERR_INVALID, "buffer too small");
+  uint64_t hdr[2] = {0x3153505342303032ull, g.num_storage};
+  std::memcpy(buf, hdr, 16);
+  const SpotDev& s = G->b->h_spots[0];
+  CU(cudaMemcpy((char*)buf + 16, s.S, 4 * g.num_storage, cudaMemcpyDeviceToHost));
+  CU(cudaMemcpy((char*)buf + 16 + 4 * g.num_storage, s.R, 4 * g.num_storage, cudaMemcpyDeviceToHost));
+  return PS_OK;
+}
+
+int ps_state_import(ps_game* G, const void* buf, uint64_t size) {
+  if (!G || !buf) return fail(PS_ERR_INVALID, "null argument");
+  if (G->state == GState::TreeBuilt) return fail(PS_ERR_STATE, "Memory is not allocated");
+  Game& g = *G->g;
+  uint64_t hdr[2];
+  if (size < 16) return fail(PS_ERR_INVALID, "storage size mismatch");
+  std::memcpy(hdr, buf, 16);
+  if (hdr[0] != 0x3153505342303032ull || hdr[1] != g.num_storage || size != 16 + 8 * g.num_storage)
+    return fail(PS_ERR_INVALID, "storage size mismatch");
+  const SpotDev& s = G->b->h_spots[0];
+  CU(cudaMemcpy(s.S, (const char*)buf + 16, 4 * g.num_storage, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(s.R, (const char*)buf + 16 + 4 * g.num_storage, 4 * g.num_storage, cudaMemcpyHostToDevice));
+  G->host_dirty = true;
+  return PS_OK;
+}
+
+// ---- batch ----
+struct ps_batch {
+  std::unique_ptr<Batch> b;
+};
+
+int ps_batch_new(const ps_card_config* cards, const ps_tree_config* trees, int32_t n, const ps_batch_opts* opts,
+                 ps_batch** out) {
+  if (!cards || !trees || !out || n <= 0) return fail(PS_ERR_INVALID, "bad argument");
+  *out = nullptr;
+  auto B = std::make_unique<Batch>();
+  B->games.resize(n);
+  std::vector<std::string> errs(n);
+  // tree construction is host work per spot: spread over the host cores
+  int T = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
+  std::vector<std::thread> th;
+  std::vector<int> ok(n, 0);
+  for (int t = 0; t < T; ++t)
+    th.emplace_back([&, t]() {
+      for (int i = t; i < n; i += T) {
+        TreeCfg tc;
+        if (!parse_tree_config(&trees[i], tc, errs[i])) continue;
+        auto g = std::make_unique<Game>();
+        const ps_card_config& c = cards[i];
+        uint8_t board[5] = {c.flop[0], c.flop[1], c.flop[2], c.turn, c.river};
+        if (!c.range[0] || !c.range[1]) {
+          errs[i] = "null range";
+          continue;
+        }
+        if (!g->init(c.range[0], c.range[1], board, tc, errs[i])) continue;
+        if (g->num_boundary > 0) {
+          errs[i] = "depth-boundary trees are not supported in batches";
+          continue;
+        }
+        B->games[i] = std::move(g);
+        ok[i] = 1;
+      }
+    });
+  for (auto& x : th) x.join();
+  for (int i = 0; i < n; ++i)
+    if (!ok[i]) return fail(PS_ERR_INVALID, "spot " + std::to_string(i) + ": " + errs[i]);
+  int rc = B->build(opts);
+  if (rc) return rc;
+  auto* pb = new ps_batch();
+  pb->b = std::move(B);
+  *out = pb;
+  return PS_OK;
+}
+
+void ps_batch_free(ps_batch* b) { delete b; }
+
+int ps_batch_solve(ps_batch* pb, uint32_t max_iter, const float* target) {
+  if (!pb || !target) return fail(PS_ERR_INVALID, "bad argument");
+  return pb->b->solve(max_iter, target, true);
+}
+
+int ps_batch_results(ps_batch* pb, float* expl, int32_t* iters) {
+  if (!pb) return fail(PS_ERR_INVALID, "null batch");
+  Batch& B = *pb->b;
+  if (B.h_expl.empty()) return fail(PS_ERR_STATE, "batch not solved");
+  if (expl) std::copy(B.h_expl.begin(), B.h_expl.end(), expl);
+  if (iters) std::copy(B.h_iters.begin(), B.h_iters.end(), iters);
+  return PS_OK;
+}
+
+int ps_batch_root_strategy(ps_batch* pb, int32_t spot, float* out) {
+  if (!pb || spot < 0 || spot >= (int)pb->b->games.size()) return fail(PS_ERR_INVALID, "bad spot");
+  Batch& B = *pb->b;
+  Game& g = *B.games[spot];
+  size_t root = 0;
+  while (!g.arena[root].terminal() && !g.arena[root].chance() && g.arena[root].nch == 1) root += g.arena[root].child_off;
+  const ArenaNode& n = g.arena[root];
+  int p = n.player, H = g.H[p], hs = g.hs[p], na = n.nch;
+  std::vector<float> S((size_t)na * hs);
+  CU(cudaMemcpy(S.data(), B.h_spots[spot].S + n.rs_off, 4 * S.size(), cudaMemcpyDeviceToHost));
+  float def = 1.0f / (float)na;
+  for (int h = 0; h < H; ++h) {
+    float d = S[h];
+    for (int a = 1; a < na; ++a) d += S[(size_t)a * hs + h];
+    for (int a = 0; a < na; ++a) out[(size_t)a * H + h] = d == 0.0f ? def : S[(size_t)a * hs + h] / d;
+  }
+  return na * H;
+}
+
+int ps_batch_last_timing(ps_batch* pb, float* solve_ms, float* setup_ms) {
+  if (!pb) return fail(PS_ERR_INVALID, "null batch");
+  if (solve_ms) *solve_ms = pb->b->last_solve_ms;
+  if (setup_ms) *setup_ms = pb->b->last_setup_ms;
+  return PS_OK;
+}
+
+double ps_batch_iteration_bytes(ps_batch* pb, int32_t spot) {
+  if (!pb || spot < 0 || spot >= (int)pb->b->games.size()) return -1.0;
+  Game& g = *pb->b->games[spot];
+  double s = 0;
+  for (const auto& n : g.arena)
+    if (!n.terminal() && !n.chance() && n.nch > 1) s += (double)n.nch * g.H[n.player];
+  return 20.0 * s;
+}
+
+int ps_batch_io_bytes(ps_batch* pb, uint64_t* h2d, uint64_t* d2h) {
+  if (!pb) return fail(PS_ERR_INVALID, "null batch");
+  Batch& B = *pb->b;
+  const size_t n = B.games.size();
+  if (h2d) *h2d = B.static_bytes + n * (sizeof(SpotDev) + sizeof(int) + sizeof(float)) + (size_t)B.nwork * sizeof(int2);
+  if (d2h) *d2h = n * (sizeof(float) + sizeof(int));
+  return PS_OK;
+}
+
+int ps_batch_config(ps_batch* pb, int32_t* block, int32_t* grid, int32_t* cps) {
+  if (!pb) return fail(PS_ERR_INVALID, "null batch");
+  if (block) *block = pb->b->block;
+  if (grid) *grid = pb->b->grid;
+  if (cps) *cps = pb->b->ctas_per_sm;
+  return PS_OK;
+}
+
+}  // extern "C"

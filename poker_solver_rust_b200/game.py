@@ -1,0 +1,461 @@
+"""Python mirror of the reference's game / solve API (crates/range-solver).
+
+Names follow the reference: ``TreeConfig`` / ``BetSizeOptions`` /
+``ActionTree`` (action_tree.rs, bet_size.rs), ``CardConfig`` (card.rs),
+``PostFlopGame`` with ``with_config`` / ``allocate_memory`` and the query
+methods (game/interpreter.rs, game/query.rs), and the solver functions
+``solve``, ``solve_step``, ``compute_exploitability``, ``finalize``,
+``root_cfvalues``, ``root_cfvalues_with_reach`` (solver.rs, utility.rs).
+Every call goes through the C ABI of ``_lib/libps_b200.so``; there is no
+Python or CPU fallback for any of the compute.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from enum import IntEnum
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _native as N
+from .cards import NOT_DEALT, Range
+
+ACTION_NAMES = ["None", "Fold", "Check", "Call", "Bet", "Raise", "AllIn", "Chance"]
+
+
+class BoardState(IntEnum):  # action_tree.rs:76-84
+    Flop = 0
+    Turn = 1
+    River = 2
+
+
+@dataclass
+class BetSizeOptions:
+    """Bet and raise size strings exactly as the reference parses them
+    (bet_size.rs:82-112), e.g. ``BetSizeOptions("50%, 100%, a", "100%")``."""
+
+    bet: str = ""
+    raise_: str = ""
+
+
+@dataclass
+class TreeConfig:  # action_tree.rs:130-192
+    initial_state: BoardState = BoardState.Flop
+    starting_pot: int = 0
+    effective_stack: int = 0
+    rake_rate: float = 0.0
+    rake_cap: float = 0.0
+    flop_bet_sizes: Sequence[BetSizeOptions] = field(default_factory=lambda: [BetSizeOptions(), BetSizeOptions()])
+    turn_bet_sizes: Sequence[BetSizeOptions] = field(default_factory=lambda: [BetSizeOptions(), BetSizeOptions()])
+    river_bet_sizes: Sequence[BetSizeOptions] = field(default_factory=lambda: [BetSizeOptions(), BetSizeOptions()])
+    turn_donk_sizes: Optional[str] = None
+    river_donk_sizes: Optional[str] = None
+    add_allin_threshold: float = 0.0
+    force_allin_threshold: float = 0.0
+    merging_threshold: float = 0.0
+    depth_limit: Optional[int] = None
+    max_bets: int = 0  # extension (0 = no cap, as the reference)
+
+    def to_c(self) -> N.PsTreeConfig:
+        c = N.PsTreeConfig()
+        c.initial_state = int(self.initial_state)
+        c.starting_pot = int(self.starting_pot)
+        c.effective_stack = int(self.effective_stack)
+        c.depth_limit = -1 if self.depth_limit is None else int(self.depth_limit)
+        c.rake_rate = float(self.rake_rate)
+        c.rake_cap = float(self.rake_cap)
+        c.add_allin_threshold = float(self.add_allin_threshold)
+        c.force_allin_threshold = float(self.force_allin_threshold)
+        c.merging_threshold = float(self.merging_threshold)
+        c.max_bets = int(self.max_bets)
+        keep = []
+        for si, street in enumerate((self.flop_bet_sizes, self.turn_bet_sizes, self.river_bet_sizes)):
+            for p in range(2):
+                for k, s in enumerate((street[p].bet, street[p].raise_)):
+                    b = s.encode()
+                    keep.append(b)
+                    c.bet_sizes[si * 4 + p * 2 + k] = b
+        for k, d in enumerate((self.turn_donk_sizes, self.river_donk_sizes)):
+            if d is not None:
+                b = d.encode()
+                keep.append(b)
+                c.donk_sizes[k] = b
+        c._keep = keep
+        return c
+
+    def to_dict(self) -> dict:
+        """Plain form used to feed the same configuration to the oracle."""
+        def ms(street):
+            return [(street[p].bet, street[p].raise_) for p in range(2)]
+        return {
+            "initial_state": ["flop", "turn", "river"][int(self.initial_state)],
+            "starting_pot": self.starting_pot,
+            "effective_stack": self.effective_stack,
+            "rake_rate": self.rake_rate,
+            "rake_cap": self.rake_cap,
+            "flop_bet_sizes": ms(self.flop_bet_sizes),
+            "turn_bet_sizes": ms(self.turn_bet_sizes),
+            "river_bet_sizes": ms(self.river_bet_sizes),
+            "turn_donk_sizes": self.turn_donk_sizes,
+            "river_donk_sizes": self.river_donk_sizes,
+            "add_allin_threshold": self.add_allin_threshold,
+            "force_allin_threshold": self.force_allin_threshold,
+            "merging_threshold": self.merging_threshold,
+            "depth_limit": self.depth_limit,
+        }
+
+
+class ActionTree:
+    """The abstract betting tree of a TreeConfig (action_tree.rs:326-334).
+    The tree itself is built inside the library when the game is created."""
+
+    def __init__(self, config: TreeConfig):
+        self.config = config
+
+    @classmethod
+    def new(cls, config: TreeConfig):
+        return cls(config)
+
+
+@dataclass
+class CardConfig:  # card.rs:19-32
+    range: Sequence[Range]
+    flop: Sequence[int]
+    turn: int = NOT_DEALT
+    river: int = NOT_DEALT
+
+    def to_c(self) -> N.PsCardConfig:
+        c = N.PsCardConfig()
+        r0 = np.ascontiguousarray(self.range[0].raw_data(), np.float32)
+        r1 = np.ascontiguousarray(self.range[1].raw_data(), np.float32)
+        c.range[0] = r0.ctypes.data_as(C.POINTER(C.c_float))
+        c.range[1] = r1.ctypes.data_as(C.POINTER(C.c_float))
+        for i in range(3):
+            c.flop[i] = int(self.flop[i])
+        c.turn = int(self.turn)
+        c.river = int(self.river)
+        c._keep = (r0, r1)
+        return c
+
+
+def _f32(n):
+    return np.zeros(n, np.float32)
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class PostFlopGame:
+    """A subgame on the GPU (game/mod.rs PostFlopGame)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def with_config(cls, card_config: CardConfig, action_tree: ActionTree) -> "PostFlopGame":
+        L = N.lib()
+        cc = card_config.to_c()
+        tc = action_tree.config.to_c()
+        h = C.c_void_p()
+        N.check(L.ps_game_new(C.byref(cc), C.byref(tc), C.byref(h)))
+        return cls(h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            N.lib().ps_game_free(h)
+            self._h = None
+
+    # ---- construction ----
+    def memory_usage(self) -> int:
+        v = C.c_uint64()
+        N.check(N.lib().ps_game_memory_usage(self._h, C.byref(v)))
+        return int(v.value)
+
+    def allocate_memory(self, enable_compression: bool = False) -> None:
+        N.check(N.lib().ps_game_allocate_memory(self._h, int(enable_compression)))
+
+    def num_private_hands(self, player: int) -> int:
+        return N.check(N.lib().ps_num_private_hands(self._h, player))
+
+    def private_cards(self, player: int) -> np.ndarray:
+        n = self.num_private_hands(player)
+        out = np.zeros(2 * n, np.uint8)
+        N.check(N.lib().ps_private_cards(self._h, player, out.ctypes.data_as(C.POINTER(C.c_uint8))))
+        return out.reshape(n, 2)
+
+    def initial_weights(self, player: int) -> np.ndarray:
+        out = _f32(self.num_private_hands(player))
+        N.check(N.lib().ps_initial_weights(self._h, player, _fp(out)))
+        return out
+
+    def num_combinations(self) -> float:
+        return float(N.lib().ps_num_combinations(self._h))
+
+    def num_nodes(self) -> int:
+        return int(N.lib().ps_num_nodes(self._h))
+
+    def node_info(self, idx: int) -> dict:
+        out = np.zeros(8, np.int32)
+        N.check(N.lib().ps_node_info(self._h, idx, out.ctypes.data_as(C.POINTER(C.c_int32))))
+        keys = ("player", "amount", "turn", "river", "num_children", "children_offset", "prev_kind", "prev_amount")
+        return dict(zip(keys, (int(x) for x in out)))
+
+    def child_indices(self, idx: int):
+        out = np.zeros(64, np.int64)
+        n = N.check(N.lib().ps_child_indices(self._h, idx, out.ctypes.data_as(C.POINTER(C.c_int64)), 64))
+        return [int(x) for x in out[:n]]
+
+    def same_hand_index(self, player: int) -> np.ndarray:
+        out = np.zeros(self.num_private_hands(player), np.uint16)
+        N.check(N.lib().ps_same_hand_index(self._h, player, out.ctypes.data_as(C.POINTER(C.c_uint16))))
+        return out
+
+    def hand_strength(self, turn: int, river: int, player: int):
+        s = np.zeros(2000, np.uint16)
+        i = np.zeros(2000, np.uint16)
+        n = N.check(N.lib().ps_hand_strength(self._h, turn, river, player, s.ctypes.data_as(C.POINTER(C.c_uint16)),
+                                             i.ctypes.data_as(C.POINTER(C.c_uint16))))
+        return s[:n].copy(), i[:n].copy()
+
+    def valid_indices(self, turn: int, river: int, player: int) -> np.ndarray:
+        out = np.zeros(2000, np.uint16)
+        n = N.check(N.lib().ps_valid_indices(self._h, turn, river, player, out.ctypes.data_as(C.POINTER(C.c_uint16))))
+        return out[:n].copy()
+
+    def strategy_at_index(self, idx: int) -> np.ndarray:
+        out = _f32(200000)
+        n = N.check(N.lib().ps_strategy_at_index(self._h, idx, _fp(out)))
+        return out[:n].copy()
+
+    def node_storage(self, idx: int, which: int) -> np.ndarray:
+        out = _f32(200000)
+        n = N.check(N.lib().ps_node_storage(self._h, idx, which, _fp(out)))
+        return out[:n].copy()
+
+    # ---- depth boundary ----
+    def num_boundary_nodes(self) -> int:
+        return int(N.lib().ps_num_boundary_nodes(self._h))
+
+    def boundary_node_indices(self):
+        n = self.num_boundary_nodes()
+        out = np.zeros(max(n, 1), np.int64)
+        N.check(N.lib().ps_boundary_node_indices(self._h, out.ctypes.data_as(C.POINTER(C.c_int64))))
+        return out[:n].copy()
+
+    def set_boundary_cfvs(self, ordinal: int, player: int, cfvs) -> None:
+        v = np.ascontiguousarray(cfvs, np.float32)
+        N.check(N.lib().ps_set_boundary_cfvs(self._h, ordinal, player, _fp(v), len(v)))
+
+    # ---- navigation / queries ----
+    def back_to_root(self):
+        N.check(N.lib().ps_back_to_root(self._h))
+
+    def play(self, action: int):
+        N.check(N.lib().ps_play(self._h, action))
+
+    def available_actions(self):
+        k = np.zeros(256, np.int32)
+        a = np.zeros(256, np.int32)
+        n = N.check(N.lib().ps_available_actions(self._h, k.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                 a.ctypes.data_as(C.POINTER(C.c_int32)), 256))
+        return [(ACTION_NAMES[k[i]], int(a[i])) for i in range(n)]
+
+    def is_terminal_node(self) -> bool:
+        return bool(N.check(N.lib().ps_is_terminal_node(self._h)))
+
+    def is_chance_node(self) -> bool:
+        return bool(N.check(N.lib().ps_is_chance_node(self._h)))
+
+    def current_player(self) -> int:
+        return N.check(N.lib().ps_current_player(self._h))
+
+    def current_node_index(self) -> int:
+        return int(N.lib().ps_current_node_index(self._h))
+
+    def possible_cards(self) -> int:
+        return int(N.lib().ps_possible_cards(self._h))
+
+    def strategy(self) -> np.ndarray:
+        out = _f32(200000)
+        n = N.check(N.lib().ps_strategy(self._h, _fp(out)))
+        return out[:n].copy()
+
+    def cache_normalized_weights(self):
+        N.check(N.lib().ps_cache_normalized_weights(self._h))
+
+    def weights(self, player: int) -> np.ndarray:
+        out = _f32(self.num_private_hands(player))
+        N.check(N.lib().ps_weights(self._h, player, 0, _fp(out)))
+        return out
+
+    def normalized_weights(self, player: int) -> np.ndarray:
+        out = _f32(self.num_private_hands(player))
+        N.check(N.lib().ps_weights(self._h, player, 1, _fp(out)))
+        return out
+
+    def expected_values(self, player: int) -> np.ndarray:
+        out = _f32(200000)
+        n = N.check(N.lib().ps_expected_values(self._h, player, 0, _fp(out)))
+        return out[:n].copy()
+
+    def expected_values_detail(self, player: int) -> np.ndarray:
+        out = _f32(200000)
+        n = N.check(N.lib().ps_expected_values(self._h, player, 1, _fp(out)))
+        return out[:n].copy()
+
+    def total_bet_amount(self):
+        out = np.zeros(2, np.int32)
+        N.check(N.lib().ps_total_bet_amount(self._h, out.ctypes.data_as(C.POINTER(C.c_int32))))
+        return [int(out[0]), int(out[1])]
+
+    # ---- checkpoint ----
+    def storage_export(self) -> bytes:
+        need = C.c_uint64()
+        N.check(N.lib().ps_state_export(self._h, None, 0, C.byref(need)))
+        buf = C.create_string_buffer(need.value)
+        N.check(N.lib().ps_state_export(self._h, buf, need.value, C.byref(need)))
+        return buf.raw
+
+    def storage_import(self, data: bytes):
+        N.check(N.lib().ps_state_import(self._h, data, len(data)))
+
+    @property
+    def last_iterations(self) -> int:
+        v = C.c_uint32()
+        N.check(N.lib().ps_last_iterations(self._h, C.byref(v)))
+        return int(v.value)
+
+
+# ---- solver functions (solver.rs, utility.rs) ----
+def solve(game: PostFlopGame, max_num_iterations: int, target_exploitability: float, print_progress: bool = False) -> float:
+    e = C.c_float()
+    N.check(N.lib().ps_solve(game._h, max_num_iterations, target_exploitability, int(print_progress), C.byref(e)))
+    return float(e.value)
+
+
+def solve_step(game: PostFlopGame, current_iteration: int) -> None:
+    N.check(N.lib().ps_solve_step(game._h, current_iteration))
+
+
+def compute_exploitability(game: PostFlopGame) -> float:
+    e = C.c_float()
+    N.check(N.lib().ps_compute_exploitability(game._h, C.byref(e)))
+    return float(e.value)
+
+
+def finalize(game: PostFlopGame) -> None:
+    N.check(N.lib().ps_finalize(game._h))
+
+
+def root_cfvalues_with_reach(game: PostFlopGame, player: int, opp_reach) -> np.ndarray:
+    r = None if opp_reach is None else np.ascontiguousarray(opp_reach, np.float32)
+    out = _f32(game.num_private_hands(player))
+    N.check(N.lib().ps_root_cfvalues_with_reach(game._h, player, None if r is None else _fp(r), _fp(out)))
+    return out
+
+
+def root_cfvalues(game: PostFlopGame, player: int) -> np.ndarray:
+    return root_cfvalues_with_reach(game, player, None)
+
+
+def compute_average(values, weights) -> float:  # utility.rs:127-136
+    v = np.asarray(values, np.float64)
+    w = np.asarray(weights, np.float64)
+    return float(np.float32((v * w).sum() / w.sum()))
+
+
+def discount_params(t: int):
+    out = np.zeros(3, np.float32)
+    N.check(N.lib().ps_discount_params(t, _fp(out)))
+    return float(out[0]), float(out[1]), float(out[2])
+
+
+BET_KINDS = ["PotRelative", "PrevBetRelative", "Additive", "Geometric", "AllIn"]
+
+
+def parse_bet_sizes(sizes: str, is_raise: bool):
+    """BetSizeOptions::try_from for one list: [(kind, float, int, cap)]."""
+    k = np.zeros(64, np.int32)
+    f = np.zeros(64)
+    i = np.zeros(64, np.int32)
+    c = np.zeros(64, np.int32)
+    n = N.check(N.lib().ps_parse_bet_sizes(sizes.encode(), int(is_raise), k.ctypes.data_as(C.POINTER(C.c_int32)),
+                                           f.ctypes.data_as(C.POINTER(C.c_double)),
+                                           i.ctypes.data_as(C.POINTER(C.c_int32)),
+                                           c.ctypes.data_as(C.POINTER(C.c_int32)), 64))
+    return [(BET_KINDS[k[j]], float(f[j]), int(i[j]), int(c[j])) for j in range(n)]
+
+
+def hand_table() -> np.ndarray:
+    out = np.zeros(8192, np.int32)
+    n = N.lib().ps_hand_table(out.ctypes.data_as(C.POINTER(C.c_int32)), 8192)
+    return out[:n].copy()
+
+
+# ---- batched datagen path ----
+class BatchSolver:
+    """Thousands of independent subgames solved by one persistent launch
+    (replaces the per-spot GpuBatchSolver launches of the reference's GPU
+    datagen, crates/cfvnet/src/datagen/domain/pipeline.rs:232-343)."""
+
+    def __init__(self, card_configs: Sequence[CardConfig], tree_configs: Sequence[TreeConfig],
+                 block_threads: int = 0, ctas_per_sm: int = 0, sort_by_cost: bool = True):
+        n = len(card_configs)
+        cc = (N.PsCardConfig * n)()
+        tc = (N.PsTreeConfig * n)()
+        keep = []
+        for i in range(n):
+            c = card_configs[i].to_c()
+            t = tree_configs[i].to_c()
+            keep.append((c._keep, t._keep))
+            cc[i] = c
+            tc[i] = t
+        opts = N.PsBatchOpts(block_threads, ctas_per_sm, int(sort_by_cost), 0)
+        h = C.c_void_p()
+        N.check(N.lib().ps_batch_new(cc, tc, n, C.byref(opts), C.byref(h)))
+        self._h = h
+        self.n = n
+        self.starting_pots = np.array([t.starting_pot for t in tree_configs], np.float32)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            N.lib().ps_batch_free(h)
+            self._h = None
+
+    def solve(self, max_num_iterations: int, target_exploitability) -> None:
+        t = np.ascontiguousarray(np.broadcast_to(np.asarray(target_exploitability, np.float32), (self.n,)))
+        N.check(N.lib().ps_batch_solve(self._h, max_num_iterations, _fp(t)))
+
+    def results(self):
+        e = _f32(self.n)
+        it = np.zeros(self.n, np.int32)
+        N.check(N.lib().ps_batch_results(self._h, _fp(e), it.ctypes.data_as(C.POINTER(C.c_int32))))
+        return e, it
+
+    def root_strategy(self, spot: int) -> np.ndarray:
+        out = _f32(200000)
+        n = N.check(N.lib().ps_batch_root_strategy(self._h, spot, _fp(out)))
+        return out[:n].copy()
+
+    def last_timing(self):
+        a, b = C.c_float(), C.c_float()
+        N.check(N.lib().ps_batch_last_timing(self._h, C.byref(a), C.byref(b)))
+        return float(a.value), float(b.value)
+
+    def iteration_bytes(self, spot: int) -> float:
+        return float(N.lib().ps_batch_iteration_bytes(self._h, spot))
+
+    def io_bytes(self):
+        a, b = C.c_uint64(), C.c_uint64()
+        N.check(N.lib().ps_batch_io_bytes(self._h, C.byref(a), C.byref(b)))
+        return int(a.value), int(b.value)
+
+    def config(self):
+        a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
+        N.check(N.lib().ps_batch_config(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return {"block_threads": a.value, "grid": b.value, "ctas_per_sm": c.value}

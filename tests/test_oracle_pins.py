@@ -1,0 +1,159 @@
+"""The oracle (CPU restatement of crates/range-solver) against the reference's
+own known answers and golden values (tests/golden/reference_pins.json)."""
+
+import hashlib
+import os
+import struct
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests import spots
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_hand_table_digest(pins):
+    t = O.hand_table()
+    p = pins["hand_table"]
+    assert len(t) == p["len"] == 4824
+    raw = b"".join(struct.pack("<i", int(v)) for v in t)
+    assert hashlib.sha256(raw).hexdigest() == p["sha256_le_i32"]
+    assert list(t[:5]) == p["first"] and list(t[-3:]) == p["last"]
+
+
+def test_hand_category_counts(pins):
+    # written by the oracle build from the exhaustive C(52,7) enumeration
+    with open(os.path.join(ROOT, "oracle", "_build", "hand_counts.txt")) as f:
+        vals = [int(x) for x in f.read().split()]
+    assert vals[0] == 4824
+    assert vals[1:] == pins["hand_category_counts"]["counts"]
+
+
+def test_hand_ordering_known_answers():
+    # hand.rs:168-385 style orderings: royal flush > quads > full house > ... > high card
+    def c(r, s):
+        return 4 * r + s
+    royal = [c(12, 0), c(11, 0), c(10, 0), c(9, 0), c(8, 0), c(0, 1), c(1, 2)]
+    quads = [c(5, 0), c(5, 1), c(5, 2), c(5, 3), c(12, 0), c(0, 1), c(1, 2)]
+    boat = [c(5, 0), c(5, 1), c(5, 2), c(7, 3), c(7, 0), c(0, 1), c(1, 2)]
+    wheel = [c(12, 0), c(0, 1), c(1, 2), c(2, 3), c(3, 0), c(8, 1), c(9, 2)]
+    six_high = [c(4, 0), c(0, 1), c(1, 2), c(2, 3), c(3, 0), c(8, 1), c(9, 3)]
+    high = [c(12, 0), c(10, 1), c(8, 2), c(6, 3), c(4, 0), c(2, 1), c(0, 2)]
+    v = [O.hand_evaluate(x) for x in (royal, quads, boat, six_high, wheel, high)]
+    assert v == sorted(v, reverse=True) and len(set(v)) == 6
+
+
+def test_discount_params(pins):
+    p = pins["discount_params"]
+    a, b, g = O.discount_params(0)
+    assert (a, b, g) == (p["t0"]["alpha"], p["t0"]["beta"], p["t0"]["gamma"])
+    a, b, _ = O.discount_params(1)
+    assert (a, b) == (p["t1"]["alpha"], p["t1"]["beta"])
+    assert O.discount_params(4)[2] == p["t4_gamma"]
+    assert abs(O.discount_params(5)[2] - p["t5_gamma"]) < 1e-6
+    assert O.discount_params(100)[0] > p["t100_alpha_gt"]
+
+
+def _expected(kind, args):
+    f = [float(x.replace("f64::INFINITY", "inf")) for x in args] if args else []
+    if kind in ("PotRelative", "PrevBetRelative"):
+        return (kind, f[0], 0, 0)
+    if kind == "Additive":
+        return (kind, 0.0, int(f[0]), int(f[1]))
+    if kind == "Geometric":
+        return (kind, f[1], int(f[0]), 0)
+    return (kind, 0.0, 0, 0)
+
+
+def test_bet_size_parser(pins):
+    for s, kind, args in pins["bet_size_from_str"]["ok"]:
+        got = O.parse_bet_sizes(s, True)
+        assert got == [_expected(kind, args)], s
+    for s in pins["bet_size_from_str"]["errors"]:
+        if s == "":
+            continue  # an empty list is valid for the list parser
+        with pytest.raises(ValueError):
+            O.parse_bet_sizes(s, True)
+
+
+def _basic_config(pins):
+    import poker_solver_rust_b200 as ps
+    from poker_solver_rust_b200 import BetSizeOptions as B, BoardState, TreeConfig
+
+    e = pins["basic_example"]
+    r0 = ps.Range.from_str(e["oop_range"]).raw_data()
+    r1 = ps.Range.from_str(e["ip_range"]).raw_data()
+    board = ps.flop_from_str(e["flop"]) + [ps.card_from_str(e["turn"])]
+    sz = B(*e["bet_sizes"])
+    tc = TreeConfig(initial_state=BoardState.Turn, starting_pot=e["starting_pot"],
+                    effective_stack=e["effective_stack"], flop_bet_sizes=[sz, sz], turn_bet_sizes=[sz, sz],
+                    river_bet_sizes=[sz, sz], river_donk_sizes=e["river_donk"],
+                    add_allin_threshold=e["add_allin_threshold"],
+                    force_allin_threshold=e["force_allin_threshold"], merging_threshold=e["merging_threshold"])
+    return [r0, r1], board, tc
+
+
+def _fmt(actions):
+    return "[" + ", ".join(k if k in ("Fold", "Check", "Call") else f"{k}({a})" for k, a in actions) + "]"
+
+
+def test_basic_example_oracle(pins):
+    import poker_solver_rust_b200 as ps
+
+    e = pins["basic_example"]
+    r, board, tc = _basic_config(pins)
+    g = spots.oracle_game(r, board, tc, allocate=False)
+    assert ps.holes_to_strings(g.private_cards(0))[:10] == e["oop_first10"]
+    assert g.num_private_hands(1) == e["ip_hands"]
+    assert _fmt(g.available_actions()) == e["root_actions"]
+    # navigate to the node after Bet(120) through the arena
+    info = g.node_info(0)
+    child = info["children_offset"] + 1
+    ci = g.node_info(child)
+    kids = [g.node_info(child + ci["children_offset"] + k) for k in range(ci["num_children"])]
+    acts = [(O.ACTION_NAMES[k["prev_kind"]], k["prev_amount"]) for k in kids]
+    assert _fmt(acts) == e["after_bet_actions"]
+
+
+def test_oracle_solves_reference_fixture():
+    # solver.rs:772-806: AA,KK,QQ,AKs vs QQ-JJ,AQs,AJs on Qs Jh 2c 8d 3s,
+    # pot 100 / stack 100, "50%, a"; exploitability < 10 after 100 iterations
+    import poker_solver_rust_b200 as ps
+    from poker_solver_rust_b200 import BetSizeOptions as B, BoardState, TreeConfig
+
+    r = [ps.Range.from_str("AA,KK,QQ,AKs").raw_data(), ps.Range.from_str("QQ-JJ,AQs,AJs").raw_data()]
+    board = ps.flop_from_str("Qs Jh 2c") + [ps.card_from_str("8d"), ps.card_from_str("3s")]
+    s = B("50%, a", "")
+    tc = TreeConfig(initial_state=BoardState.River, starting_pot=100, effective_stack=100, river_bet_sizes=[s, s])
+    g = spots.oracle_game(r, board, tc)
+    e = g.solve(100, 0.0)
+    assert 0.0 <= e < 10.0
+
+
+def test_oracle_fp32_tracks_fp64():
+    r, board, tc = spots.river_spot(11)
+    g32 = spots.oracle_game(r, board, tc)
+    g64 = spots.oracle_game(r, board, tc, fp64=True)
+    for t in range(50):
+        g32.solve_step(t)
+        g64.solve_step(t)
+    e32, e64 = g32.compute_exploitability(), g64.compute_exploitability()
+    assert abs(e32 - e64) <= 1e-3 * max(1.0, abs(e64))
+
+
+def test_oracle_evaluation_properties():
+    # evaluation.rs:706-885: fold values signed by who folded; zero reach -> zero values
+    r, board, tc = spots.river_spot(3)
+    g = spots.oracle_game(r, board, tc)
+    n = g.num_nodes()
+    for idx in range(n):
+        info = g.node_info(idx)
+        if info["player"] & 24 == 24:  # fold terminal
+            folded = info["player"] & 3
+            for p in range(2):
+                v = g.evaluate_node(idx, p, np.ones(g.num_private_hands(p ^ 1), np.float32))
+                assert (v >= 0).all() if folded != p else (v <= 0).all()
+                z = g.evaluate_node(idx, p, np.zeros(g.num_private_hands(p ^ 1), np.float32))
+                assert (z == 0).all()
