@@ -169,6 +169,7 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=32)
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
+    ap.add_argument("--e2e-steps", type=int, default=3)
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -241,7 +242,7 @@ def main():
     # ---- end to end through the public API (host buffers) ----
     e2e_ms = []
     h2d = d2h = 0
-    for k in range(max(1, min(args.steps, 3))):
+    for k in range(min(args.steps, args.e2e_steps)):
         barrier()
         t0 = time.perf_counter()
         b2 = ps.BatchSolver(cc, tcs, block_threads=args.block, ctas_per_sm=args.ctas_per_sm)
@@ -251,8 +252,8 @@ def main():
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
         h2d, d2h = b2.io_bytes()
         del b2
-    e2e_step = max_over_ranks(statistics.median(e2e_ms))
-    e2e_value = world * args.spots / (e2e_step / 1e3)
+    e2e_step = max_over_ranks(statistics.median(e2e_ms)) if e2e_ms else float("nan")
+    e2e_value = world * args.spots / (e2e_step / 1e3) if e2e_ms else None
 
     # ---- plain per-instance GPU path on a sample (one game, one launch per spot) ----
     plain = None

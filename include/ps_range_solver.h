@@ -95,6 +95,9 @@ int ps_strategy_at_index(ps_game* g, int64_t node, float* out);     /* query.rs:
 /* raw per-node storage: 1 cumulative strategy, 2 regrets (cfvalues after finalize),
  * 3 IP cfvalues, 4 chance cfvalues; returns the element count */
 int64_t ps_node_storage(ps_game* g, int64_t node, int which, float* out);
+/* writes one node's storage (which = 1 cumulative strategy, 2 regrets), rows of
+ * H_actor values per action - the general form of seed_strategy (query.rs:438-469) */
+int ps_seed_node_storage(ps_game* g, int64_t node, int which, const float* values, int64_t n);
 int ps_same_hand_index(ps_game* g, int player, uint16_t* out);      /* game/mod.rs:288 */
 /* hand strength order for board (turn, river) as computed on the device:
  * ascending (strength, index) items incl. the (0,0) / (65535,65535) sentinels

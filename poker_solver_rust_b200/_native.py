@@ -89,6 +89,7 @@ _sig("ps_node_info", i32, vp, i64, P(i32))
 _sig("ps_child_indices", i32, vp, i64, P(i64), i32)
 _sig("ps_strategy_at_index", i32, vp, i64, P(f32))
 _sig("ps_node_storage", i64, vp, i64, i32, P(f32))
+_sig("ps_seed_node_storage", i32, vp, i64, i32, P(f32), i64)
 _sig("ps_same_hand_index", i32, vp, i32, P(C.c_uint16))
 _sig("ps_hand_strength", i32, vp, i32, i32, i32, P(C.c_uint16), P(C.c_uint16))
 _sig("ps_valid_indices", i32, vp, i32, i32, i32, P(C.c_uint16))

@@ -766,6 +766,25 @@ int64_t ps_node_storage(ps_game* G, int64_t idx, int which, float* out) {
   return (int64_t)n.nch * H;
 }
 
+int ps_seed_node_storage(ps_game* G, int64_t idx, int which, const float* v, int64_t n) {
+  if (!G || !v || idx < 0 || idx >= (int64_t)G->g->arena.size() || (which != 1 && which != 2))
+    return fail(PS_ERR_INVALID, "bad argument");
+  if (G->state != GState::MemoryAllocated) return fail(PS_ERR_STATE, "Game is not ready");
+  Game& g = *G->g;
+  const ArenaNode& nd = g.arena[idx];
+  if (nd.terminal() || nd.chance()) return fail(PS_ERR_INVALID, "seed requires a decision node");
+  int p = nd.player, H = g.H[p], hs = g.hs[p];
+  if (n != (int64_t)nd.nch * H) return fail(PS_ERR_INVALID, "expected num_actions * num_hands values");
+  std::vector<float> rows((size_t)nd.nch * hs, 0.f);
+  for (int a = 0; a < nd.nch; ++a)
+    for (int h = 0; h < H; ++h) rows[(size_t)a * hs + h] = v[(size_t)a * H + h];
+  const SpotDev& s = G->b->h_spots[0];
+  float* dst = (which == 1 ? s.S : s.R) + nd.rs_off;
+  CU(cudaMemcpy(dst, rows.data(), 4 * rows.size(), cudaMemcpyHostToDevice));
+  G->host_dirty = true;
+  return PS_OK;
+}
+
 int ps_same_hand_index(ps_game* G, int p, uint16_t* out) {
   if (!G || !out) return fail(PS_ERR_INVALID, "null argument");
   std::copy(G->g->same[p & 1].begin(), G->g->same[p & 1].end(), out);

@@ -236,6 +236,11 @@ class PostFlopGame:
         n = N.check(N.lib().ps_node_storage(self._h, idx, which, _fp(out)))
         return out[:n].copy()
 
+    def seed_node_storage(self, idx: int, which: int, values) -> None:
+        """Writes a decision node's cumulative strategy (1) or regrets (2)."""
+        v = np.ascontiguousarray(values, np.float32)
+        N.check(N.lib().ps_seed_node_storage(self._h, idx, which, _fp(v), len(v)))
+
     # ---- depth boundary ----
     def num_boundary_nodes(self) -> int:
         return int(N.lib().ps_num_boundary_nodes(self._h))
