@@ -87,6 +87,8 @@ def lib():
                 "orc_solve": (f32, [vp, u32, f32, i32, P(u32)]),
                 "orc_solve_step": (i32, [vp, u32]),
                 "orc_exploitability": (f32, [vp]),
+                "orc_solve_pass": (i32, [vp, u32, i32]),
+                "orc_seed_node_storage": (i32, [vp, i64, i32, P(f32), i64]),
                 "orc_mes_ev": (i32, [vp, P(f32)]),
                 "orc_current_ev": (i32, [vp, P(f32)]),
                 "orc_finalize": (i32, [vp]),
@@ -298,6 +300,13 @@ class OracleGame:
 
     def solve_step(self, t):
         self._check(lib().orc_solve_step(self.h, t))
+
+    def solve_pass(self, t, player):
+        self._check(lib().orc_solve_pass(self.h, t, player))
+
+    def seed_node_storage(self, idx, which, values):
+        v = np.ascontiguousarray(values, np.float32)
+        self._check(lib().orc_seed_node_storage(self.h, idx, which, _p(v, C.c_float), len(v)))
 
     def compute_exploitability(self):
         return float(lib().orc_exploitability(self.h))

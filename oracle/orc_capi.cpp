@@ -292,6 +292,21 @@ int orc_solve_step(void* p, uint32_t t) {
   ORC_TRY(return with((OrcGame*)p, [&](auto& g) { g.solve_step(t); return 0; });)
 }
 
+int orc_solve_pass(void* p, uint32_t t, int player) {
+  ORC_TRY(return with((OrcGame*)p, [&](auto& g) { g.solve_pass(t, player); return 0; });)
+}
+
+// Overwrites one decision node's storage (1 strategy sums, 2 regrets) from float32 rows.
+int orc_seed_node_storage(void* p, int64_t idx, int which, const float* v, int64_t n) {
+  return with((OrcGame*)p, [&](auto& g) {
+    const Node& nd = g.arena[idx];
+    if (nd.is_terminal() || nd.is_chance() || (int64_t)nd.num_elements != n) return -1;
+    auto& st = which == 1 ? g.storage1 : g.storage2;
+    for (int64_t i = 0; i < n; ++i) st[nd.s1 + i] = v[i];
+    return 0;
+  });
+}
+
 float orc_exploitability(void* p) {
   try {
     return with((OrcGame*)p, [](auto& g) { return g.compute_exploitability(); });

@@ -1475,6 +1475,15 @@ void Game<F>::solve_step(uint32_t t) {
   }
 }
 
+// one player's traversal of solve_step (solver.rs:197-208), for per-pass checks
+template <class F>
+void Game<F>::solve_pass(uint32_t t, int p) {
+  if (!is_ready()) throw std::runtime_error("Game is not ready");
+  DiscountParams params(t);
+  std::vector<F> result(num_private_hands(p));
+  solve_recursive(result.data(), &arena[0], p, initial_weights[p ^ 1].data(), params);
+}
+
 // solver.rs:108-176
 template <class F>
 float Game<F>::solve(uint32_t max_iter, float target, bool print, uint32_t* iters_run) {

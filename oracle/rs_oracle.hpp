@@ -226,6 +226,7 @@ struct Game {
   // -------- solver (solver.rs, utility.rs) --------
   void solve_recursive(F* result, Node* node, int player, const F* cfreach, const DiscountParams& p);
   void solve_step(uint32_t t);
+  void solve_pass(uint32_t t, int player);  // one traverser pass of solve_step
   float solve(uint32_t max_iter, float target, bool print, uint32_t* iters_run = nullptr);
   void compute_cfvalue_recursive(F* result, Node* node, int player, const F* cfreach, bool save);
   void compute_best_cfv_recursive(F* result, Node* node, int player, const F* cfreach);

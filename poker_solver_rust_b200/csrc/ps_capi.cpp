@@ -135,7 +135,7 @@ struct Batch {
   int* d_order = nullptr;
   int block = 256, grid = 1, ctas_per_sm = 0;
   int max_vstride = 32;
-  size_t smem = 0;
+  SmemPlan plan{};
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   float last_solve_ms = 0, last_setup_ms = 0;
   std::vector<float> h_expl;
@@ -306,10 +306,22 @@ struct Batch {
     CU(cudaMalloc(&d_counter, sizeof(int)));
     CU(cudaMalloc(&d_err, sizeof(int)));
     CU(cudaMalloc(&d_order, sizeof(int) * n));
-    // launch configuration
-    block = opts && opts->block_threads > 0 ? opts->block_threads : 256;
-    smem = solve_smem(max_vstride);
-    int occ = solve_occupancy(block, smem);
+    // launch configuration: a block covers the largest hand vector four hands
+    // per thread; terminals per batch and staged tables sized to the spots
+    int hs_max = 4;
+    bool single_board = true;
+    for (auto& gp : games) {
+      hs_max = std::max(hs_max, std::max(gp->hs[0], gp->hs[1]));
+      single_board &= gp->boards.size() == 1;
+    }
+    block = opts && opts->block_threads > 0 ? opts->block_threads
+                                            : std::min(256, std::max(128, ((hs_max / 4 + 31) / 32) * 32));
+    block = std::min(block, 256);
+    plan.vstride = max_vstride;
+    plan.hs_max = hs_max;
+    plan.kt = 2;
+    plan.tables = single_board ? table_bytes_for(hs_max, hs_max) : 0;
+    int occ = solve_occupancy(block, plan);
     ctas_per_sm = opts && opts->ctas_per_sm > 0 ? std::min(opts->ctas_per_sm, occ) : occ;
     grid = std::max(1, std::min(n, dc->nsm * ctas_per_sm));
     for (auto& gp : games) scratch_floats = std::max(scratch_floats, (size_t)gp->num_slots * gp->vstride);
@@ -382,7 +394,7 @@ struct Batch {
     if (!fresh) CU(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
     CU(cudaEventRecord(ev[2], stream));
     CU(launch_solve(d_spots, n, d_order, d_counter, d_disc, (int)max_iter, d_target, d_scratch, scratch_floats,
-                    d_expl, d_iters, d_err, grid, block, smem, stream));
+                    d_expl, d_iters, d_err, grid, block, plan, stream));
     CU(cudaEventRecord(ev[3], stream));
     h_expl.resize(n);
     h_iters.resize(n);
@@ -456,7 +468,7 @@ float expl_run(ps_game* G, int* rc) {
   float e = 0;
   cudaError_t ce = cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream);
   if (ce == cudaSuccess)
-    ce = launch_exploitability(B.d_spots, 1, B.d_scratch, B.scratch_floats, B.d_expl, B.d_err, 1, B.block, B.smem,
+    ce = launch_exploitability(B.d_spots, 1, B.d_scratch, B.scratch_floats, B.d_expl, B.d_err, 1, B.block, B.plan,
                                B.stream);
   if (ce == cudaSuccess) ce = cudaMemcpyAsync(&e, B.d_expl, 4, cudaMemcpyDeviceToHost, B.stream);
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(B.stream);
@@ -626,7 +638,7 @@ int ps_solve_step(ps_game* G, uint32_t t) {
   if ((rc = B.ensure_disc(t + 1))) return rc;
   CU(cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream));
   CU(launch_iterate(B.d_spots, 1, B.d_disc, (int)t, (int)t + 1, B.d_scratch, B.scratch_floats, B.d_err, 1, B.block,
-                    B.smem, B.stream));
+                    B.plan, B.stream));
   G->host_dirty = true;
   return B.check_err();
 }
@@ -649,7 +661,7 @@ int ps_finalize(ps_game* G) {
   Batch& B = *G->b;
   CU(cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream));
   CU(launch_average(B.d_spots, 1, 1, 0, nullptr, B.d_scratch, B.scratch_floats, nullptr, B.d_err, 1, B.block,
-                    B.smem, B.stream));
+                    B.plan, B.stream));
   if ((rc = B.check_err())) return rc;
   G->state = GState::Solved;
   G->host_dirty = true;
@@ -677,7 +689,7 @@ int ps_root_cfvalues_with_reach(ps_game* G, int player, const float* opp_reach, 
   CU(cudaMemcpyAsync(d_reach, r.data(), 4 * r.size(), cudaMemcpyHostToDevice, B.stream));
   CU(cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream));
   CU(launch_average(B.d_spots, 1, 0, player, d_reach, B.d_scratch, B.scratch_floats, d_out, B.d_err, 1, B.block,
-                    B.smem, B.stream));
+                    B.plan, B.stream));
   CU(cudaMemcpyAsync(out, d_out, 4 * (size_t)g.H[player], cudaMemcpyDeviceToHost, B.stream));
   CU(cudaStreamSynchronize(B.stream));
   cudaFree(d_reach);
@@ -840,7 +852,7 @@ int ps_valid_indices(ps_game* G, int turn, int river, int p, uint16_t* out) {
   CU(cudaMemcpy(thr.data(), s.thr[p] + (size_t)b * g.hs[p] * kThrWords, 2 * thr.size(), cudaMemcpyDeviceToHost));
   int n = 0;
   for (int h = 0; h < g.H[p]; ++h)
-    if (thr[(size_t)h * kThrWords + 6]) out[n++] = (uint16_t)h;
+    if (thr[(size_t)h * kThrWords] != 0xFFFF || thr[(size_t)h * kThrWords + 1] != 0xFFFF) out[n++] = (uint16_t)h;
   return n;
 }
 
@@ -1097,7 +1109,7 @@ int ps_expected_values(ps_game* G, int player, int detail, float* out) {  // que
     op.fold_pl = n.player & PL_MASK;
     if (n.boundary() && (rc = need_boundaries(G))) return rc;
     CU(cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream));
-    CU(launch_eval_terminal(B.d_spots, op, player, B.d_scratch, B.scratch_floats, B.d_err, B.block, B.smem, B.stream));
+    CU(launch_eval_terminal(B.d_spots, op, player, B.d_scratch, B.scratch_floats, B.d_err, B.block, B.plan, B.stream));
     ret.resize(H);
     CU(cudaMemcpyAsync(ret.data(), B.d_scratch + g.vstride, 4 * (size_t)H, cudaMemcpyDeviceToHost, B.stream));
     CU(cudaStreamSynchronize(B.stream));

@@ -3,22 +3,27 @@
 // Work decomposition: one CTA owns one game ("spot") at a time and walks its
 // level-ordered tree program (ps_device.hpp): forward steps propagate the
 // opponent's reach top-down, backward steps evaluate terminals and combine
-// children bottom-up with the DCFR regret / strategy update fused in.  Every
-// hand vector is processed by all threads of the CTA (one hand per thread per
-// sweep of the loop); steps are separated by __syncthreads only, so a whole
-// solve of a spot - all iterations plus the exploitability checks - runs
-// inside one persistent launch that pulls spots from a device work queue.
+// children bottom-up with the DCFR regret / strategy update fused in.  A hand
+// vector is split across the CTA four hands per thread (128-bit loads and
+// stores of regrets, strategy sums and the per-node reach / value vectors);
+// steps are separated by __syncthreads only, so a whole solve of a spot - all
+// iterations plus the exploitability checks - runs inside one persistent
+// launch that pulls spots from a device work queue.  Several CTAs share an SM
+// so that one CTA's memory latency overlaps another's work.
 //
 // Terminal evaluation restates crates/range-solver/src/game/evaluation.rs
 // without its sequential merge: the opponent reach is gathered into
 // hand-strength order and into per-card groups (both precomputed per board by
-// k_setup), scanned with warp shuffles, and every hand reads its win / lose /
-// blocked sums at precomputed thresholds - O(n) work per terminal.
+// k_setup and staged in shared memory for single-board spots), scanned with
+// warp shuffles, and every hand reads its win / lose / blocked sums at
+// precomputed thresholds - O(n) work per terminal.  Terminals of a step are
+// evaluated in batches so that a batch shares its barriers.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "ps_device.hpp"
 #include "ps_handeval.hpp"
+#include "ps_launch.hpp"
 
 namespace ps {
 
@@ -28,15 +33,26 @@ enum Mode { M_DCFR = 0, M_BR = 1, M_AVG = 2, M_AVG_SAVE = 3 };
 constexpr int ERR_SCRATCH = 1;  // a spot needed more scratch than its CTA owns
 constexpr int ERR_SETUP = 2;    // setup tables exceeded their bounds
 
+constexpr uint32_t THR_INVALID = 0xFFFFFFFFu;
+
+struct Tables {  // board tables of one board, in shared or global memory
+  const uint16_t* gidx[2];
+  const uint16_t* coff[2];
+  const uint2* thr[2];
+  int nvalid[2];
+};
+
 struct Ctx {
   const SpotDev* sp;
   float* slots;
   int vstride;
+  int kt;
   const float* root_reach;
-  float* rch;    // smem: staged opponent reach  [vstride]
-  float* buf;    // smem: scan results           [3 * vstride]
-  float* carry;  // smem: per-warp chunk totals  [32]
+  float* rch;    // smem: staged opponent reach  [kt][vstride]
+  float* buf;    // smem: scan results           [kt][3 * vstride]
+  float* carry;  // smem: per-warp chunk totals  [kt][32]
   double* red;   // smem: reduction scratch      [32]
+  Tables t0;     // board-0 tables (shared memory when staged, else global)
 };
 
 __device__ __forceinline__ const float* slot_in(const Ctx& c, uint16_t id) {
@@ -48,6 +64,30 @@ __device__ __forceinline__ float* slot_at(const Ctx& c, uint16_t id) {
 
 // max(x, y) of the reference (sliceop.rs:5-12): no NaN propagation.
 __device__ __forceinline__ float fmax_ref(float x, float y) { return x > y ? x : y; }
+
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+
+__device__ __forceinline__ float4 max0(float4 a) {
+  return make_float4(fmax_ref(a.x, 0.f), fmax_ref(a.y, 0.f), fmax_ref(a.z, 0.f), fmax_ref(a.w, 0.f));
+}
+__device__ __forceinline__ float4 add4(float4 a, float4 b) {
+  return make_float4(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z), __fadd_rn(a.w, b.w));
+}
+__device__ __forceinline__ float4 mul4(float4 a, float4 b) {
+  return make_float4(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y), __fmul_rn(a.z, b.z), __fmul_rn(a.w, b.w));
+}
+__device__ __forceinline__ float div_def(float m, float d, float def) { return d == 0.0f ? def : __fdiv_rn(m, d); }
+__device__ __forceinline__ float4 sigma4(float4 m, float4 d, float def) {
+  return make_float4(div_def(m.x, d.x, def), div_def(m.y, d.y, def), div_def(m.z, d.z, def), div_def(m.w, d.w, def));
+}
+__device__ __forceinline__ float4 max4(float4 a, float4 b) {
+  return make_float4(fmax_ref(a.x, b.x), fmax_ref(a.y, b.y), fmax_ref(a.z, b.z), fmax_ref(a.w, b.w));
+}
+// DCFR regret update of one element (solver.rs:570-589): R * (R >= +0 ? alpha : beta) + cfv - result
+__device__ __forceinline__ float regret_upd(float r, float cv, float res, float alpha, float beta) {
+  return __fsub_rn(__fadd_rn(__fmul_rn(r, signbit(r) ? beta : alpha), cv), res);
+}
 
 __device__ __forceinline__ float warp_incl_scan(float x, int lane) {
 #pragma unroll
@@ -64,41 +104,42 @@ __device__ __forceinline__ float warp_incl_scan(float x, int lane) {
 
 // Opponent decision node (solver.rs:418-445; utility.rs:227-250 for BR / AVG):
 // sigma from regret matching (DCFR) or from the normalised cumulative strategy,
-// then children's reach = sigma_a * reach.
+// then children's reach = sigma_a * reach.  Two sweeps over the actions: the
+// first forms the denominator, the second (L1 hits) the children.
 template <int MODE>
 __device__ void op_fwd_opp(const Ctx& c, const Op& op, int o) {
   const SpotDev& sp = *c.sp;
-  const int hso = sp.hs[o], na = op.na;
+  const int hso = sp.hs[o], na = op.na, q4 = hso >> 2;
   const float* base = (MODE == M_DCFR ? sp.R : sp.S) + sp.nodes[op.node].rs_off;
   const float* src = slot_in(c, op.src);
   float* dst = slot_at(c, op.blk);
   const float def = 1.0f / (float)na;
-  for (int h = threadIdx.x; h < hso; h += blockDim.x) {
-    float v[kMaxActions];
-    float d = 0.f;
-#pragma unroll
-    for (int a = 0; a < kMaxActions; ++a) {
-      if (a < na) {
-        float x = base[a * hso + h];
-        v[a] = MODE == M_DCFR ? fmax_ref(x, 0.0f) : x;
-        d = a == 0 ? v[a] : __fadd_rn(d, v[a]);
-      }
+  for (int q = threadIdx.x; q < q4; q += blockDim.x) {
+    const int h = q << 2;
+    float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int a = 0; a < na; ++a) {
+      float4 x = ld4(base + a * hso + h);
+      if (MODE == M_DCFR) x = max0(x);
+      d = a == 0 ? x : add4(d, x);
     }
-    const float r = src[h];
-#pragma unroll
-    for (int a = 0; a < kMaxActions; ++a)
-      if (a < na) dst[(size_t)a * c.vstride + h] = __fmul_rn(d == 0.0f ? def : __fdiv_rn(v[a], d), r);
+    const float4 r = ld4(src + h);
+    for (int a = 0; a < na; ++a) {
+      float4 x = ld4(base + a * hso + h);
+      if (MODE == M_DCFR) x = max0(x);
+      st4(dst + (size_t)a * c.vstride + h, mul4(sigma4(x, d, def), r));
+    }
   }
 }
 
 // Chance node (solver.rs:264-276): one scaled reach shared by all children.
 __device__ void op_fwd_chance(const Ctx& c, const Op& op, int o) {
   const SpotDev& sp = *c.sp;
-  const int hso = sp.hs[o];
+  const int q4 = sp.hs[o] >> 2;
   const float f = __fdiv_rn(1.0f, (float)sp.nodes[op.node].chance_factor);
+  const float4 f4 = make_float4(f, f, f, f);
   const float* src = slot_in(c, op.src);
   float* dst = slot_at(c, op.blk);
-  for (int h = threadIdx.x; h < hso; h += blockDim.x) dst[h] = __fmul_rn(src[h], f);
+  for (int q = threadIdx.x; q < q4; q += blockDim.x) st4(dst + (q << 2), mul4(ld4(src + (q << 2)), f4));
 }
 
 // ---------------------------------------------------------------------------
@@ -110,75 +151,63 @@ __device__ void op_fwd_chance(const Ctx& c, const Op& op, int o) {
 //        S = S * gamma + sigma; R = R * (R >= +0 ? alpha : beta) + cfv_a - cfv.
 //   BR   (utility.rs:953-966): cfv = max_a cfv_a.
 //   AVG  (utility.rs:689-727): sigma = S / sum S; cfv = sum sigma_a cfv_a; SAVE stores cfv_a.
+// Three sweeps over the actions (denominator, result + S, regrets) keep the
+// per-thread state to a few float4 registers; repeated loads hit L1.
 template <int MODE>
 __device__ void op_bwd_trav(const Ctx& c, const Op& op, int p, const Discount dc) {
   const SpotDev& sp = *c.sp;
-  const int hsp = sp.hs[p], na = op.na;
-  const NodeDev nd = sp.nodes[op.node];
+  const int hsp = sp.hs[p], na = op.na, q4 = hsp >> 2;
+  const NodeDev& nd = sp.nodes[op.node];
   float* R = sp.R + nd.rs_off;
   float* S = sp.S + nd.rs_off;
   const float* cb = slot_at(c, op.blk);
   float* dst = slot_at(c, op.dst);
   const float def = 1.0f / (float)na;
-  for (int h = threadIdx.x; h < hsp; h += blockDim.x) {
-    float cv[kMaxActions];
-#pragma unroll
-    for (int a = 0; a < kMaxActions; ++a)
-      if (a < na) cv[a] = cb[(size_t)a * c.vstride + h];
-    float res = 0.f;
+  for (int q = threadIdx.x; q < q4; q += blockDim.x) {
+    const int h = q << 2;
+    float4 res = make_float4(0.f, 0.f, 0.f, 0.f);
     if (MODE == M_BR) {
-      res = cv[0];
-#pragma unroll
-      for (int a = 1; a < kMaxActions; ++a)
-        if (a < na) res = fmax_ref(res, cv[a]);
-    } else if (MODE == M_DCFR) {
-      float r[kMaxActions], m[kMaxActions];
-      float d = 0.f;
-#pragma unroll
-      for (int a = 0; a < kMaxActions; ++a) {
-        if (a < na) {
-          r[a] = R[a * hsp + h];
-          m[a] = fmax_ref(r[a], 0.0f);
-          d = a == 0 ? m[a] : __fadd_rn(d, m[a]);
-        }
-      }
-#pragma unroll
-      for (int a = 0; a < kMaxActions; ++a) {
-        if (a < na) {
-          m[a] = d == 0.0f ? def : __fdiv_rn(m[a], d);
-          float t = __fmul_rn(m[a], cv[a]);
-          res = a == 0 ? t : __fadd_rn(res, t);
-          S[a * hsp + h] = __fadd_rn(__fmul_rn(S[a * hsp + h], dc.gamma), m[a]);
-        }
-      }
-#pragma unroll
-      for (int a = 0; a < kMaxActions; ++a) {
-        if (a < na) {
-          float coef = signbit(r[a]) ? dc.beta : dc.alpha;
-          R[a * hsp + h] = __fsub_rn(__fadd_rn(__fmul_rn(r[a], coef), cv[a]), res);
-        }
-      }
+      res = ld4(cb + h);
+      for (int a = 1; a < na; ++a) res = max4(res, ld4(cb + (size_t)a * c.vstride + h));
     } else {
-      float s[kMaxActions];
-      float d = 0.f;
-#pragma unroll
-      for (int a = 0; a < kMaxActions; ++a) {
-        if (a < na) {
-          s[a] = S[a * hsp + h];
-          d = a == 0 ? s[a] : __fadd_rn(d, s[a]);
+      const float* W = MODE == M_DCFR ? R : S;
+      float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int a = 0; a < na; ++a) {
+        float4 x = ld4(W + a * hsp + h);
+        if (MODE == M_DCFR) x = max0(x);
+        d = a == 0 ? x : add4(d, x);
+      }
+      for (int a = 0; a < na; ++a) {
+        float4 x = ld4(W + a * hsp + h);
+        if (MODE == M_DCFR) x = max0(x);
+        const float4 s = sigma4(x, d, def);
+        const float4 cv = ld4(cb + (size_t)a * c.vstride + h);
+        const float4 t = mul4(s, cv);
+        res = a == 0 ? t : add4(res, t);
+        if (MODE == M_DCFR) {
+          const float4 g = make_float4(dc.gamma, dc.gamma, dc.gamma, dc.gamma);
+          st4(S + a * hsp + h, add4(mul4(ld4(S + a * hsp + h), g), s));
+        } else if (MODE == M_AVG_SAVE) {
+          st4(R + a * hsp + h, cv);
         }
       }
-#pragma unroll
-      for (int a = 0; a < kMaxActions; ++a) {
-        if (a < na) {
-          float t = __fmul_rn(d == 0.0f ? def : __fdiv_rn(s[a], d), cv[a]);
-          res = a == 0 ? t : __fadd_rn(res, t);
-          if (MODE == M_AVG_SAVE) R[a * hsp + h] = cv[a];
+      if (MODE == M_DCFR) {
+        for (int a = 0; a < na; ++a) {
+          const float4 r = ld4(R + a * hsp + h);
+          const float4 cv = ld4(cb + (size_t)a * c.vstride + h);
+          st4(R + a * hsp + h, make_float4(regret_upd(r.x, cv.x, res.x, dc.alpha, dc.beta),
+                                           regret_upd(r.y, cv.y, res.y, dc.alpha, dc.beta),
+                                           regret_upd(r.z, cv.z, res.z, dc.alpha, dc.beta),
+                                           regret_upd(r.w, cv.w, res.w, dc.alpha, dc.beta)));
         }
       }
     }
-    dst[h] = res;
-    if (MODE == M_AVG_SAVE && p == 1 && nd.ip_off != 0xFFFFFFFFu && h < sp.H[1]) sp.ipcfv[nd.ip_off + h] = res;
+    st4(dst + h, res);
+    if (MODE == M_AVG_SAVE && p == 1 && nd.ip_off != 0xFFFFFFFFu) {
+      const float v[4] = {res.x, res.y, res.z, res.w};
+      for (int k = 0; k < 4; ++k)
+        if (h + k < sp.H[1]) sp.ipcfv[nd.ip_off + h + k] = v[k];
+    }
   }
 }
 
@@ -186,15 +215,20 @@ __device__ void op_bwd_trav(const Ctx& c, const Op& op, int p, const Discount dc
 template <int MODE>
 __device__ void op_bwd_opp(const Ctx& c, const Op& op, int p) {
   const SpotDev& sp = *c.sp;
-  const int hsp = sp.hs[p], na = op.na;
-  const NodeDev nd = sp.nodes[op.node];
+  const int q4 = sp.hs[p] >> 2, na = op.na;
+  const NodeDev& nd = sp.nodes[op.node];
   const float* cb = slot_at(c, op.blk);
   float* dst = slot_at(c, op.dst);
-  for (int h = threadIdx.x; h < hsp; h += blockDim.x) {
-    float res = cb[h];
-    for (int a = 1; a < na; ++a) res = __fadd_rn(res, cb[(size_t)a * c.vstride + h]);
-    dst[h] = res;
-    if (MODE == M_AVG_SAVE && p == 1 && nd.ip_off != 0xFFFFFFFFu && h < sp.H[1]) sp.ipcfv[nd.ip_off + h] = res;
+  for (int q = threadIdx.x; q < q4; q += blockDim.x) {
+    const int h = q << 2;
+    float4 res = ld4(cb + h);
+    for (int a = 1; a < na; ++a) res = add4(res, ld4(cb + (size_t)a * c.vstride + h));
+    st4(dst + h, res);
+    if (MODE == M_AVG_SAVE && p == 1 && nd.ip_off != 0xFFFFFFFFu) {
+      const float v[4] = {res.x, res.y, res.z, res.w};
+      for (int k = 0; k < 4; ++k)
+        if (h + k < sp.H[1]) sp.ipcfv[nd.ip_off + h + k] = v[k];
+    }
   }
 }
 
@@ -204,7 +238,7 @@ template <int MODE>
 __device__ void op_bwd_chance(const Ctx& c, const Op& op, int p) {
   const SpotDev& sp = *c.sp;
   const int hsp = sp.hs[p], na = op.na;
-  const NodeDev nd = sp.nodes[op.node];
+  const NodeDev& nd = sp.nodes[op.node];
   const float* cb = slot_at(c, op.blk);
   float* dst = slot_at(c, op.dst);
   int i0 = 0, i1 = 0;
@@ -229,38 +263,54 @@ __device__ void op_bwd_chance(const Ctx& c, const Op& op, int p) {
 // Terminal evaluation (game/evaluation.rs:57-634)
 // ---------------------------------------------------------------------------
 //
-// Per board b and opponent o the gather list holds the V valid opponent hands
-// in (strength, index) order followed by, for every card c, the valid
-// opponent hands holding c in the same order (segment [coff[c], coff[c+1])).
-// After the scans, for a hand h with thresholds
+// Per board and opponent o the gather list holds the V valid opponent hands in
+// (strength, index) order followed by, for every card c, the valid opponent
+// hands holding c in the same order (segment [coff[c], coff[c+1])).  After the
+// scans, for a hand h with thresholds
 //   lt = #opp weaker, le = #opp weaker-or-tied, ltc / lec = the same counts
 //   inside each of its two card segments,
 // the reference's sums are prefix lookups:
 //   win  = P(lt) - Q_c1(ltc1) - Q_c2(ltc2)       (strictly weaker, not blocked)
 //   lose = (T - P(le)) - (M_c1 - Q_c1(lec1)) - (M_c2 - Q_c2(lec2))
 //   fold = T + r_same - M_c1 - M_c2               (inclusion-exclusion)
-__device__ void op_term(const Ctx& c, const Op& op, int p) {
+__device__ __forceinline__ void board_tables(const Ctx& c, int b, Tables& t) {
+  if (b == 0) {
+    t = c.t0;
+    return;
+  }
+  const SpotDev& sp = *c.sp;
+  for (int q = 0; q < 2; ++q) {
+    t.gidx[q] = sp.gidx[q] + (size_t)b * 3 * sp.hs[q];
+    t.coff[q] = sp.coff[q] + (size_t)b * 56;
+    t.thr[q] = reinterpret_cast<const uint2*>(sp.thr[q]) + (size_t)b * sp.hs[q];
+    t.nvalid[q] = sp.nvalid[q][b];
+  }
+}
+
+// Evaluates ops[0..n) (n <= c.kt terminals of one step) for traverser p.
+__device__ void term_batch(const Ctx& c, const Op* ops, int n, int p) {
   const SpotDev& sp = *c.sp;
   const int o = p ^ 1;
-  const int Ho = sp.H[o], Hp = sp.H[p], hso = sp.hs[o], hsp = sp.hs[p];
-  const int b = op.board;
-  const int V = sp.nvalid[o][b];
-  const uint16_t* g = sp.gidx[o] + (size_t)b * 3 * hso;
-  const uint16_t* co = sp.coff[o] + (size_t)b * 56;
-  const float* src = slot_in(c, op.src);
-  float* dst = slot_at(c, op.dst);
-  float* rch = c.rch;
-  float* buf = c.buf;
+  const int Ho = sp.H[o], Hp = sp.H[p], hsp = sp.hs[p];
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-
-  __syncthreads();  // the previous terminal's lookups are done with rch / buf
-  for (int i = tid; i < Ho; i += nt) rch[i] = src[i];
+  __syncthreads();  // the previous batch's lookups are done with rch / buf
+  for (int j = 0; j < n; ++j) {
+    const float* src = slot_in(c, ops[j].src);
+    float* rch = c.rch + (size_t)j * c.vstride;
+    for (int q = tid; q < (Ho + 3) >> 2; q += nt) st4(rch + (q << 2), ld4(src + (q << 2)));
+  }
   __syncthreads();
-
-  const int ntile = (V + 31) >> 5;
-  const int cpw = (ntile + nw - 1) / nw;
-  {  // strength-ordered segment: each warp scans a contiguous chunk of tiles
-    float run = 0.f;
+  for (int j = 0; j < n; ++j) {
+    Tables T;
+    board_tables(c, ops[j].board, T);
+    const int V = T.nvalid[o];
+    const uint16_t* g = T.gidx[o];
+    const uint16_t* co = T.coff[o];
+    const float* rch = c.rch + (size_t)j * c.vstride;
+    float* buf = c.buf + (size_t)j * 3 * c.vstride;
+    const int ntile = (V + 31) >> 5;
+    const int cpw = (ntile + nw - 1) / nw;
+    float run = 0.f;  // strength-ordered part: each warp scans a chunk of tiles
     const int t0 = warp * cpw, t1 = min(ntile, t0 + cpw);
     for (int t = t0; t < t1; ++t) {
       const int k = t * 32 + lane;
@@ -269,89 +319,87 @@ __device__ void op_term(const Ctx& c, const Op& op, int p) {
       if (k < V) buf[k] = x;
       run = __shfl_sync(0xffffffffu, x, 31);
     }
-    if (lane == 0) c.carry[warp] = run;
-  }
-  for (int cc = warp; cc < 52; cc += nw) {  // per-card segments
-    const int s0 = co[cc], s1 = co[cc + 1];
-    float run = 0.f;
-    for (int k0 = s0; k0 < s1; k0 += 32) {
-      const int k = k0 + lane;
-      float x = k < s1 ? rch[g[V + k]] : 0.f;
-      x = warp_incl_scan(x, lane) + run;
-      if (k < s1) buf[V + k] = x;
-      run = __shfl_sync(0xffffffffu, x, 31);
+    if (lane == 0) c.carry[j * 32 + warp] = run;
+    for (int cc = warp; cc < 52; cc += nw) {  // per-card segments
+      const int s0 = co[cc], s1 = co[cc + 1];
+      float r2 = 0.f;
+      for (int k0 = s0; k0 < s1; k0 += 32) {
+        const int k = k0 + lane;
+        float x = k < s1 ? rch[g[V + k]] : 0.f;
+        x = warp_incl_scan(x, lane) + r2;
+        if (k < s1) buf[V + k] = x;
+        r2 = __shfl_sync(0xffffffffu, x, 31);
+      }
     }
   }
   __syncthreads();
-
-  // exclusive prefix of the chunk totals, one per lane
-  float cpre = lane < nw ? c.carry[lane] : 0.f;
-  {
-    float incl = warp_incl_scan(cpre, lane);
-    cpre = incl - cpre;
-  }
-  const NodeDev nd = sp.nodes[op.node];
-  const uint16_t* thr = sp.thr[p] + (size_t)b * hsp * kThrWords;
   const uint8_t* pc = sp.cards[p];
   const uint16_t* same = sp.same[p];
-  // T = sum of all valid opponent reach
-  float T;
-  {
-    int j = V - 1;
-    int w = j >= 0 ? (j >> 5) / cpw : 0;
-    float base = j >= 0 ? buf[j] : 0.f;
-    float add = __shfl_sync(0xffffffffu, cpre, w & 31);
-    T = j >= 0 ? base + add : 0.f;
-  }
-  for (int h0 = 0; h0 < hsp; h0 += nt) {  // uniform trip count: shuffles below
-    const int h = h0 + tid;
-    float v = 0.f;
-    uint4 t = make_uint4(0, 0, 0, 0);
-    if (h < Hp) t = *reinterpret_cast<const uint4*>(thr + (size_t)h * kThrWords);
-    const int lt = t.x & 0xFFFF, le = t.x >> 16;
-    // prefix sums over the strength-ordered part need the chunk carry
-    const int jl = lt - 1, je = le - 1;
-    const int wl = jl >= 0 ? (jl >> 5) / cpw : 0, we = je >= 0 ? (je >> 5) / cpw : 0;
-    const float cl = __shfl_sync(0xffffffffu, cpre, wl & 31);
-    const float ce = __shfl_sync(0xffffffffu, cpre, we & 31);
-    const bool valid = h < Hp && (t.w & 0xFFFF) != 0 && V > 0;
-    if (valid) {
-      const int c1 = pc[2 * h], c2 = pc[2 * h + 1];
-      const int s1a = co[c1], s1b = co[c1 + 1], s2a = co[c2], s2b = co[c2 + 1];
-      const float* q1 = buf + V + s1a;
-      const float* q2 = buf + V + s2a;
-      const float M1 = s1b > s1a ? q1[s1b - s1a - 1] : 0.f;
-      const float M2 = s2b > s2a ? q2[s2b - s2a - 1] : 0.f;
-      if (op.term == TERM_SHOWDOWN) {
-        const int ltc1 = t.y & 0xFFFF, lec1 = t.y >> 16, ltc2 = t.z & 0xFFFF, lec2 = t.z >> 16;
-        const float Plt = jl >= 0 ? buf[jl] + cl : 0.f;
-        const float Ple = je >= 0 ? buf[je] + ce : 0.f;
-        const float Q1lt = ltc1 > 0 ? q1[ltc1 - 1] : 0.f, Q1le = lec1 > 0 ? q1[lec1 - 1] : 0.f;
-        const float Q2lt = ltc2 > 0 ? q2[ltc2 - 1] : 0.f, Q2le = lec2 > 0 ? q2[lec2 - 1] : 0.f;
-        const float win = Plt - Q1lt - Q2lt;
-        if (!sp.raked) {
-          const float lose = (T - Ple) - (M1 - Q1le) - (M2 - Q2le);
-          v = __fadd_rn(__fmul_rn(nd.amount_win, win), __fmul_rn(nd.amount_lose, lose));
+  for (int j = 0; j < n; ++j) {
+    const Op& op = ops[j];
+    Tables T;
+    board_tables(c, op.board, T);
+    const int V = T.nvalid[o];
+    const uint16_t* co = T.coff[o];
+    const uint2* thr = T.thr[p];
+    const float* rch = c.rch + (size_t)j * c.vstride;
+    const float* buf = c.buf + (size_t)j * 3 * c.vstride;
+    const int ntile = (V + 31) >> 5;
+    const int cpw = max(1, (ntile + nw - 1) / nw);
+    float cpre = lane < nw ? c.carry[j * 32 + lane] : 0.f;  // exclusive prefix of chunk totals
+    cpre = warp_incl_scan(cpre, lane) - cpre;
+    const NodeDev& nd = sp.nodes[op.node];
+    float* dst = slot_at(c, op.dst);
+    const float ctot = __shfl_sync(0xffffffffu, cpre, V > 0 ? (((V - 1) >> 5) / cpw) & 31 : 0);
+    const float Tsum = V > 0 ? buf[V - 1] + ctot : 0.f;
+    for (int h0 = 0; h0 < hsp; h0 += nt) {  // uniform trip count: shuffles below
+      const int h = h0 + tid;
+      float v = 0.f;
+      uint2 t = make_uint2(THR_INVALID, 0);
+      if (h < Hp) t = thr[h];
+      const bool valid = t.x != THR_INVALID && V > 0;
+      const int lt = valid ? (int)(t.x & 0xFFFF) : 0, le = valid ? (int)(t.x >> 16) : 0;
+      const int jl = lt - 1, je = le - 1;
+      const float cl = __shfl_sync(0xffffffffu, cpre, jl >= 0 ? ((jl >> 5) / cpw) & 31 : 0);
+      const float ce = __shfl_sync(0xffffffffu, cpre, je >= 0 ? ((je >> 5) / cpw) & 31 : 0);
+      if (valid) {
+        const int c1 = pc[2 * h], c2 = pc[2 * h + 1];
+        const int s1a = co[c1], s1b = co[c1 + 1], s2a = co[c2], s2b = co[c2 + 1];
+        const float* q1 = buf + V + s1a;
+        const float* q2 = buf + V + s2a;
+        const float M1 = s1b > s1a ? q1[s1b - s1a - 1] : 0.f;
+        const float M2 = s2b > s2a ? q2[s2b - s2a - 1] : 0.f;
+        if (op.term == TERM_SHOWDOWN) {
+          const int ltc1 = t.y & 0xFF, lec1 = (t.y >> 8) & 0xFF, ltc2 = (t.y >> 16) & 0xFF, lec2 = t.y >> 24;
+          const float Plt = jl >= 0 ? buf[jl] + cl : 0.f;
+          const float Ple = je >= 0 ? buf[je] + ce : 0.f;
+          const float Q1lt = ltc1 > 0 ? q1[ltc1 - 1] : 0.f, Q1le = lec1 > 0 ? q1[lec1 - 1] : 0.f;
+          const float Q2lt = ltc2 > 0 ? q2[ltc2 - 1] : 0.f, Q2le = lec2 > 0 ? q2[lec2 - 1] : 0.f;
+          const float win = Plt - Q1lt - Q2lt;
+          if (!sp.raked) {
+            const float lose = (Tsum - Ple) - (M1 - Q1le) - (M2 - Q2le);
+            v = __fadd_rn(__fmul_rn(nd.amount_win, win), __fmul_rn(nd.amount_lose, lose));
+          } else {
+            const uint16_t si = same[h];
+            const float rs = si != 0xFFFF ? rch[si] : 0.f;
+            const float tie = Ple - Q1le - Q2le;
+            const float tot = Tsum - M1 - M2;
+            v = nd.amount_win * win + nd.amount_tie * (tie - win + rs) + nd.amount_lose * (tot - tie);
+          }
         } else {
           const uint16_t si = same[h];
           const float rs = si != 0xFFFF ? rch[si] : 0.f;
-          const float tie = Ple - Q1le - Q2le;
-          const float tot = T - M1 - M2;
-          v = nd.amount_win * win + nd.amount_tie * (tie - win + rs) + nd.amount_lose * (tot - tie);
-        }
-      } else {
-        const uint16_t si = same[h];
-        const float rs = si != 0xFFFF ? rch[si] : 0.f;
-        const float adj = T + rs - M1 - M2;
-        if (op.term == TERM_FOLD) {
-          v = __fmul_rn(op.fold_pl != p ? nd.amount_win : nd.amount_lose, adj);
-        } else {
-          const float bv = sp.bcfv[((size_t)nd.boundary * 2 + p) * c.vstride + h];
-          v = __fmul_rn(__fmul_rn(bv, nd.payoff_scale), adj);
+          const float adj = Tsum + rs - M1 - M2;
+          if (op.term == TERM_FOLD) {
+            v = __fmul_rn(op.fold_pl != p ? nd.amount_win : nd.amount_lose, adj);
+          } else {
+            const float bv = sp.bcfv[((size_t)nd.boundary * 2 + p) * c.vstride + h];
+            v = __fmul_rn(__fmul_rn(bv, nd.payoff_scale), adj);
+          }
         }
       }
+      if (h < hsp) dst[h] = v;
     }
-    if (h < hsp) dst[h] = v;
   }
 }
 
@@ -377,7 +425,8 @@ __device__ void run_pass(const Ctx& c, int p, const Discount dc) {
         default: break;
       }
     }
-    for (int i = 0; i < st.n_term; ++i) op_term(c, ops[st.begin + st.n_elem + i], p);
+    for (int i = 0; i < st.n_term; i += c.kt)
+      term_batch(c, ops + st.begin + st.n_elem + i, min(c.kt, st.n_term - i), p);
     __syncthreads();
   }
 }
@@ -427,39 +476,73 @@ __device__ void dcfr_iteration(Ctx& c, const Discount dc) {
   }
 }
 
-__device__ bool bind_ctx(Ctx& c, const SpotDev* sp, float* scratch, size_t scratch_floats, float* smem,
-                         int* err) {
+// Binds a CTA to a spot: scratch slots, shared-memory regions and the board-0
+// tables, copied into shared memory when the plan reserves room for them.
+__device__ bool bind_ctx(Ctx& c, const SpotDev* sp, float* scratch, size_t scratch_floats, char* smem,
+                         const SmemPlan plan, int* err) {
   c.sp = sp;
   c.vstride = sp->vstride;
+  c.kt = plan.kt;
   c.slots = scratch;
-  c.rch = smem;
-  c.buf = smem + sp->vstride;
-  c.carry = smem + 4 * sp->vstride;
-  c.red = reinterpret_cast<double*>(smem + 4 * sp->vstride + 32);
-  if ((size_t)sp->num_slots * sp->vstride > scratch_floats) {
+  char* p = smem;
+  const int tb = table_bytes_for(sp->hs[0], sp->hs[1]);
+  const bool staged = sp->num_boards == 1 && tb <= plan.tables;
+  char* tables = p;
+  p += plan.tables;
+  c.rch = reinterpret_cast<float*>(p);
+  p += (size_t)plan.kt * plan.vstride * 4;
+  c.buf = reinterpret_cast<float*>(p);
+  p += (size_t)plan.kt * 3 * plan.vstride * 4;
+  c.carry = reinterpret_cast<float*>(p);
+  p += (size_t)plan.kt * 32 * 4;
+  c.red = reinterpret_cast<double*>(p);
+  if ((size_t)sp->num_slots * sp->vstride > scratch_floats || sp->vstride > plan.vstride) {
     if (threadIdx.x == 0) atomicOr(err, ERR_SCRATCH);
     return false;
+  }
+  for (int q = 0; q < 2; ++q) {
+    c.t0.gidx[q] = sp->gidx[q];
+    c.t0.coff[q] = sp->coff[q];
+    c.t0.thr[q] = reinterpret_cast<const uint2*>(sp->thr[q]);
+    c.t0.nvalid[q] = sp->nvalid[q][0];
+  }
+  if (staged) {
+    __syncthreads();  // the previous spot's users of the staged tables are done
+    uint2* thr_s = reinterpret_cast<uint2*>(tables);
+    uint16_t* u16 = reinterpret_cast<uint16_t*>(tables + 8 * (sp->hs[0] + sp->hs[1]));
+    for (int q = 0; q < 2; ++q) {
+      const int hs = sp->hs[q];
+      uint2* ts = thr_s + (q ? sp->hs[0] : 0);
+      const uint2* tg = reinterpret_cast<const uint2*>(sp->thr[q]);
+      for (int i = threadIdx.x; i < hs; i += blockDim.x) ts[i] = tg[i];
+      uint16_t* gs = u16 + (q ? 3 * sp->hs[0] : 0);
+      for (int i = threadIdx.x; i < 3 * hs; i += blockDim.x) gs[i] = sp->gidx[q][i];
+      uint16_t* cs = u16 + 3 * (sp->hs[0] + sp->hs[1]) + q * 56;
+      for (int i = threadIdx.x; i < 56; i += blockDim.x) cs[i] = sp->coff[q][i];
+      c.t0.thr[q] = ts;
+      c.t0.gidx[q] = gs;
+      c.t0.coff[q] = cs;
+    }
+    __syncthreads();
   }
   return true;
 }
 
-// Dynamic shared memory needed for a given max vstride.
-__host__ __device__ inline size_t smem_bytes(int vstride) { return (size_t)(4 * vstride + 32) * 4 + 32 * 8; }
-
 // ---------------------------------------------------------------------------
 // Kernels
 // ---------------------------------------------------------------------------
+#define PS_SOLVE_BOUNDS __launch_bounds__(256, 3)
 
 // Batched persistent solve: CTAs pull spots from `counter` (in `order`), and
 // run the full reference solve loop (solver.rs:108-176) per spot:
 //   expl = exploitability; for t < max_iter { if expl <= target break;
 //   iterate(t); if (t+1) % 5 == 0 || t+1 == max_iter: expl = exploitability }.
-__global__ void k_solve(const SpotDev* __restrict__ spots, int nspots, const int* __restrict__ order,
-                        int* counter, const Discount* __restrict__ disc, int max_iter,
-                        const float* __restrict__ target, float* scratch, size_t scratch_floats,
-                        float* out_expl, int* out_iters, int* err) {
+__global__ void PS_SOLVE_BOUNDS k_solve(const SpotDev* __restrict__ spots, int nspots, const int* __restrict__ order,
+                                        int* counter, const Discount* __restrict__ disc, int max_iter,
+                                        const float* __restrict__ target, float* scratch, size_t scratch_floats,
+                                        float* out_expl, int* out_iters, SmemPlan plan, int* err) {
   extern __shared__ float4 smem4[];
-  float* smem = reinterpret_cast<float*>(smem4);
+  char* smem = reinterpret_cast<char*>(smem4);
   __shared__ int s_spot;
   float* my_scratch = scratch + (size_t)blockIdx.x * scratch_floats;
   for (;;) {
@@ -470,7 +553,7 @@ __global__ void k_solve(const SpotDev* __restrict__ spots, int nspots, const int
     if (k >= nspots) return;
     const int si = order ? order[k] : k;
     Ctx c;
-    if (!bind_ctx(c, &spots[si], my_scratch, scratch_floats, smem, err)) continue;
+    if (!bind_ctx(c, &spots[si], my_scratch, scratch_floats, smem, plan, err)) continue;
     const float tgt = target[si];
     float expl = spot_exploitability(c);
     int t = 0;
@@ -487,27 +570,28 @@ __global__ void k_solve(const SpotDev* __restrict__ spots, int nspots, const int
 }
 
 // Fixed iteration range [t0, t1) for every spot (CTA-strided), no checks.
-__global__ void k_iterate(const SpotDev* __restrict__ spots, int nspots, const Discount* __restrict__ disc,
-                          int t0, int t1, float* scratch, size_t scratch_floats, int* err) {
+__global__ void PS_SOLVE_BOUNDS k_iterate(const SpotDev* __restrict__ spots, int nspots,
+                                          const Discount* __restrict__ disc, int t0, int t1, float* scratch,
+                                          size_t scratch_floats, SmemPlan plan, int* err) {
   extern __shared__ float4 smem4[];
-  float* smem = reinterpret_cast<float*>(smem4);
+  char* smem = reinterpret_cast<char*>(smem4);
   float* my_scratch = scratch + (size_t)blockIdx.x * scratch_floats;
   for (int si = blockIdx.x; si < nspots; si += gridDim.x) {
     Ctx c;
-    if (!bind_ctx(c, &spots[si], my_scratch, scratch_floats, smem, err)) continue;
+    if (!bind_ctx(c, &spots[si], my_scratch, scratch_floats, smem, plan, err)) continue;
     for (int t = t0; t < t1; ++t) dcfr_iteration(c, disc[t]);
     __syncthreads();
   }
 }
 
-__global__ void k_exploitability(const SpotDev* __restrict__ spots, int nspots, float* scratch,
-                                 size_t scratch_floats, float* out, int* err) {
+__global__ void PS_SOLVE_BOUNDS k_exploitability(const SpotDev* __restrict__ spots, int nspots, float* scratch,
+                                                 size_t scratch_floats, float* out, SmemPlan plan, int* err) {
   extern __shared__ float4 smem4[];
-  float* smem = reinterpret_cast<float*>(smem4);
+  char* smem = reinterpret_cast<char*>(smem4);
   float* my_scratch = scratch + (size_t)blockIdx.x * scratch_floats;
   for (int si = blockIdx.x; si < nspots; si += gridDim.x) {
     Ctx c;
-    if (!bind_ctx(c, &spots[si], my_scratch, scratch_floats, smem, err)) continue;
+    if (!bind_ctx(c, &spots[si], my_scratch, scratch_floats, smem, plan, err)) continue;
     float e = spot_exploitability(c);
     if (threadIdx.x == 0) out[si] = e;
     __syncthreads();
@@ -517,16 +601,16 @@ __global__ void k_exploitability(const SpotDev* __restrict__ spots, int nspots, 
 // Average-strategy values (utility.rs:552-795).  save != 0: finalize (stores
 // the per-node cfvalues for queries) for both players.  Otherwise one pass for
 // `player` from `root_reach` (root_cfvalues_with_reach), root values to out.
-__global__ void k_average(const SpotDev* __restrict__ spots, int nspots, int save, int player,
-                          const float* root_reach, float* scratch, size_t scratch_floats, float* out,
-                          int* err) {
+__global__ void PS_SOLVE_BOUNDS k_average(const SpotDev* __restrict__ spots, int nspots, int save, int player,
+                                          const float* root_reach, float* scratch, size_t scratch_floats, float* out,
+                                          SmemPlan plan, int* err) {
   extern __shared__ float4 smem4[];
-  float* smem = reinterpret_cast<float*>(smem4);
+  char* smem = reinterpret_cast<char*>(smem4);
   float* my_scratch = scratch + (size_t)blockIdx.x * scratch_floats;
   const Discount dz{0.f, 0.f, 0.f, 0.f};
   for (int si = blockIdx.x; si < nspots; si += gridDim.x) {
     Ctx c;
-    if (!bind_ctx(c, &spots[si], my_scratch, scratch_floats, smem, err)) continue;
+    if (!bind_ctx(c, &spots[si], my_scratch, scratch_floats, smem, plan, err)) continue;
     const SpotDev& sp = spots[si];
     if (save) {
       for (int p = 0; p < 2; ++p) {
@@ -543,11 +627,23 @@ __global__ void k_average(const SpotDev* __restrict__ spots, int nspots, int sav
   }
 }
 
+// Single-terminal evaluation for host queries (query.rs:699-712 evaluates a
+// terminal with the current weights): reach in slot 0, values out in slot 1.
+__global__ void k_eval_terminal(const SpotDev* __restrict__ spots, Op op, int player, float* scratch,
+                                size_t scratch_floats, SmemPlan plan, int* err) {
+  extern __shared__ float4 smem4[];
+  char* smem = reinterpret_cast<char*>(smem4);
+  Ctx c;
+  if (!bind_ctx(c, &spots[0], scratch, scratch_floats, smem, plan, err)) return;
+  c.root_reach = nullptr;
+  term_batch(c, &op, 1, player);
+}
+
 // ---------------------------------------------------------------------------
 // Board setup: strengths, orders, card groups and thresholds (card.rs:163-226,
 // card.rs:81-156).  One CTA per (spot, board).
 // ---------------------------------------------------------------------------
-constexpr int kSetupMaxH = 1344;  // >= 1326 rounded for sorting headroom
+constexpr int kSetupMaxH = 1344;  // >= 1326
 constexpr int kSortN = 2048;      // next power of two >= max hands
 constexpr int kSortN2 = 4096;     // >= 2 * max valid hands
 
@@ -593,7 +689,7 @@ struct SetupSmem {
   uint32_t keys[kSortN2];
   uint16_t sord[2][kSortN];   // strengths in order, per player
   uint16_t ord[2][kSortN];    // hand index in order
-  uint16_t istr[2][kSortN2 / 2 * 2];  // strength of each card-group entry
+  uint16_t istr[2][kSortN2];  // strength of each card-group entry
   uint16_t coff[2][56];
   uint16_t strength[2][kSetupMaxH];
   int nvalid[2];
@@ -681,58 +777,33 @@ __global__ void k_setup(const SpotDev* __restrict__ spots, const int2* __restric
       if (threadIdx.x == 0) sp.nvalid[q][b] = V;
       __syncthreads();
     }
-    // thresholds of player p's hands against opponent o = p ^ 1
+    // thresholds of player p's hands against opponent o = p ^ 1, 8 bytes per hand:
+    // x = lt | le << 16; y = ltc1 | lec1 << 8 | ltc2 << 16 | lec2 << 24; x = ~0 if blocked
     for (int p = 0; p < 2; ++p) {
       const int o = p ^ 1;
       const int Hp = sp.H[p], hsp = sp.hs[p], Vo = S.nvalid[o];
-      uint16_t* thr = sp.thr[p] + (size_t)b * hsp * kThrWords;
+      uint2* thr = reinterpret_cast<uint2*>(sp.thr[p]) + (size_t)b * hsp;
       for (int h = threadIdx.x; h < hsp; h += blockDim.x) {
-        uint16_t r[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        uint2 v = make_uint2(THR_INVALID, 0);
         if (h < Hp) {
           const int c1 = sp.cards[p][2 * h], c2 = sp.cards[p][2 * h + 1];
           const bool ok = !((bmask >> c1) & 1) && !((bmask >> c2) & 1);
           if (ok) {
             const uint16_t s = S.strength[p][h];
-            r[0] = (uint16_t)lower_bound_u16(S.sord[o], Vo, s);
-            r[1] = (uint16_t)upper_bound_u16(S.sord[o], Vo, s);
+            const uint32_t lt = lower_bound_u16(S.sord[o], Vo, s), le = upper_bound_u16(S.sord[o], Vo, s);
             const int a1 = S.coff[o][c1], n1 = S.coff[o][c1 + 1] - a1;
             const int a2 = S.coff[o][c2], n2 = S.coff[o][c2 + 1] - a2;
-            r[2] = (uint16_t)lower_bound_u16(S.istr[o] + a1, n1, s);
-            r[3] = (uint16_t)upper_bound_u16(S.istr[o] + a1, n1, s);
-            r[4] = (uint16_t)lower_bound_u16(S.istr[o] + a2, n2, s);
-            r[5] = (uint16_t)upper_bound_u16(S.istr[o] + a2, n2, s);
-            r[6] = 1;
+            const uint32_t l1 = lower_bound_u16(S.istr[o] + a1, n1, s), e1 = upper_bound_u16(S.istr[o] + a1, n1, s);
+            const uint32_t l2 = lower_bound_u16(S.istr[o] + a2, n2, s), e2 = upper_bound_u16(S.istr[o] + a2, n2, s);
+            v.x = lt | (le << 16);
+            v.y = l1 | (e1 << 8) | (l2 << 16) | (e2 << 24);
           }
         }
-        uint4 v;
-        v.x = r[0] | ((uint32_t)r[1] << 16);
-        v.y = r[2] | ((uint32_t)r[3] << 16);
-        v.z = r[4] | ((uint32_t)r[5] << 16);
-        v.w = r[6] | ((uint32_t)r[7] << 16);
-        *reinterpret_cast<uint4*>(thr + (size_t)h * kThrWords) = v;
+        thr[h] = v;
       }
     }
     __syncthreads();
   }
-}
-
-size_t setup_smem_bytes() { return sizeof(SetupSmem); }
-
-}  // namespace ps
-
-// ---------------------------------------------------------------------------
-// Single-terminal evaluation for host queries (query.rs:699-712 evaluates a
-// terminal with the current weights): reach in slot 0, values out in slot 1.
-// ---------------------------------------------------------------------------
-namespace ps {
-__global__ void k_eval_terminal(const SpotDev* __restrict__ spots, Op op, int player, float* scratch,
-                                size_t scratch_floats, int* err) {
-  extern __shared__ float4 smem4[];
-  float* smem = reinterpret_cast<float*>(smem4);
-  Ctx c;
-  if (!bind_ctx(c, &spots[0], scratch, scratch_floats, smem, err)) return;
-  c.root_reach = nullptr;
-  op_term(c, op, player);
 }
 
 // ---------------------------------------------------------------------------
@@ -742,7 +813,7 @@ static cudaError_t set_smem(const void* fn, size_t bytes) {
   return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-size_t solve_smem(int vstride) { return smem_bytes(vstride); }
+size_t setup_smem_bytes() { return sizeof(SetupSmem); }
 
 cudaError_t launch_setup(const SpotDev* spots, const int2* work, int nwork, const int32_t* table, int* err,
                          int grid, cudaStream_t s) {
@@ -755,52 +826,60 @@ cudaError_t launch_setup(const SpotDev* spots, const int2* work, int nwork, cons
 
 cudaError_t launch_solve(const SpotDev* spots, int nspots, const int* order, int* counter, const Discount* disc,
                          int max_iter, const float* target, float* scratch, size_t scratch_floats, float* out_expl,
-                         int* out_iters, int* err, int grid, int block, size_t smem, cudaStream_t s) {
+                         int* out_iters, int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s) {
+  size_t smem = plan.total();
   cudaError_t e = set_smem((const void*)k_solve, smem);
   if (e != cudaSuccess) return e;
-  k_solve<<<grid, block, smem, s>>>(spots, nspots, order, counter, disc, max_iter, target, scratch,
-                                     scratch_floats, out_expl, out_iters, err);
+  k_solve<<<grid, block, smem, s>>>(spots, nspots, order, counter, disc, max_iter, target, scratch, scratch_floats,
+                                     out_expl, out_iters, plan, err);
   return cudaGetLastError();
 }
 
-cudaError_t launch_iterate(const SpotDev* spots, int nspots, const Discount* disc, int t0, int t1,
-                           float* scratch, size_t scratch_floats, int* err, int grid, int block, size_t smem,
+cudaError_t launch_iterate(const SpotDev* spots, int nspots, const Discount* disc, int t0, int t1, float* scratch,
+                           size_t scratch_floats, int* err, int grid, int block, const SmemPlan& plan,
                            cudaStream_t s) {
+  size_t smem = plan.total();
   cudaError_t e = set_smem((const void*)k_iterate, smem);
   if (e != cudaSuccess) return e;
-  k_iterate<<<grid, block, smem, s>>>(spots, nspots, disc, t0, t1, scratch, scratch_floats, err);
+  k_iterate<<<grid, block, smem, s>>>(spots, nspots, disc, t0, t1, scratch, scratch_floats, plan, err);
   return cudaGetLastError();
 }
 
 cudaError_t launch_exploitability(const SpotDev* spots, int nspots, float* scratch, size_t scratch_floats,
-                                  float* out, int* err, int grid, int block, size_t smem, cudaStream_t s) {
+                                  float* out, int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s) {
+  size_t smem = plan.total();
   cudaError_t e = set_smem((const void*)k_exploitability, smem);
   if (e != cudaSuccess) return e;
-  k_exploitability<<<grid, block, smem, s>>>(spots, nspots, scratch, scratch_floats, out, err);
+  k_exploitability<<<grid, block, smem, s>>>(spots, nspots, scratch, scratch_floats, out, plan, err);
   return cudaGetLastError();
 }
 
 cudaError_t launch_average(const SpotDev* spots, int nspots, int save, int player, const float* root_reach,
                            float* scratch, size_t scratch_floats, float* out, int* err, int grid, int block,
-                           size_t smem, cudaStream_t s) {
+                           const SmemPlan& plan, cudaStream_t s) {
+  size_t smem = plan.total();
   cudaError_t e = set_smem((const void*)k_average, smem);
   if (e != cudaSuccess) return e;
-  k_average<<<grid, block, smem, s>>>(spots, nspots, save, player, root_reach, scratch, scratch_floats, out, err);
+  k_average<<<grid, block, smem, s>>>(spots, nspots, save, player, root_reach, scratch, scratch_floats, out, plan,
+                                       err);
   return cudaGetLastError();
 }
 
 cudaError_t launch_eval_terminal(const SpotDev* spots, Op op, int player, float* scratch, size_t scratch_floats,
-                                 int* err, int block, size_t smem, cudaStream_t s) {
+                                 int* err, int block, const SmemPlan& plan, cudaStream_t s) {
+  size_t smem = plan.total();
   cudaError_t e = set_smem((const void*)k_eval_terminal, smem);
   if (e != cudaSuccess) return e;
-  k_eval_terminal<<<1, block, smem, s>>>(spots, op, player, scratch, scratch_floats, err);
+  k_eval_terminal<<<1, block, smem, s>>>(spots, op, player, scratch, scratch_floats, plan, err);
   return cudaGetLastError();
 }
 
-int solve_occupancy(int block, size_t smem) {
+int solve_occupancy(int block, const SmemPlan& plan) {
   int n = 0;
+  size_t smem = plan.total();
   set_smem((const void*)k_solve, smem);
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solve, block, smem) != cudaSuccess) return 1;
   return n < 1 ? 1 : n;
 }
+
 }  // namespace ps

@@ -1,4 +1,5 @@
-// Host-callable launchers of the kernels in ps_kernels.cu.
+// Host-callable launchers of the kernels in ps_kernels.cu and the shared
+// memory plan they share with the host.
 #pragma once
 #include <cuda_runtime.h>
 #include <cstddef>
@@ -6,22 +7,40 @@
 #include "ps_device.hpp"
 
 namespace ps {
-size_t solve_smem(int vstride);
+
+// Board tables of one board staged in shared memory: gidx (u16, 3 * hs per
+// player), coff (u16, 56 per player) and thresholds (8 bytes per hand).
+__host__ __device__ inline int table_bytes_for(int hs0, int hs1) {
+  int b = 2 * (3 * hs0 + 3 * hs1) + 2 * 2 * 56 + 8 * (hs0 + hs1);
+  return (b + 15) & ~15;
+}
+
+// Shared-memory plan of one solve CTA (computed on the host per launch).
+struct SmemPlan {
+  int vstride;  // max slot stride of the launch (floats)
+  int hs_max;   // max padded hand count
+  int kt;       // terminals evaluated per batch
+  int tables;   // bytes reserved for staged board tables (0 = tables stay in global memory)
+  __host__ __device__ size_t total() const {
+    return (size_t)tables + (size_t)kt * (4 * vstride + 32) * 4 + 32 * 8;
+  }
+};
+
 size_t setup_smem_bytes();
-int solve_occupancy(int block, size_t smem);
+int solve_occupancy(int block, const SmemPlan& plan);
 cudaError_t launch_setup(const SpotDev* spots, const int2* work, int nwork, const int32_t* table, int* err,
                          int grid, cudaStream_t s);
 cudaError_t launch_solve(const SpotDev* spots, int nspots, const int* order, int* counter, const Discount* disc,
                          int max_iter, const float* target, float* scratch, size_t scratch_floats, float* out_expl,
-                         int* out_iters, int* err, int grid, int block, size_t smem, cudaStream_t s);
+                         int* out_iters, int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s);
 cudaError_t launch_iterate(const SpotDev* spots, int nspots, const Discount* disc, int t0, int t1,
-                           float* scratch, size_t scratch_floats, int* err, int grid, int block, size_t smem,
-                           cudaStream_t s);
+                           float* scratch, size_t scratch_floats, int* err, int grid, int block,
+                           const SmemPlan& plan, cudaStream_t s);
 cudaError_t launch_exploitability(const SpotDev* spots, int nspots, float* scratch, size_t scratch_floats,
-                                  float* out, int* err, int grid, int block, size_t smem, cudaStream_t s);
+                                  float* out, int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s);
 cudaError_t launch_average(const SpotDev* spots, int nspots, int save, int player, const float* root_reach,
                            float* scratch, size_t scratch_floats, float* out, int* err, int grid, int block,
-                           size_t smem, cudaStream_t s);
+                           const SmemPlan& plan, cudaStream_t s);
 cudaError_t launch_eval_terminal(const SpotDev* spots, Op op, int player, float* scratch, size_t scratch_floats,
-                                 int* err, int block, size_t smem, cudaStream_t s);
+                                 int* err, int block, const SmemPlan& plan, cudaStream_t s);
 }  // namespace ps
