@@ -103,7 +103,7 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct Layout {  // byte offsets inside the pool
   size_t cards[2], w[2], same[2], ops[2], steps[2], nodes, board_cards, iso_perm[2], iso_off, iso_ent;  // static
-  size_t gidx[2], coff[2], thr[2], nvalid[2];                                                         // setup
+  size_t gidx[2], coff[2], thr[2], nvalid[2], heads[2];                                                       // setup
   size_t R, S, ipcfv, chcfv, bcfv;                                                                    // state
 };
 
@@ -189,6 +189,7 @@ struct Batch {
         L.coff[p] = take(su, nb * 56 * 2);
         L.thr[p] = take(su, nb * g.hs[p] * kThrWords * 2);
         L.nvalid[p] = take(su, nb * 4);
+        L.heads[p] = take(su, nb * 4 * (size_t)head_words(g.hs[p]));
       }
       L.nodes = take(so, g.arena.size() * sizeof(NodeDev));
       L.board_cards = take(so, nb * 5);
@@ -248,6 +249,7 @@ struct Batch {
         s.coff[p] = (uint16_t*)(dU + L.coff[p]);
         s.thr[p] = (uint16_t*)(dU + L.thr[p]);
         s.nvalid[p] = (int32_t*)(dU + L.nvalid[p]);
+        s.heads[p] = (uint32_t*)(dU + L.heads[p]);
       }
       NodeDev* nd = (NodeDev*)(h_static + L.nodes);
       for (size_t k = 0; k < g.arena.size(); ++k) {

@@ -19,7 +19,7 @@ enum TermKind : uint8_t { TERM_FOLD = 0, TERM_SHOWDOWN = 1, TERM_BOUNDARY = 2 };
 
 constexpr uint16_t SLOT_ROOT_REACH = 0xFFFF;  // the opponent's initial weights
 constexpr int kMaxActions = 16;
-constexpr int kThrWords = 4;  // per-hand threshold record (u16 x 4 = 8 bytes)
+constexpr int kThrWords = 8;  // per-hand lookup record (u16 x 8 = 16 bytes)
 
 // 16-byte op record.
 struct Op {
@@ -80,7 +80,8 @@ struct SpotDev {
   const uint8_t* board_cards; // [num_boards][5], 255 = none
   uint16_t* gidx[2];   // opponent o: [num_boards][3 * hs[o]] gather order (ord, then by card)
   uint16_t* coff[2];   // opponent o: [num_boards][56] card segment starts within the card part
-  uint16_t* thr[2];    // player p: [num_boards][hs[p]] 8-byte threshold records vs the opponent
+  uint16_t* thr[2];    // player p: [num_boards][hs[p]] 16-byte lookup records vs the opponent
+  uint32_t* heads[2];  // opponent o: [num_boards][(3 * hs[o] + 31) / 32] segment-start bits of the gather list
   int32_t* nvalid[2];  // player: [num_boards] valid hand count
   const float* bcfv;   // boundary cfvs [num_boundary][2][vstride] (pot-normalised)
   const uint16_t* iso_perm[2]; // player: [perm id][hs] index of the suit-swapped hand

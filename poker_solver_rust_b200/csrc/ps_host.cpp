@@ -796,9 +796,18 @@ void Game::compile(int p) {
       P.ops.push_back(o);
     }
     int ne = (int)P.ops.size() - begin;
-    for (size_t n : at[d]) {
+    std::vector<size_t> terms;
+    for (size_t n : at[d])
+      if (arena[n].terminal()) terms.push_back(n);
+    // terminals reading the same reach on the same board are adjacent, so a
+    // batch scans that reach once
+    std::stable_sort(terms.begin(), terms.end(), [&](size_t x, size_t y) {
+      int bx = node_board[x], by = node_board[y];
+      if (bx != by) return bx < by;
+      return reach_slot(x) < reach_slot(y);
+    });
+    for (size_t n : terms) {
       const ArenaNode& a = arena[n];
-      if (!a.terminal()) continue;
       Op o{};
       o.type = OP_TERM;
       o.node = (uint32_t)n;

@@ -36,9 +36,9 @@ constexpr int ERR_SETUP = 2;    // setup tables exceeded their bounds
 constexpr uint32_t THR_INVALID = 0xFFFFFFFFu;
 
 struct Tables {  // board tables of one board, in shared or global memory
-  const uint16_t* gidx[2];
-  const uint16_t* coff[2];
-  const uint2* thr[2];
+  const uint16_t* gidx[2];   // opponent-indexed gather lists
+  const uint32_t* heads[2];  // opponent-indexed segment-start bitmaps
+  const uint4* thr[2];       // player-indexed lookup records
   int nvalid[2];
 };
 
@@ -50,7 +50,7 @@ struct Ctx {
   const float* root_reach;
   float* rch;    // smem: staged opponent reach  [kt][vstride]
   float* buf;    // smem: scan results           [kt][3 * vstride]
-  float* carry;  // smem: per-warp chunk totals  [kt][32]
+  float* carry;  // smem: per-warp chunk tails   [kt][64] (value, first head)
   double* red;   // smem: reduction scratch      [32]
   Tables t0;     // board-0 tables (shared memory when staged, else global)
 };
@@ -281,113 +281,163 @@ __device__ __forceinline__ void board_tables(const Ctx& c, int b, Tables& t) {
   const SpotDev& sp = *c.sp;
   for (int q = 0; q < 2; ++q) {
     t.gidx[q] = sp.gidx[q] + (size_t)b * 3 * sp.hs[q];
-    t.coff[q] = sp.coff[q] + (size_t)b * 56;
-    t.thr[q] = reinterpret_cast<const uint2*>(sp.thr[q]) + (size_t)b * sp.hs[q];
+    t.heads[q] = sp.heads[q] + (size_t)b * head_words(sp.hs[q]);
+    t.thr[q] = reinterpret_cast<const uint4*>(sp.thr[q]) + (size_t)b * sp.hs[q];
     t.nvalid[q] = sp.nvalid[q][b];
   }
 }
 
 // Evaluates ops[0..n) (n <= c.kt terminals of one step) for traverser p.
+//
+// The gather list of a terminal (3V entries: strength order, then per-card
+// groups) is scanned as one segmented inclusive scan: each warp owns a chunk
+// of whole 128-entry rows, each thread four consecutive entries; a second
+// phase adds the carry flowing in from earlier chunks to the entries of a
+// chunk that precede its first segment start.  Terminals that read the same
+// reach on the same board share one scan.
 __device__ void term_batch(const Ctx& c, const Op* ops, int n, int p) {
   const SpotDev& sp = *c.sp;
   const int o = p ^ 1;
   const int Ho = sp.H[o], Hp = sp.H[p], hsp = sp.hs[p];
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  // scan buffer used by op j: the first op of its run of equal (src, board)
+  int own[8];
+  for (int j = 0; j < n; ++j)
+    own[j] = (j > 0 && ops[j].src == ops[j - 1].src && ops[j].board == ops[j - 1].board) ? own[j - 1] : j;
   __syncthreads();  // the previous batch's lookups are done with rch / buf
   for (int j = 0; j < n; ++j) {
+    if (own[j] != j) continue;
     const float* src = slot_in(c, ops[j].src);
     float* rch = c.rch + (size_t)j * c.vstride;
     for (int q = tid; q < (Ho + 3) >> 2; q += nt) st4(rch + (q << 2), ld4(src + (q << 2)));
   }
   __syncthreads();
-  for (int j = 0; j < n; ++j) {
+  for (int j = 0; j < n; ++j) {  // segmented scan, one chunk per warp
+    if (own[j] != j) continue;
     Tables T;
     board_tables(c, ops[j].board, T);
-    const int V = T.nvalid[o];
+    const int V = T.nvalid[o], n3 = 3 * V;
     const uint16_t* g = T.gidx[o];
-    const uint16_t* co = T.coff[o];
+    const uint32_t* hd = T.heads[o];
     const float* rch = c.rch + (size_t)j * c.vstride;
     float* buf = c.buf + (size_t)j * 3 * c.vstride;
-    const int ntile = (V + 31) >> 5;
-    const int cpw = (ntile + nw - 1) / nw;
-    float run = 0.f;  // strength-ordered part: each warp scans a chunk of tiles
-    const int t0 = warp * cpw, t1 = min(ntile, t0 + cpw);
-    for (int t = t0; t < t1; ++t) {
-      const int k = t * 32 + lane;
-      float x = k < V ? rch[g[k]] : 0.f;
-      x = warp_incl_scan(x, lane) + run;
-      if (k < V) buf[k] = x;
-      run = __shfl_sync(0xffffffffu, x, 31);
-    }
-    if (lane == 0) c.carry[j * 32 + warp] = run;
-    for (int cc = warp; cc < 52; cc += nw) {  // per-card segments
-      const int s0 = co[cc], s1 = co[cc + 1];
-      float r2 = 0.f;
-      for (int k0 = s0; k0 < s1; k0 += 32) {
-        const int k = k0 + lane;
-        float x = k < s1 ? rch[g[V + k]] : 0.f;
-        x = warp_incl_scan(x, lane) + r2;
-        if (k < s1) buf[V + k] = x;
-        r2 = __shfl_sync(0xffffffffu, x, 31);
+    const int rows = (n3 + 127) >> 7;
+    const int rpw = (rows + nw - 1) / nw;
+    const int k0 = warp * rpw * 128, k1 = min(n3, k0 + rpw * 128);
+    float carry = 0.f;
+    int first_head = 0x7FFFFFFF;
+    for (int base = k0; base < k1; base += 128) {
+      const int k = base + 4 * lane;
+      const uint32_t word = k < n3 ? hd[k >> 5] : 0u;
+      const uint32_t f4 = (word >> (k & 31)) & 0xFu;
+      float x0 = k < n3 ? rch[g[k]] : 0.f;
+      float x1 = k + 1 < n3 ? rch[g[k + 1]] : 0.f;
+      float x2 = k + 2 < n3 ? rch[g[k + 2]] : 0.f;
+      float x3 = k + 3 < n3 ? rch[g[k + 3]] : 0.f;
+      x1 = (f4 & 2) ? x1 : x0 + x1;  // in-thread segmented scan
+      x2 = (f4 & 4) ? x2 : x1 + x2;
+      x3 = (f4 & 8) ? x3 : x2 + x3;
+      bool F = f4 != 0;
+      float v = x3;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {  // segmented warp scan of thread totals
+        const float vv = __shfl_up_sync(0xffffffffu, v, d);
+        const bool ff = __shfl_up_sync(0xffffffffu, (int)F, d) != 0;
+        if (lane >= d) {
+          if (!F) v += vv;
+          F = F || ff;
+        }
       }
+      float ev = __shfl_up_sync(0xffffffffu, v, 1);   // exclusive: lanes before this one
+      bool eF = __shfl_up_sync(0xffffffffu, (int)F, 1) != 0;
+      if (lane == 0) {
+        ev = 0.f;
+        eF = false;
+      }
+      const float in = eF ? ev : carry + ev;  // value flowing into this thread's first entry
+      if (!(f4 & 1)) x0 += in;
+      if (!(f4 & 3)) x1 += in;
+      if (!(f4 & 7)) x2 += in;
+      if (!(f4 & 15)) x3 += in;
+      if (k < n3) buf[k] = x0;
+      if (k + 1 < n3) buf[k + 1] = x1;
+      if (k + 2 < n3) buf[k + 2] = x2;
+      if (k + 3 < n3) buf[k + 3] = x3;
+      const float vl = __shfl_sync(0xffffffffu, v, 31);
+      const bool Fl = __shfl_sync(0xffffffffu, (int)F, 31) != 0;
+      carry = Fl ? vl : carry + vl;
+      const uint32_t hb = __ballot_sync(0xffffffffu, f4 != 0);
+      if (hb && first_head == 0x7FFFFFFF) {
+        const int l = __ffs(hb) - 1;
+        const uint32_t fl = __shfl_sync(0xffffffffu, f4, l);
+        first_head = base + 4 * l + (__ffs(fl) - 1);
+      }
+    }
+    if (lane == 0) {
+      c.carry[j * 64 + warp] = carry;
+      reinterpret_cast<int*>(c.carry)[j * 64 + 32 + warp] = k1 > k0 ? first_head : 0;
     }
   }
   __syncthreads();
-  const uint8_t* pc = sp.cards[p];
-  const uint16_t* same = sp.same[p];
+  for (int j = 0; j < n; ++j) {  // carries into chunks whose first entries continue a segment
+    if (own[j] != j) continue;
+    Tables T;
+    board_tables(c, ops[j].board, T);
+    const int V = T.nvalid[o], n3 = 3 * V;
+    const int rows = (n3 + 127) >> 7;
+    const int rpw = (rows + nw - 1) / nw;
+    const int k0 = warp * rpw * 128, k1 = min(n3, k0 + rpw * 128);
+    if (warp == 0 || k0 >= k1) continue;
+    const int* fh = reinterpret_cast<const int*>(c.carry) + j * 64 + 32;
+    float cin = 0.f;
+    for (int w = 0; w < warp; ++w) {
+      const int wk0 = w * rpw * 128;
+      const bool head_in_w = fh[w] < 0x7FFFFFFF && fh[w] >= wk0;
+      cin = head_in_w ? c.carry[j * 64 + w] : cin + c.carry[j * 64 + w];
+    }
+    float* buf = c.buf + (size_t)j * 3 * c.vstride;
+    const int stop = min(k1, fh[warp]);
+    for (int k = k0 + lane; k < stop; k += 32) buf[k] += cin;
+  }
+  __syncthreads();
   for (int j = 0; j < n; ++j) {
     const Op& op = ops[j];
     Tables T;
     board_tables(c, op.board, T);
     const int V = T.nvalid[o];
-    const uint16_t* co = T.coff[o];
-    const uint2* thr = T.thr[p];
-    const float* rch = c.rch + (size_t)j * c.vstride;
-    const float* buf = c.buf + (size_t)j * 3 * c.vstride;
-    const int ntile = (V + 31) >> 5;
-    const int cpw = max(1, (ntile + nw - 1) / nw);
-    float cpre = lane < nw ? c.carry[j * 32 + lane] : 0.f;  // exclusive prefix of chunk totals
-    cpre = warp_incl_scan(cpre, lane) - cpre;
+    const uint4* thr = T.thr[p];
+    const float* rch = c.rch + (size_t)own[j] * c.vstride;
+    const float* buf = c.buf + (size_t)own[j] * 3 * c.vstride;
+    const float* cp = buf + V;  // card-group part
     const NodeDev& nd = sp.nodes[op.node];
     float* dst = slot_at(c, op.dst);
-    const float ctot = __shfl_sync(0xffffffffu, cpre, V > 0 ? (((V - 1) >> 5) / cpw) & 31 : 0);
-    const float Tsum = V > 0 ? buf[V - 1] + ctot : 0.f;
-    for (int h0 = 0; h0 < hsp; h0 += nt) {  // uniform trip count: shuffles below
-      const int h = h0 + tid;
+    const float Tsum = V > 0 ? buf[V - 1] : 0.f;
+    for (int h = tid; h < hsp; h += nt) {
       float v = 0.f;
-      uint2 t = make_uint2(THR_INVALID, 0);
-      if (h < Hp) t = thr[h];
-      const bool valid = t.x != THR_INVALID && V > 0;
-      const int lt = valid ? (int)(t.x & 0xFFFF) : 0, le = valid ? (int)(t.x >> 16) : 0;
-      const int jl = lt - 1, je = le - 1;
-      const float cl = __shfl_sync(0xffffffffu, cpre, jl >= 0 ? ((jl >> 5) / cpw) & 31 : 0);
-      const float ce = __shfl_sync(0xffffffffu, cpre, je >= 0 ? ((je >> 5) / cpw) & 31 : 0);
-      if (valid) {
-        const int c1 = pc[2 * h], c2 = pc[2 * h + 1];
-        const int s1a = co[c1], s1b = co[c1 + 1], s2a = co[c2], s2b = co[c2 + 1];
-        const float* q1 = buf + V + s1a;
-        const float* q2 = buf + V + s2a;
-        const float M1 = s1b > s1a ? q1[s1b - s1a - 1] : 0.f;
-        const float M2 = s2b > s2a ? q2[s2b - s2a - 1] : 0.f;
+      const uint4 t = h < Hp ? thr[h] : make_uint4(THR_INVALID, 0, 0, 0);
+      if (t.x != THR_INVALID && V > 0) {
+        const int s1 = t.z & 0xFFFF, s2 = t.z >> 16, n1 = t.w & 0xFF, n2 = (t.w >> 8) & 0xFF;
+        const float M1 = n1 ? cp[s1 + n1 - 1] : 0.f;
+        const float M2 = n2 ? cp[s2 + n2 - 1] : 0.f;
         if (op.term == TERM_SHOWDOWN) {
+          const int lt = t.x & 0xFFFF, le = t.x >> 16;
           const int ltc1 = t.y & 0xFF, lec1 = (t.y >> 8) & 0xFF, ltc2 = (t.y >> 16) & 0xFF, lec2 = t.y >> 24;
-          const float Plt = jl >= 0 ? buf[jl] + cl : 0.f;
-          const float Ple = je >= 0 ? buf[je] + ce : 0.f;
-          const float Q1lt = ltc1 > 0 ? q1[ltc1 - 1] : 0.f, Q1le = lec1 > 0 ? q1[lec1 - 1] : 0.f;
-          const float Q2lt = ltc2 > 0 ? q2[ltc2 - 1] : 0.f, Q2le = lec2 > 0 ? q2[lec2 - 1] : 0.f;
+          const float Plt = lt ? buf[lt - 1] : 0.f, Ple = le ? buf[le - 1] : 0.f;
+          const float Q1lt = ltc1 ? cp[s1 + ltc1 - 1] : 0.f, Q1le = lec1 ? cp[s1 + lec1 - 1] : 0.f;
+          const float Q2lt = ltc2 ? cp[s2 + ltc2 - 1] : 0.f, Q2le = lec2 ? cp[s2 + lec2 - 1] : 0.f;
           const float win = Plt - Q1lt - Q2lt;
           if (!sp.raked) {
             const float lose = (Tsum - Ple) - (M1 - Q1le) - (M2 - Q2le);
             v = __fadd_rn(__fmul_rn(nd.amount_win, win), __fmul_rn(nd.amount_lose, lose));
           } else {
-            const uint16_t si = same[h];
+            const uint32_t si = t.w >> 16;
             const float rs = si != 0xFFFF ? rch[si] : 0.f;
             const float tie = Ple - Q1le - Q2le;
             const float tot = Tsum - M1 - M2;
             v = nd.amount_win * win + nd.amount_tie * (tie - win + rs) + nd.amount_lose * (tot - tie);
           }
         } else {
-          const uint16_t si = same[h];
+          const uint32_t si = t.w >> 16;
           const float rs = si != 0xFFFF ? rch[si] : 0.f;
           const float adj = Tsum + rs - M1 - M2;
           if (op.term == TERM_FOLD) {
@@ -398,7 +448,7 @@ __device__ void term_batch(const Ctx& c, const Op* ops, int n, int p) {
           }
         }
       }
-      if (h < hsp) dst[h] = v;
+      dst[h] = v;
     }
   }
 }
@@ -494,7 +544,7 @@ __device__ bool bind_ctx(Ctx& c, const SpotDev* sp, float* scratch, size_t scrat
   c.buf = reinterpret_cast<float*>(p);
   p += (size_t)plan.kt * 3 * plan.vstride * 4;
   c.carry = reinterpret_cast<float*>(p);
-  p += (size_t)plan.kt * 32 * 4;
+  p += (size_t)plan.kt * 64 * 4;
   c.red = reinterpret_cast<double*>(p);
   if ((size_t)sp->num_slots * sp->vstride > scratch_floats || sp->vstride > plan.vstride) {
     if (threadIdx.x == 0) atomicOr(err, ERR_SCRATCH);
@@ -502,26 +552,27 @@ __device__ bool bind_ctx(Ctx& c, const SpotDev* sp, float* scratch, size_t scrat
   }
   for (int q = 0; q < 2; ++q) {
     c.t0.gidx[q] = sp->gidx[q];
-    c.t0.coff[q] = sp->coff[q];
-    c.t0.thr[q] = reinterpret_cast<const uint2*>(sp->thr[q]);
+    c.t0.heads[q] = sp->heads[q];
+    c.t0.thr[q] = reinterpret_cast<const uint4*>(sp->thr[q]);
     c.t0.nvalid[q] = sp->nvalid[q][0];
   }
   if (staged) {
     __syncthreads();  // the previous spot's users of the staged tables are done
-    uint2* thr_s = reinterpret_cast<uint2*>(tables);
-    uint16_t* u16 = reinterpret_cast<uint16_t*>(tables + 8 * (sp->hs[0] + sp->hs[1]));
+    uint4* thr_s = reinterpret_cast<uint4*>(tables);
+    uint32_t* hd_s = reinterpret_cast<uint32_t*>(tables + 16 * (sp->hs[0] + sp->hs[1]));
+    uint16_t* g_s = reinterpret_cast<uint16_t*>(hd_s + head_words(sp->hs[0]) + head_words(sp->hs[1]));
     for (int q = 0; q < 2; ++q) {
       const int hs = sp->hs[q];
-      uint2* ts = thr_s + (q ? sp->hs[0] : 0);
-      const uint2* tg = reinterpret_cast<const uint2*>(sp->thr[q]);
+      uint4* ts = thr_s + (q ? sp->hs[0] : 0);
+      const uint4* tg = reinterpret_cast<const uint4*>(sp->thr[q]);
       for (int i = threadIdx.x; i < hs; i += blockDim.x) ts[i] = tg[i];
-      uint16_t* gs = u16 + (q ? 3 * sp->hs[0] : 0);
+      uint32_t* hs_ = hd_s + (q ? head_words(sp->hs[0]) : 0);
+      for (int i = threadIdx.x; i < head_words(hs); i += blockDim.x) hs_[i] = sp->heads[q][i];
+      uint16_t* gs = g_s + (q ? 3 * sp->hs[0] : 0);
       for (int i = threadIdx.x; i < 3 * hs; i += blockDim.x) gs[i] = sp->gidx[q][i];
-      uint16_t* cs = u16 + 3 * (sp->hs[0] + sp->hs[1]) + q * 56;
-      for (int i = threadIdx.x; i < 56; i += blockDim.x) cs[i] = sp->coff[q][i];
       c.t0.thr[q] = ts;
+      c.t0.heads[q] = hs_;
       c.t0.gidx[q] = gs;
-      c.t0.coff[q] = cs;
     }
     __syncthreads();
   }
@@ -775,16 +826,41 @@ __global__ void k_setup(const SpotDev* __restrict__ spots, const int2* __restric
       uint16_t* co = sp.coff[q] + (size_t)b * 56;
       if (threadIdx.x < 56) co[threadIdx.x] = threadIdx.x <= 52 ? S.coff[q][threadIdx.x] : 0;
       if (threadIdx.x == 0) sp.nvalid[q][b] = V;
+      // segment starts of the gather list: 0 (strength order) and every non-empty card group
+      uint32_t* hd = sp.heads[q] + (size_t)b * head_words(sp.hs[q]);
+      for (int i = threadIdx.x; i < head_words(sp.hs[q]); i += blockDim.x) {
+        uint32_t wv = 0;
+        for (int bit = 0; bit < 32; ++bit) {
+          const int k = 32 * i + bit;
+          bool h = k == 0 && V > 0;
+          if (k >= V && k < 3 * V) {
+            const int r = k - V;
+            // r starts a group if it equals coff[c] for a non-empty group c
+            int lo = 0, hi = 52;
+            while (lo < hi) {
+              const int m = (lo + hi) >> 1;
+              if (S.coff[q][m + 1] <= r) lo = m + 1;
+              else hi = m;
+            }
+            h = S.coff[q][lo] == r;
+          }
+          if (h) wv |= 1u << bit;
+        }
+        hd[i] = wv;
+      }
       __syncthreads();
     }
-    // thresholds of player p's hands against opponent o = p ^ 1, 8 bytes per hand:
-    // x = lt | le << 16; y = ltc1 | lec1 << 8 | ltc2 << 16 | lec2 << 24; x = ~0 if blocked
+    // lookup records of player p's hands against opponent o = p ^ 1, 16 bytes per hand:
+    //   x = lt | le << 16  (opponent hands strictly weaker / weaker-or-tied)
+    //   y = ltc1 | lec1 << 8 | ltc2 << 16 | lec2 << 24  (the same inside each card group)
+    //   z = start of card group c1 | start of c2 << 16  (within the card part of the list)
+    //   w = size of c1 | size of c2 << 8 | same-hand index << 16;  x = ~0 if blocked
     for (int p = 0; p < 2; ++p) {
       const int o = p ^ 1;
       const int Hp = sp.H[p], hsp = sp.hs[p], Vo = S.nvalid[o];
-      uint2* thr = reinterpret_cast<uint2*>(sp.thr[p]) + (size_t)b * hsp;
+      uint4* thr = reinterpret_cast<uint4*>(sp.thr[p]) + (size_t)b * hsp;
       for (int h = threadIdx.x; h < hsp; h += blockDim.x) {
-        uint2 v = make_uint2(THR_INVALID, 0);
+        uint4 v = make_uint4(THR_INVALID, 0, 0, 0);
         if (h < Hp) {
           const int c1 = sp.cards[p][2 * h], c2 = sp.cards[p][2 * h + 1];
           const bool ok = !((bmask >> c1) & 1) && !((bmask >> c2) & 1);
@@ -797,6 +873,8 @@ __global__ void k_setup(const SpotDev* __restrict__ spots, const int2* __restric
             const uint32_t l2 = lower_bound_u16(S.istr[o] + a2, n2, s), e2 = upper_bound_u16(S.istr[o] + a2, n2, s);
             v.x = lt | (le << 16);
             v.y = l1 | (e1 << 8) | (l2 << 16) | (e2 << 24);
+            v.z = (uint32_t)a1 | ((uint32_t)a2 << 16);
+            v.w = (uint32_t)n1 | ((uint32_t)n2 << 8) | ((uint32_t)sp.same[p][h] << 16);
           }
         }
         thr[h] = v;

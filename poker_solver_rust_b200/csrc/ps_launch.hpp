@@ -8,10 +8,12 @@
 
 namespace ps {
 
-// Board tables of one board staged in shared memory: gidx (u16, 3 * hs per
-// player), coff (u16, 56 per player) and thresholds (8 bytes per hand).
+__host__ __device__ inline int head_words(int hs) { return (3 * hs + 31) / 32; }
+
+// Board tables of one board staged in shared memory: lookup records (16 bytes
+// per hand), gather lists (u16, 3 * hs per player) and segment-start bitmaps.
 __host__ __device__ inline int table_bytes_for(int hs0, int hs1) {
-  int b = 2 * (3 * hs0 + 3 * hs1) + 2 * 2 * 56 + 8 * (hs0 + hs1);
+  int b = 16 * (hs0 + hs1) + 4 * (head_words(hs0) + head_words(hs1)) + 2 * (3 * hs0 + 3 * hs1);
   return (b + 15) & ~15;
 }
 
@@ -22,7 +24,7 @@ struct SmemPlan {
   int kt;       // terminals evaluated per batch
   int tables;   // bytes reserved for staged board tables (0 = tables stay in global memory)
   __host__ __device__ size_t total() const {
-    return (size_t)tables + (size_t)kt * (4 * vstride + 32) * 4 + 32 * 8;
+    return (size_t)tables + (size_t)kt * (4 * vstride + 64) * 4 + 32 * 8;
   }
 };
 
