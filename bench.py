@@ -170,6 +170,7 @@ def main():
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--stage", type=int, default=-1)
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -211,7 +212,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    bs = ps.BatchSolver(cc, tcs, block_threads=args.block, ctas_per_sm=args.ctas_per_sm)
+    bs = ps.BatchSolver(cc, tcs, block_threads=args.block, ctas_per_sm=args.ctas_per_sm, stage_tables=args.stage)
     for _ in range(args.warmup):
         bs.solve(MAX_ITER, targets)
 
@@ -245,7 +246,8 @@ def main():
     for k in range(min(args.steps, args.e2e_steps)):
         barrier()
         t0 = time.perf_counter()
-        b2 = ps.BatchSolver(cc, tcs, block_threads=args.block, ctas_per_sm=args.ctas_per_sm)
+        b2 = ps.BatchSolver(cc, tcs, block_threads=args.block, ctas_per_sm=args.ctas_per_sm,
+                            stage_tables=args.stage)
         b2.solve(MAX_ITER, targets)
         e2, _ = b2.results()
         torch.cuda.synchronize()

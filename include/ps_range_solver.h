@@ -134,10 +134,11 @@ int ps_state_import(ps_game* g, const void* buf, uint64_t size);
  *      crates/gpu-range-solver/src/batch.rs:79-610) ---- */
 typedef struct ps_batch ps_batch;
 typedef struct ps_batch_opts {
-  int32_t block_threads;  /* 0 = autotuned */
-  int32_t ctas_per_sm;    /* 0 = autotuned */
+  int32_t block_threads;  /* threads per CTA, a multiple of 32 up to 256 (0 = default 256) */
+  int32_t ctas_per_sm;    /* 0 = as many as fit */
   int32_t sort_by_cost;   /* 1 = hand out the largest spots first */
-  int32_t reserved;
+  int32_t stage_tables;   /* 1 = copy a spot's board tables to shared memory, 0 = read them
+                             from global memory, -1 = default (0) */
 } ps_batch_opts;
 int ps_batch_new(const ps_card_config* cards, const ps_tree_config* trees, int32_t n,
                  const ps_batch_opts* opts, ps_batch** out);

@@ -52,7 +52,7 @@ class PsBatchOpts(C.Structure):
         ("block_threads", C.c_int32),
         ("ctas_per_sm", C.c_int32),
         ("sort_by_cost", C.c_int32),
-        ("reserved", C.c_int32),
+        ("stage_tables", C.c_int32),
     ]
 
 

@@ -102,7 +102,7 @@ bool parse_tree_config(const ps_tree_config* c, TreeCfg& t, std::string& err) {
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct Layout {  // byte offsets inside the pool
-  size_t cards[2], w[2], same[2], ops[2], steps[2], nodes, board_cards, iso_perm[2], iso_off, iso_ent;  // static
+  size_t cards[2], w[2], same[2], ops[2], steps[2], groups[2], nodes, board_cards, iso_perm[2], iso_off, iso_ent;  // static
   size_t gidx[2], coff[2], thr[2], nvalid[2], heads[2];                                                       // setup
   size_t R, S, ipcfv, chcfv, bcfv;                                                                    // state
 };
@@ -184,6 +184,7 @@ struct Batch {
         L.same[p] = take(so, (size_t)g.hs[p] * 2);
         L.ops[p] = take(so, g.prog[p].ops.size() * sizeof(Op));
         L.steps[p] = take(so, g.prog[p].steps.size() * sizeof(Step));
+        L.groups[p] = take(so, g.prog[p].groups.size() * 2 + 16);
         L.iso_perm[p] = take(so, g.iso_perm[p].size() * (size_t)g.hs[p] * 2 + 16);
         L.gidx[p] = take(su, nb * 3 * g.hs[p] * 2);
         L.coff[p] = take(su, nb * 56 * 2);
@@ -232,6 +233,7 @@ struct Batch {
         }
         std::memcpy(h_static + L.ops[p], g.prog[p].ops.data(), g.prog[p].ops.size() * sizeof(Op));
         std::memcpy(h_static + L.steps[p], g.prog[p].steps.data(), g.prog[p].steps.size() * sizeof(Step));
+        std::memcpy(h_static + L.groups[p], g.prog[p].groups.data(), g.prog[p].groups.size() * 2);
         uint16_t* ip = (uint16_t*)(h_static + L.iso_perm[p]);
         for (size_t k = 0; k < g.iso_perm[p].size(); ++k)
           std::memcpy(ip + k * g.hs[p], g.iso_perm[p][k].data(), (size_t)g.hs[p] * 2);
@@ -244,6 +246,7 @@ struct Batch {
         s.same[p] = (const uint16_t*)(dS + L.same[p]);
         s.ops[p] = (const Op*)(dS + L.ops[p]);
         s.steps[p] = (const Step*)(dS + L.steps[p]);
+        s.groups[p] = (const uint16_t*)(dS + L.groups[p]);
         s.iso_perm[p] = (const uint16_t*)(dS + L.iso_perm[p]);
         s.gidx[p] = (uint16_t*)(dU + L.gidx[p]);
         s.coff[p] = (uint16_t*)(dU + L.coff[p]);
@@ -308,21 +311,21 @@ struct Batch {
     CU(cudaMalloc(&d_counter, sizeof(int)));
     CU(cudaMalloc(&d_err, sizeof(int)));
     CU(cudaMalloc(&d_order, sizeof(int) * n));
-    // launch configuration: a block covers the largest hand vector four hands
-    // per thread; terminals per batch and staged tables sized to the spots
+    // launch configuration: warps per CTA (one op per warp at a time) and
+    // whether single-board spots stage their board tables in shared memory
     int hs_max = 4;
     bool single_board = true;
     for (auto& gp : games) {
       hs_max = std::max(hs_max, std::max(gp->hs[0], gp->hs[1]));
       single_board &= gp->boards.size() == 1;
     }
-    block = opts && opts->block_threads > 0 ? opts->block_threads
-                                            : std::min(256, std::max(128, ((hs_max / 4 + 31) / 32) * 32));
-    block = std::min(block, 256);
+    block = opts && opts->block_threads > 0 ? opts->block_threads : 256;
+    block = std::max(64, std::min(256, (block / 32) * 32));
+    const int stage = opts ? opts->stage_tables : -1;
     plan.vstride = max_vstride;
     plan.hs_max = hs_max;
-    plan.kt = 2;
-    plan.tables = single_board ? table_bytes_for(hs_max, hs_max) : 0;
+    plan.warps = block / 32;
+    plan.tables = (single_board && stage == 1) ? table_bytes_for(hs_max, hs_max) : 0;
     int occ = solve_occupancy(block, plan);
     ctas_per_sm = opts && opts->ctas_per_sm > 0 ? std::min(opts->ctas_per_sm, occ) : occ;
     grid = std::max(1, std::min(n, dc->nsm * ctas_per_sm));

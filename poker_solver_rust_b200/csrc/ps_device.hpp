@@ -35,9 +35,14 @@ struct Op {
 };
 static_assert(sizeof(Op) == 16, "Op must stay 16 bytes");
 
-// Program step: ops[begin, begin + n) run between two barriers.
+// Program step: ops[begin, begin + n_elem) are node ops, the next n_term ops
+// are terminals grouped in runs that read the same reach on the same board
+// (group g starts at begin + n_elem + groups[gbegin + g]; the leader's `na`
+// holds the run length).  All of a step's ops are independent.
 struct Step {
-  int32_t begin, n_elem, n_term, pad;
+  int32_t begin;
+  int16_t n_elem, n_term, n_groups, pad;
+  int32_t gbegin;
 };
 
 // Per-node tables indexed by arena index.
@@ -76,6 +81,7 @@ struct SpotDev {
   const uint16_t* same[2];   // [hs] same-hand index in the opponent list
   const Op* ops[2];
   const Step* steps[2];
+  const uint16_t* groups[2];  // terminal-group leader offsets of every step
   const NodeDev* nodes;
   const uint8_t* board_cards; // [num_boards][5], 255 = none
   uint16_t* gidx[2];   // opponent o: [num_boards][3 * hs[o]] gather order (ord, then by card)

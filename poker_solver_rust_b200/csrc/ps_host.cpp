@@ -662,6 +662,7 @@ void Game::compile(int p) {
   Program& P = prog[p];
   P.ops.clear();
   P.steps.clear();
+  P.groups.clear();
   auto eff = [&](size_t c) {
     while (!arena[c].terminal() && !arena[c].chance() && arena[c].nch == 1) c += arena[c].child_off;
     return c;
@@ -752,7 +753,23 @@ void Game::compile(int p) {
   std::vector<std::vector<size_t>> at(D + 1);
   for (size_t n : order) at[depth[n]].push_back(n);
   auto push_step = [&](int begin, int ne, int nt) {
-    if (ne + nt > 0) P.steps.push_back({begin, ne, nt, 0});
+    if (ne + nt == 0) return;
+    Step st{};
+    st.begin = begin;
+    st.n_elem = (int16_t)ne;
+    st.n_term = (int16_t)nt;
+    st.gbegin = (int32_t)P.groups.size();
+    // runs of terminals with the same (board, reach): the leader carries the run length
+    for (int i = 0; i < nt;) {
+      int j = i + 1;
+      Op& lead = P.ops[begin + ne + i];
+      while (j < nt && j - i < 255 && P.ops[begin + ne + j].board == lead.board && P.ops[begin + ne + j].src == lead.src) ++j;
+      lead.na = (uint8_t)(j - i);
+      P.groups.push_back((uint16_t)i);
+      i = j;
+    }
+    st.n_groups = (int16_t)(P.groups.size() - st.gbegin);
+    P.steps.push_back(st);
   };
   for (int d = 0; d <= D; ++d) {
     int begin = (int)P.ops.size();
@@ -847,6 +864,9 @@ bool Game::init(const float* r0, const float* r1, const uint8_t b[5], const Tree
   compile(1);
   num_slots = std::max(prog[0].num_slots, prog[1].num_slots);
   if (num_slots >= 0xFFF0) { err = "Tree too wide for the slot allocator"; return false; }
+  for (int p = 0; p < 2; ++p)
+    for (const auto& st : prog[p].steps)
+      if (st.n_elem > 32000 || st.n_term > 32000) { err = "Tree level too wide"; return false; }
   return true;
 }
 

@@ -86,6 +86,7 @@ struct ArenaNode {
 struct Program {
   std::vector<Op> ops;
   std::vector<Step> steps;
+  std::vector<uint16_t> groups;
   int root_slot = -1;
   int num_slots = 0;
 };

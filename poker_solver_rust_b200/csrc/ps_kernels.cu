@@ -3,21 +3,22 @@
 // Work decomposition: one CTA owns one game ("spot") at a time and walks its
 // level-ordered tree program (ps_device.hpp): forward steps propagate the
 // opponent's reach top-down, backward steps evaluate terminals and combine
-// children bottom-up with the DCFR regret / strategy update fused in.  A hand
-// vector is split across the CTA four hands per thread (128-bit loads and
-// stores of regrets, strategy sums and the per-node reach / value vectors);
-// steps are separated by __syncthreads only, so a whole solve of a spot - all
-// iterations plus the exploitability checks - runs inside one persistent
-// launch that pulls spots from a device work queue.  Several CTAs share an SM
-// so that one CTA's memory latency overlaps another's work.
+// children bottom-up with the DCFR regret / strategy update fused in.  The ops
+// of one step are independent, so each warp takes whole ops (a node's update,
+// or a run of terminals that read the same reach): hand vectors are streamed
+// by the warp four hands per lane (128-bit loads and stores of regrets,
+// strategy sums and the per-node reach / value vectors), different warps
+// overlap different nodes' memory latency, and a step ends with one
+// __syncthreads.  A whole solve of a spot - all iterations plus the
+// exploitability checks - runs inside one persistent launch that pulls spots
+// from a device work queue.
 //
 // Terminal evaluation restates crates/range-solver/src/game/evaluation.rs
 // without its sequential merge: the opponent reach is gathered into
 // hand-strength order and into per-card groups (both precomputed per board by
-// k_setup and staged in shared memory for single-board spots), scanned with
-// warp shuffles, and every hand reads its win / lose / blocked sums at
-// precomputed thresholds - O(n) work per terminal.  Terminals of a step are
-// evaluated in batches so that a batch shares its barriers.
+// k_setup), the warp scans that list segment by segment into its shared-memory
+// buffer, and every hand reads its win / lose / blocked sums at precomputed
+// positions - O(n) work per terminal, no CTA-wide barrier.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -46,12 +47,9 @@ struct Ctx {
   const SpotDev* sp;
   float* slots;
   int vstride;
-  int kt;
   const float* root_reach;
-  float* rch;    // smem: staged opponent reach  [kt][vstride]
-  float* buf;    // smem: scan results           [kt][3 * vstride]
-  float* carry;  // smem: per-warp chunk tails   [kt][64] (value, first head)
-  double* red;   // smem: reduction scratch      [32]
+  float* buf;    // smem: this warp's scan buffer [3 * vstride]
+  double* red;   // smem: reduction scratch       [32]
   Tables t0;     // board-0 tables (shared memory when staged, else global)
 };
 
@@ -114,7 +112,7 @@ __device__ void op_fwd_opp(const Ctx& c, const Op& op, int o) {
   const float* src = slot_in(c, op.src);
   float* dst = slot_at(c, op.blk);
   const float def = 1.0f / (float)na;
-  for (int q = threadIdx.x; q < q4; q += blockDim.x) {
+  for (int q = (threadIdx.x & 31); q < q4; q += 32) {
     const int h = q << 2;
     float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int a = 0; a < na; ++a) {
@@ -139,7 +137,7 @@ __device__ void op_fwd_chance(const Ctx& c, const Op& op, int o) {
   const float4 f4 = make_float4(f, f, f, f);
   const float* src = slot_in(c, op.src);
   float* dst = slot_at(c, op.blk);
-  for (int q = threadIdx.x; q < q4; q += blockDim.x) st4(dst + (q << 2), mul4(ld4(src + (q << 2)), f4));
+  for (int q = (threadIdx.x & 31); q < q4; q += 32) st4(dst + (q << 2), mul4(ld4(src + (q << 2)), f4));
 }
 
 // ---------------------------------------------------------------------------
@@ -163,7 +161,7 @@ __device__ void op_bwd_trav(const Ctx& c, const Op& op, int p, const Discount dc
   const float* cb = slot_at(c, op.blk);
   float* dst = slot_at(c, op.dst);
   const float def = 1.0f / (float)na;
-  for (int q = threadIdx.x; q < q4; q += blockDim.x) {
+  for (int q = (threadIdx.x & 31); q < q4; q += 32) {
     const int h = q << 2;
     float4 res = make_float4(0.f, 0.f, 0.f, 0.f);
     if (MODE == M_BR) {
@@ -219,7 +217,7 @@ __device__ void op_bwd_opp(const Ctx& c, const Op& op, int p) {
   const NodeDev& nd = sp.nodes[op.node];
   const float* cb = slot_at(c, op.blk);
   float* dst = slot_at(c, op.dst);
-  for (int q = threadIdx.x; q < q4; q += blockDim.x) {
+  for (int q = (threadIdx.x & 31); q < q4; q += 32) {
     const int h = q << 2;
     float4 res = ld4(cb + h);
     for (int a = 1; a < na; ++a) res = add4(res, ld4(cb + (size_t)a * c.vstride + h));
@@ -246,7 +244,7 @@ __device__ void op_bwd_chance(const Ctx& c, const Op& op, int p) {
     i0 = sp.iso_off[op.board];
     i1 = sp.iso_off[op.board + 1];
   }
-  for (int h = threadIdx.x; h < hsp; h += blockDim.x) {
+  for (int h = (threadIdx.x & 31); h < hsp; h += 32) {
     float res = cb[h];
     for (int a = 1; a < na; ++a) res = __fadd_rn(res, cb[(size_t)a * c.vstride + h]);
     for (int i = i0; i < i1; ++i) {
@@ -287,132 +285,77 @@ __device__ __forceinline__ void board_tables(const Ctx& c, int b, Tables& t) {
   }
 }
 
-// Evaluates ops[0..n) (n <= c.kt terminals of one step) for traverser p.
+// Evaluates a run of n terminals that read the same reach on the same board,
+// for traverser p, with the calling warp alone.
 //
-// The gather list of a terminal (3V entries: strength order, then per-card
-// groups) is scanned as one segmented inclusive scan: each warp owns a chunk
-// of whole 128-entry rows, each thread four consecutive entries; a second
-// phase adds the carry flowing in from earlier chunks to the entries of a
-// chunk that precede its first segment start.  Terminals that read the same
-// reach on the same board share one scan.
-__device__ void term_batch(const Ctx& c, const Op* ops, int n, int p) {
+// The gather list (3V entries: strength order, then per-card groups) is
+// scanned as one segmented inclusive scan, 128 entries per row (four per
+// lane), the running value carried from row to row; segment starts come from
+// the per-board bitmap.  The lookups then read the scan from shared memory.
+__device__ void warp_terms(const Ctx& c, const Op* ops, int n, int p) {
   const SpotDev& sp = *c.sp;
   const int o = p ^ 1;
-  const int Ho = sp.H[o], Hp = sp.H[p], hsp = sp.hs[p];
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-  // scan buffer used by op j: the first op of its run of equal (src, board)
-  int own[8];
-  for (int j = 0; j < n; ++j)
-    own[j] = (j > 0 && ops[j].src == ops[j - 1].src && ops[j].board == ops[j - 1].board) ? own[j - 1] : j;
-  __syncthreads();  // the previous batch's lookups are done with rch / buf
-  for (int j = 0; j < n; ++j) {
-    if (own[j] != j) continue;
-    const float* src = slot_in(c, ops[j].src);
-    float* rch = c.rch + (size_t)j * c.vstride;
-    for (int q = tid; q < (Ho + 3) >> 2; q += nt) st4(rch + (q << 2), ld4(src + (q << 2)));
-  }
-  __syncthreads();
-  for (int j = 0; j < n; ++j) {  // segmented scan, one chunk per warp
-    if (own[j] != j) continue;
-    Tables T;
-    board_tables(c, ops[j].board, T);
-    const int V = T.nvalid[o], n3 = 3 * V;
-    const uint16_t* g = T.gidx[o];
-    const uint32_t* hd = T.heads[o];
-    const float* rch = c.rch + (size_t)j * c.vstride;
-    float* buf = c.buf + (size_t)j * 3 * c.vstride;
-    const int rows = (n3 + 127) >> 7;
-    const int rpw = (rows + nw - 1) / nw;
-    const int k0 = warp * rpw * 128, k1 = min(n3, k0 + rpw * 128);
-    float carry = 0.f;
-    int first_head = 0x7FFFFFFF;
-    for (int base = k0; base < k1; base += 128) {
-      const int k = base + 4 * lane;
-      const uint32_t word = k < n3 ? hd[k >> 5] : 0u;
-      const uint32_t f4 = (word >> (k & 31)) & 0xFu;
-      float x0 = k < n3 ? rch[g[k]] : 0.f;
-      float x1 = k + 1 < n3 ? rch[g[k + 1]] : 0.f;
-      float x2 = k + 2 < n3 ? rch[g[k + 2]] : 0.f;
-      float x3 = k + 3 < n3 ? rch[g[k + 3]] : 0.f;
-      x1 = (f4 & 2) ? x1 : x0 + x1;  // in-thread segmented scan
-      x2 = (f4 & 4) ? x2 : x1 + x2;
-      x3 = (f4 & 8) ? x3 : x2 + x3;
-      bool F = f4 != 0;
-      float v = x3;
+  const int Hp = sp.H[p], hsp = sp.hs[p];
+  const int lane = threadIdx.x & 31;
+  Tables T;
+  board_tables(c, ops[0].board, T);
+  const int V = T.nvalid[o], n3 = 3 * V;
+  const uint16_t* g = T.gidx[o];
+  const uint32_t* hd = T.heads[o];
+  const float* rch = slot_in(c, ops[0].src);
+  float* buf = c.buf;
+  float carry = 0.f;
+  for (int base = 0; base < n3; base += 128) {
+    const int k = base + 4 * lane;
+    const uint32_t word = k < n3 ? hd[k >> 5] : 0u;
+    const uint32_t f4 = (word >> (k & 31)) & 0xFu;
+    float x0 = k < n3 ? rch[g[k]] : 0.f;
+    float x1 = k + 1 < n3 ? rch[g[k + 1]] : 0.f;
+    float x2 = k + 2 < n3 ? rch[g[k + 2]] : 0.f;
+    float x3 = k + 3 < n3 ? rch[g[k + 3]] : 0.f;
+    x1 = (f4 & 2) ? x1 : x0 + x1;  // in-lane segmented scan
+    x2 = (f4 & 4) ? x2 : x1 + x2;
+    x3 = (f4 & 8) ? x3 : x2 + x3;
+    bool F = f4 != 0;
+    float v = x3;
 #pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {  // segmented warp scan of thread totals
-        const float vv = __shfl_up_sync(0xffffffffu, v, d);
-        const bool ff = __shfl_up_sync(0xffffffffu, (int)F, d) != 0;
-        if (lane >= d) {
-          if (!F) v += vv;
-          F = F || ff;
-        }
-      }
-      float ev = __shfl_up_sync(0xffffffffu, v, 1);   // exclusive: lanes before this one
-      bool eF = __shfl_up_sync(0xffffffffu, (int)F, 1) != 0;
-      if (lane == 0) {
-        ev = 0.f;
-        eF = false;
-      }
-      const float in = eF ? ev : carry + ev;  // value flowing into this thread's first entry
-      if (!(f4 & 1)) x0 += in;
-      if (!(f4 & 3)) x1 += in;
-      if (!(f4 & 7)) x2 += in;
-      if (!(f4 & 15)) x3 += in;
-      if (k < n3) buf[k] = x0;
-      if (k + 1 < n3) buf[k + 1] = x1;
-      if (k + 2 < n3) buf[k + 2] = x2;
-      if (k + 3 < n3) buf[k + 3] = x3;
-      const float vl = __shfl_sync(0xffffffffu, v, 31);
-      const bool Fl = __shfl_sync(0xffffffffu, (int)F, 31) != 0;
-      carry = Fl ? vl : carry + vl;
-      const uint32_t hb = __ballot_sync(0xffffffffu, f4 != 0);
-      if (hb && first_head == 0x7FFFFFFF) {
-        const int l = __ffs(hb) - 1;
-        const uint32_t fl = __shfl_sync(0xffffffffu, f4, l);
-        first_head = base + 4 * l + (__ffs(fl) - 1);
+    for (int d = 1; d < 32; d <<= 1) {  // segmented warp scan of the lane totals
+      const float vv = __shfl_up_sync(0xffffffffu, v, d);
+      const bool ff = __shfl_up_sync(0xffffffffu, (int)F, d) != 0;
+      if (lane >= d) {
+        if (!F) v += vv;
+        F = F || ff;
       }
     }
+    float ev = __shfl_up_sync(0xffffffffu, v, 1);  // lanes before this one
+    bool eF = __shfl_up_sync(0xffffffffu, (int)F, 1) != 0;
     if (lane == 0) {
-      c.carry[j * 64 + warp] = carry;
-      reinterpret_cast<int*>(c.carry)[j * 64 + 32 + warp] = k1 > k0 ? first_head : 0;
+      ev = 0.f;
+      eF = false;
     }
+    const float in = eF ? ev : carry + ev;  // value flowing into this lane's first entry
+    if (!(f4 & 1)) x0 += in;
+    if (!(f4 & 3)) x1 += in;
+    if (!(f4 & 7)) x2 += in;
+    if (!(f4 & 15)) x3 += in;
+    if (k < n3) buf[k] = x0;
+    if (k + 1 < n3) buf[k + 1] = x1;
+    if (k + 2 < n3) buf[k + 2] = x2;
+    if (k + 3 < n3) buf[k + 3] = x3;
+    const float vl = __shfl_sync(0xffffffffu, v, 31);
+    const bool Fl = __shfl_sync(0xffffffffu, (int)F, 31) != 0;
+    carry = Fl ? vl : carry + vl;
   }
-  __syncthreads();
-  for (int j = 0; j < n; ++j) {  // carries into chunks whose first entries continue a segment
-    if (own[j] != j) continue;
-    Tables T;
-    board_tables(c, ops[j].board, T);
-    const int V = T.nvalid[o], n3 = 3 * V;
-    const int rows = (n3 + 127) >> 7;
-    const int rpw = (rows + nw - 1) / nw;
-    const int k0 = warp * rpw * 128, k1 = min(n3, k0 + rpw * 128);
-    if (warp == 0 || k0 >= k1) continue;
-    const int* fh = reinterpret_cast<const int*>(c.carry) + j * 64 + 32;
-    float cin = 0.f;
-    for (int w = 0; w < warp; ++w) {
-      const int wk0 = w * rpw * 128;
-      const bool head_in_w = fh[w] < 0x7FFFFFFF && fh[w] >= wk0;
-      cin = head_in_w ? c.carry[j * 64 + w] : cin + c.carry[j * 64 + w];
-    }
-    float* buf = c.buf + (size_t)j * 3 * c.vstride;
-    const int stop = min(k1, fh[warp]);
-    for (int k = k0 + lane; k < stop; k += 32) buf[k] += cin;
-  }
-  __syncthreads();
+  __syncwarp();
+  const uint4* thr = T.thr[p];
+  const float* cp = buf + V;  // card-group part
+  const float Tsum = V > 0 ? buf[V - 1] : 0.f;
   for (int j = 0; j < n; ++j) {
     const Op& op = ops[j];
-    Tables T;
-    board_tables(c, op.board, T);
-    const int V = T.nvalid[o];
-    const uint4* thr = T.thr[p];
-    const float* rch = c.rch + (size_t)own[j] * c.vstride;
-    const float* buf = c.buf + (size_t)own[j] * 3 * c.vstride;
-    const float* cp = buf + V;  // card-group part
     const NodeDev& nd = sp.nodes[op.node];
     float* dst = slot_at(c, op.dst);
-    const float Tsum = V > 0 ? buf[V - 1] : 0.f;
-    for (int h = tid; h < hsp; h += nt) {
+    const float aw = nd.amount_win, al = nd.amount_lose;
+    for (int h = lane; h < hsp; h += 32) {
       float v = 0.f;
       const uint4 t = h < Hp ? thr[h] : make_uint4(THR_INVALID, 0, 0, 0);
       if (t.x != THR_INVALID && V > 0) {
@@ -428,20 +371,20 @@ __device__ void term_batch(const Ctx& c, const Op* ops, int n, int p) {
           const float win = Plt - Q1lt - Q2lt;
           if (!sp.raked) {
             const float lose = (Tsum - Ple) - (M1 - Q1le) - (M2 - Q2le);
-            v = __fadd_rn(__fmul_rn(nd.amount_win, win), __fmul_rn(nd.amount_lose, lose));
+            v = __fadd_rn(__fmul_rn(aw, win), __fmul_rn(al, lose));
           } else {
             const uint32_t si = t.w >> 16;
             const float rs = si != 0xFFFF ? rch[si] : 0.f;
             const float tie = Ple - Q1le - Q2le;
             const float tot = Tsum - M1 - M2;
-            v = nd.amount_win * win + nd.amount_tie * (tie - win + rs) + nd.amount_lose * (tot - tie);
+            v = aw * win + nd.amount_tie * (tie - win + rs) + al * (tot - tie);
           }
         } else {
           const uint32_t si = t.w >> 16;
           const float rs = si != 0xFFFF ? rch[si] : 0.f;
           const float adj = Tsum + rs - M1 - M2;
           if (op.term == TERM_FOLD) {
-            v = __fmul_rn(op.fold_pl != p ? nd.amount_win : nd.amount_lose, adj);
+            v = __fmul_rn(op.fold_pl != p ? aw : al, adj);
           } else {
             const float bv = sp.bcfv[((size_t)nd.boundary * 2 + p) * c.vstride + h];
             v = __fmul_rn(__fmul_rn(bv, nd.payoff_scale), adj);
@@ -451,6 +394,7 @@ __device__ void term_batch(const Ctx& c, const Op* ops, int n, int p) {
       dst[h] = v;
     }
   }
+  __syncwarp();  // the buffer is free for this warp's next run
 }
 
 // ---------------------------------------------------------------------------
@@ -461,22 +405,28 @@ __device__ void run_pass(const Ctx& c, int p, const Discount dc) {
   const SpotDev& sp = *c.sp;
   const Step* steps = sp.steps[p];
   const Op* ops = sp.ops[p];
+  const uint16_t* groups = sp.groups[p];
   const int o = p ^ 1;
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int s = 0; s < sp.nsteps[p]; ++s) {
     const Step st = steps[s];
-    for (int i = 0; i < st.n_elem; ++i) {
-      const Op op = ops[st.begin + i];
-      switch (op.type) {
-        case OP_FWD_OPP: op_fwd_opp<MODE>(c, op, o); break;
-        case OP_FWD_CHANCE: op_fwd_chance(c, op, o); break;
-        case OP_BWD_TRAV: op_bwd_trav<MODE>(c, op, p, dc); break;
-        case OP_BWD_OPP: op_bwd_opp<MODE>(c, op, p); break;
-        case OP_BWD_CHANCE: op_bwd_chance<MODE>(c, op, p); break;
-        default: break;
+    const int items = st.n_groups + st.n_elem;  // terminal runs first: they are the longest items
+    for (int it = warp; it < items; it += nw) {
+      if (it < st.n_groups) {
+        const Op* lead = ops + st.begin + st.n_elem + groups[st.gbegin + it];
+        warp_terms(c, lead, lead->na, p);
+      } else {
+        const Op op = ops[st.begin + (it - st.n_groups)];
+        switch (op.type) {
+          case OP_FWD_OPP: op_fwd_opp<MODE>(c, op, o); break;
+          case OP_FWD_CHANCE: op_fwd_chance(c, op, o); break;
+          case OP_BWD_TRAV: op_bwd_trav<MODE>(c, op, p, dc); break;
+          case OP_BWD_OPP: op_bwd_opp<MODE>(c, op, p); break;
+          case OP_BWD_CHANCE: op_bwd_chance<MODE>(c, op, p); break;
+          default: break;
+        }
       }
     }
-    for (int i = 0; i < st.n_term; i += c.kt)
-      term_batch(c, ops + st.begin + st.n_elem + i, min(c.kt, st.n_term - i), p);
     __syncthreads();
   }
 }
@@ -532,19 +482,14 @@ __device__ bool bind_ctx(Ctx& c, const SpotDev* sp, float* scratch, size_t scrat
                          const SmemPlan plan, int* err) {
   c.sp = sp;
   c.vstride = sp->vstride;
-  c.kt = plan.kt;
   c.slots = scratch;
   char* p = smem;
   const int tb = table_bytes_for(sp->hs[0], sp->hs[1]);
   const bool staged = sp->num_boards == 1 && tb <= plan.tables;
   char* tables = p;
   p += plan.tables;
-  c.rch = reinterpret_cast<float*>(p);
-  p += (size_t)plan.kt * plan.vstride * 4;
-  c.buf = reinterpret_cast<float*>(p);
-  p += (size_t)plan.kt * 3 * plan.vstride * 4;
-  c.carry = reinterpret_cast<float*>(p);
-  p += (size_t)plan.kt * 64 * 4;
+  c.buf = reinterpret_cast<float*>(p) + (size_t)(threadIdx.x >> 5) * 3 * plan.vstride;
+  p += (size_t)plan.warps * 3 * plan.vstride * 4;
   c.red = reinterpret_cast<double*>(p);
   if ((size_t)sp->num_slots * sp->vstride > scratch_floats || sp->vstride > plan.vstride) {
     if (threadIdx.x == 0) atomicOr(err, ERR_SCRATCH);
@@ -687,7 +632,8 @@ __global__ void k_eval_terminal(const SpotDev* __restrict__ spots, Op op, int pl
   Ctx c;
   if (!bind_ctx(c, &spots[0], scratch, scratch_floats, smem, plan, err)) return;
   c.root_reach = nullptr;
-  term_batch(c, &op, 1, player);
+  op.na = 1;
+  if (threadIdx.x < 32) warp_terms(c, &op, 1, player);
 }
 
 // ---------------------------------------------------------------------------

@@ -17,14 +17,16 @@ __host__ __device__ inline int table_bytes_for(int hs0, int hs1) {
   return (b + 15) & ~15;
 }
 
-// Shared-memory plan of one solve CTA (computed on the host per launch).
+// Shared-memory plan of one solve CTA (computed on the host per launch): one
+// terminal scan buffer (3 * vstride floats) per warp, optional staged board
+// tables, and a small reduction area.
 struct SmemPlan {
   int vstride;  // max slot stride of the launch (floats)
   int hs_max;   // max padded hand count
-  int kt;       // terminals evaluated per batch
+  int warps;    // warps per CTA (one scan buffer each)
   int tables;   // bytes reserved for staged board tables (0 = tables stay in global memory)
   __host__ __device__ size_t total() const {
-    return (size_t)tables + (size_t)kt * (4 * vstride + 64) * 4 + 32 * 8;
+    return (size_t)tables + (size_t)warps * 3 * vstride * 4 + 32 * 8;
   }
 };
 

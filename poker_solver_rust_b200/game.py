@@ -408,7 +408,8 @@ class BatchSolver:
     datagen, crates/cfvnet/src/datagen/domain/pipeline.rs:232-343)."""
 
     def __init__(self, card_configs: Sequence[CardConfig], tree_configs: Sequence[TreeConfig],
-                 block_threads: int = 0, ctas_per_sm: int = 0, sort_by_cost: bool = True):
+                 block_threads: int = 0, ctas_per_sm: int = 0, sort_by_cost: bool = True,
+                 stage_tables: int = -1):
         n = len(card_configs)
         cc = (N.PsCardConfig * n)()
         tc = (N.PsTreeConfig * n)()
@@ -419,7 +420,7 @@ class BatchSolver:
             keep.append((c._keep, t._keep))
             cc[i] = c
             tc[i] = t
-        opts = N.PsBatchOpts(block_threads, ctas_per_sm, int(sort_by_cost), 0)
+        opts = N.PsBatchOpts(block_threads, ctas_per_sm, int(sort_by_cost), stage_tables)
         h = C.c_void_p()
         N.check(N.lib().ps_batch_new(cc, tc, n, C.byref(opts), C.byref(h)))
         self._h = h
