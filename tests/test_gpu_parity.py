@@ -314,6 +314,16 @@ def test_root_cfvalues_with_reach():
 
 
 def test_batch_matches_single_and_oracle():
+    """Batch == single game bit for bit; the state the batch stops in is a state
+    of the oracle's map.
+
+    Whole trajectories are not compared here: on datagen spots the oracle's own
+    FP32 and FP64 builds part ways by whole multiples of the exploitability
+    within 60 iterations (regret-matching ties), so the stopping iteration is
+    compared only as a report.  Instead the oracle is seeded with the GPU's
+    final regrets and strategy sums: both must then agree on the exploitability
+    and on one further iteration, pass by pass.
+    """
     sp = spots.datagen_spots(6, seed=21)
     cc = [spots.card_config(r, b) for r, b, _ in sp]
     tcs = [t for _, _, t in sp]
@@ -324,13 +334,42 @@ def test_batch_matches_single_and_oracle():
     rows = []
     for i, (r, b, t) in enumerate(sp):
         g = spots.product_game(r, b, t)
-        es = ps.solve(g, 300, float(targets[i]))
-        assert es == e[i] and g.last_iterations == it[i]  # same kernels, same arithmetic
+        assert ps.solve(g, 300, float(targets[i])) == e[i] and g.last_iterations == it[i]  # same arithmetic
+        assert e[i] <= targets[i] or it[i] == 300
+        # the same solve step by step, stopped before finalize so that its
+        # regrets and strategy sums can be handed to the oracle
+        g = spots.product_game(r, b, t)
+        es, k = ps.compute_exploitability(g), 0
+        while k < 300 and not es <= targets[i]:
+            ps.solve_step(g, k)
+            k += 1
+            if k % 5 == 0 or k == 300:
+                es = ps.compute_exploitability(g)
+        assert es == e[i] and k == it[i]
         o = spots.oracle_game(r, b, t)
         eo = o.solve(300, float(targets[i]))
-        rows.append({"gpu": float(e[i]), "oracle": eo, "it": int(it[i]), "it_o": o.iterations_run})
-        assert abs(int(it[i]) - o.iterations_run) <= 5, rows[-1]
-        assert _expl_close(float(e[i]), eo, t.starting_pot) or (e[i] <= targets[i] and eo <= targets[i]), rows[-1]
+        row = {"gpu": float(e[i]), "oracle": eo, "it": int(it[i]), "it_o": o.iterations_run}
+        o2 = spots.oracle_game(r, b, t)
+        for n in range(g.num_nodes()):
+            info = g.node_info(n)
+            if not info["player"] & (4 | 8):
+                o2.seed_node_storage(n, 1, g.node_storage(n, 1))
+                o2.seed_node_storage(n, 2, g.node_storage(n, 2))
+        row["oracle_at_gpu_state"] = o2.compute_exploitability()
+        assert abs(row["oracle_at_gpu_state"] - es) <= TOL_EVAL_REL * max(abs(es), 1e-3 * t.starting_pot), row
+        ps.solve_step(g, k)
+        o2.solve_pass(k, 0)
+        dr0, ds0 = _state_diff(g, o2, player=0)
+        for n in range(g.num_nodes()):
+            info = g.node_info(n)
+            if not info["player"] & (4 | 8) and info["player"] == 0:
+                o2.seed_node_storage(n, 1, g.node_storage(n, 1))
+                o2.seed_node_storage(n, 2, g.node_storage(n, 2))
+        o2.solve_pass(k, 1)
+        dr1, ds1 = _state_diff(g, o2, player=1)
+        row["next_step_rel"] = max(dr0, ds0, dr1, ds1)
+        rows.append(row)
+        assert row["next_step_rel"] <= TOL_STEP_REL, row
     _report("batch", rows)
 
 
