@@ -77,6 +77,21 @@ int ps_last_iterations(ps_game* g, uint32_t* out);
 int ps_solve_step(ps_game* g, uint32_t current_iteration);
 /* compute_exploitability (utility.rs:380), chips */
 int ps_compute_exploitability(ps_game* g, float* out);
+/* No counterpart in the reference.  The same value as
+ * ps_compute_exploitability, for callers that cannot allocate device memory
+ * when they call it (an engine that hands plug-ins a fixed share of GPU memory
+ * reserved at start-up, or a latency-bound thread that must not take
+ * cudaMalloc's implicit device synchronisation): it allocates nothing and uses
+ * a fixed 16 MiB device array of the library for its working slots.  Games
+ * whose slots need more than that (4 Mi floats = num_slots x slot stride) get
+ * PS_ERR_INVALID: river trees fit with room to spare, turn trees usually do
+ * not (every river subtree is live at once; 100bb turn trees with one or two
+ * sizes need 10-15 Mi floats) and stay on ps_compute_exploitability.  The
+ * first call on a device looks the array up, so make it before any stream
+ * capture on that device.  All calls share the one array: calls whose kernels overlap on the
+ * GPU (different games on different streams or threads) race and must be
+ * serialised by the caller. */
+int ps_compute_exploitability_noalloc(ps_game* g, float* out);
 /* finalize (utility.rs:348) */
 int ps_finalize(ps_game* g);
 /* root_cfvalues_with_reach (utility.rs:422); opp_reach NULL = initial weights (root_cfvalues, :407) */

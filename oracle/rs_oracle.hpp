@@ -7,8 +7,9 @@
 // reference's HAND_TABLE (crates/range-solver/src/hand_table.rs, by digest) and
 // its exhaustive test (hand.rs:407-449); discount parameters against
 // solver.rs:688-722; action lists against examples/basic.rs:101-116.  No golden
-// strategy / CFV values exist in the reference, so numeric parity of the
-// solve itself rests on this line-by-line restatement.
+// strategy / CFV values exist in the reference and the Rust reference cannot
+// be built here, so the solve's floating-point results are parity unpinned:
+// they rest on this line-by-line restatement of the cited code.
 //
 // The scalar type F is float for the parity build (same rounding sequence as
 // the reference's f32 vectors with f64 accumulators) and double for the FP64

@@ -78,6 +78,7 @@ _sig("ps_solve", i32, vp, u32, f32, i32, P(f32))
 _sig("ps_last_iterations", i32, vp, P(u32))
 _sig("ps_solve_step", i32, vp, u32)
 _sig("ps_compute_exploitability", i32, vp, P(f32))
+_sig("ps_compute_exploitability_noalloc", i32, vp, P(f32))
 _sig("ps_finalize", i32, vp)
 _sig("ps_root_cfvalues_with_reach", i32, vp, i32, P(f32), P(f32))
 _sig("ps_num_private_hands", i32, vp, i32)

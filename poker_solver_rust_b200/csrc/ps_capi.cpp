@@ -659,6 +659,24 @@ int ps_compute_exploitability(ps_game* G, float* out) {
   return PS_OK;
 }
 
+int ps_compute_exploitability_noalloc(ps_game* G, float* out) {
+  if (!G || !out) return fail(PS_ERR_INVALID, "null argument");
+  if (G->state == GState::TreeBuilt) return fail(PS_ERR_STATE, "Game is not ready");
+  int rc = need_boundaries(G);
+  if (rc) return rc;
+  const size_t need = (size_t)G->g->num_slots * G->g->vstride;
+  if (need > kFixedScratchFloats)
+    return fail(PS_ERR_INVALID, "game needs " + std::to_string(need) + " floats of working slots; the fixed array of "
+                                    "the no-allocation path holds " + std::to_string(kFixedScratchFloats));
+  Batch& B = *G->b;
+  float e = 0;
+  int err = 0;
+  CU(launch_exploitability_fixed(B.d_spots, need, B.block, B.plan, B.stream, &e, &err));
+  if (err) return fail(PS_ERR_DEVICE, "kernel error flag " + std::to_string(err));
+  *out = e;
+  return PS_OK;
+}
+
 int ps_finalize(ps_game* G) {
   int rc = need_ready(G);
   if (rc) return rc;

@@ -22,6 +22,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "ps_device.hpp"
 #include "ps_handeval.hpp"
 #include "ps_launch.hpp"
@@ -896,6 +898,65 @@ cudaError_t launch_eval_terminal(const SpotDev* spots, Op op, int player, float*
   if (e != cudaSuccess) return e;
   k_eval_terminal<<<1, block, smem, s>>>(spots, op, player, scratch, scratch_floats, plan, err);
   return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Exploitability without allocation
+// ---------------------------------------------------------------------------
+// Some hosts cannot allocate device memory at the moment they evaluate a game:
+// an engine that reserves the GPU's memory for its own pool at start-up and
+// lets plug-ins use only what they were given, or a caller on a latency-bound
+// thread where cudaMalloc's implicit device synchronisation is not allowed.
+// For them the working slots of the exploitability kernel live in this fixed
+// array, sized once at build time: a 256-byte header (word 0 the result, word
+// 1 the kernel's error flag) followed by kFixedScratchFloats floats of slots.
+static __device__ __align__(256) float g_fixed_scratch[kFixedScratchHeader + kFixedScratchFloats];
+
+static std::mutex g_fixed_mu;
+static float* g_fixed_base[64];  // per device ordinal, looked up once
+
+// Looks the array up for the current device on its first use there.
+static cudaError_t fixed_scratch_base(float** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_fixed_mu);
+  if (!g_fixed_base[dev]) {
+    float* p = nullptr;
+    e = cudaGetSymbolAddress((void**)&p, g_fixed_scratch);
+    if (e != cudaSuccess) return e;
+    g_fixed_base[dev] = p;
+  }
+  *out = g_fixed_base[dev];
+  return cudaSuccess;
+}
+
+cudaError_t launch_exploitability_fixed(const SpotDev* spot, size_t slot_floats, int block, const SmemPlan& plan,
+                                        cudaStream_t s, float* host_out, int* host_err) {
+  if (slot_floats > kFixedScratchFloats) return cudaErrorInvalidValue;
+  float* base = nullptr;
+  cudaError_t e = fixed_scratch_base(&base);
+  if (e != cudaSuccess) return e;
+  // the header keeps the previous call's result and flag: clear it; the
+  // slots need no clearing, every pass writes a slot before reading it
+  e = cudaMemsetAsync(base, 0, kFixedScratchHeader * sizeof(float), s);
+  if (e != cudaSuccess) return e;
+  size_t smem = plan.total();
+  e = set_smem((const void*)k_exploitability, smem);
+  if (e != cudaSuccess) return e;
+  k_exploitability<<<1, block, smem, s>>>(spot, 1, base + kFixedScratchHeader, slot_floats, base, plan,
+                                          reinterpret_cast<int*>(base + 1));
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  float head[2];
+  e = cudaMemcpyAsync(head, base, sizeof(head), cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
+  *host_out = head[0];
+  __builtin_memcpy(host_err, &head[1], sizeof(int));
+  return cudaSuccess;
 }
 
 int solve_occupancy(int block, const SmemPlan& plan) {

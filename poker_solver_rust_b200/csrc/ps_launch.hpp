@@ -47,4 +47,16 @@ cudaError_t launch_average(const SpotDev* spots, int nspots, int save, int playe
                            const SmemPlan& plan, cudaStream_t s);
 cudaError_t launch_eval_terminal(const SpotDev* spots, Op op, int player, float* scratch, size_t scratch_floats,
                                  int* err, int block, const SmemPlan& plan, cudaStream_t s);
+
+// Exploitability of one game with its working slots in a fixed, statically
+// sized device array instead of allocated memory.  The array holds a 256-byte
+// header (result and error flag) and kFixedScratchFloats floats of slots
+// (16 MiB); a game needs num_slots * vstride of them.  The first call on a
+// device looks up the array's address (cudaGetSymbolAddress) with that device
+// current.  Every call uses the same array: calls whose kernels overlap on
+// the GPU overwrite each other's slots.
+constexpr size_t kFixedScratchHeader = 64;
+constexpr size_t kFixedScratchFloats = (size_t)4 << 20;
+cudaError_t launch_exploitability_fixed(const SpotDev* spot, size_t slot_floats, int block, const SmemPlan& plan,
+                                        cudaStream_t s, float* host_out, int* host_err);
 }  // namespace ps
