@@ -88,9 +88,9 @@ int ps_compute_exploitability(ps_game* g, float* out);
  * not (every river subtree is live at once; 100bb turn trees with one or two
  * sizes need 10-15 Mi floats) and stay on ps_compute_exploitability.  The
  * first call on a device looks the array up, so make it before any stream
- * capture on that device.  All calls share the one array: calls whose kernels overlap on the
- * GPU (different games on different streams or threads) race and must be
- * serialised by the caller. */
+ * capture on that device.  All calls share the one array: calls whose kernels
+ * overlap on the GPU (different games on different streams or threads) race
+ * and must be serialised by the caller. */
 int ps_compute_exploitability_noalloc(ps_game* g, float* out);
 /* finalize (utility.rs:348) */
 int ps_finalize(ps_game* g);
@@ -149,7 +149,7 @@ int ps_state_import(ps_game* g, const void* buf, uint64_t size);
  *      crates/gpu-range-solver/src/batch.rs:79-610) ---- */
 typedef struct ps_batch ps_batch;
 typedef struct ps_batch_opts {
-  int32_t block_threads;  /* threads per CTA, a multiple of 32 up to 256 (0 = default 256) */
+  int32_t block_threads;  /* threads per CTA, a multiple of 32 up to 256 (0 = default 128) */
   int32_t ctas_per_sm;    /* 0 = as many as fit */
   int32_t sort_by_cost;   /* 1 = hand out the largest spots first */
   int32_t stage_tables;   /* 1 = copy a spot's board tables to shared memory, 0 = read them

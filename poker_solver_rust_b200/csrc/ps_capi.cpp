@@ -319,7 +319,7 @@ struct Batch {
       hs_max = std::max(hs_max, std::max(gp->hs[0], gp->hs[1]));
       single_board &= gp->boards.size() == 1;
     }
-    block = opts && opts->block_threads > 0 ? opts->block_threads : 256;
+    block = opts && opts->block_threads > 0 ? opts->block_threads : 128;
     block = std::max(64, std::min(256, (block / 32) * 32));
     const int stage = opts ? opts->stage_tables : -1;
     plan.vstride = max_vstride;

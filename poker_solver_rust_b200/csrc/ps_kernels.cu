@@ -106,11 +106,10 @@ __device__ __forceinline__ float warp_incl_scan(float x, int lane) {
 // sigma from regret matching (DCFR) or from the normalised cumulative strategy,
 // then children's reach = sigma_a * reach.  Two sweeps over the actions: the
 // first forms the denominator, the second (L1 hits) the children.
-template <int MODE>
-__device__ void op_fwd_opp(const Ctx& c, const Op& op, int o) {
+__device__ __noinline__ void op_fwd_opp(const Ctx& c, const Op& op, int o, int mode) {
   const SpotDev& sp = *c.sp;
   const int hso = sp.hs[o], na = op.na, q4 = hso >> 2;
-  const float* base = (MODE == M_DCFR ? sp.R : sp.S) + sp.nodes[op.node].rs_off;
+  const float* base = (mode == M_DCFR ? sp.R : sp.S) + sp.nodes[op.node].rs_off;
   const float* src = slot_in(c, op.src);
   float* dst = slot_at(c, op.blk);
   const float def = 1.0f / (float)na;
@@ -119,20 +118,20 @@ __device__ void op_fwd_opp(const Ctx& c, const Op& op, int o) {
     float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int a = 0; a < na; ++a) {
       float4 x = ld4(base + a * hso + h);
-      if (MODE == M_DCFR) x = max0(x);
+      if (mode == M_DCFR) x = max0(x);
       d = a == 0 ? x : add4(d, x);
     }
     const float4 r = ld4(src + h);
     for (int a = 0; a < na; ++a) {
       float4 x = ld4(base + a * hso + h);
-      if (MODE == M_DCFR) x = max0(x);
+      if (mode == M_DCFR) x = max0(x);
       st4(dst + (size_t)a * c.vstride + h, mul4(sigma4(x, d, def), r));
     }
   }
 }
 
 // Chance node (solver.rs:264-276): one scaled reach shared by all children.
-__device__ void op_fwd_chance(const Ctx& c, const Op& op, int o) {
+__device__ __noinline__ void op_fwd_chance(const Ctx& c, const Op& op, int o) {
   const SpotDev& sp = *c.sp;
   const int q4 = sp.hs[o] >> 2;
   const float f = __fdiv_rn(1.0f, (float)sp.nodes[op.node].chance_factor);
@@ -153,8 +152,7 @@ __device__ void op_fwd_chance(const Ctx& c, const Op& op, int o) {
 //   AVG  (utility.rs:689-727): sigma = S / sum S; cfv = sum sigma_a cfv_a; SAVE stores cfv_a.
 // Three sweeps over the actions (denominator, result + S, regrets) keep the
 // per-thread state to a few float4 registers; repeated loads hit L1.
-template <int MODE>
-__device__ void op_bwd_trav(const Ctx& c, const Op& op, int p, const Discount dc) {
+__device__ __noinline__ void op_bwd_trav(const Ctx& c, const Op& op, int p, const Discount dc, int mode) {
   const SpotDev& sp = *c.sp;
   const int hsp = sp.hs[p], na = op.na, q4 = hsp >> 2;
   const NodeDev& nd = sp.nodes[op.node];
@@ -166,32 +164,32 @@ __device__ void op_bwd_trav(const Ctx& c, const Op& op, int p, const Discount dc
   for (int q = (threadIdx.x & 31); q < q4; q += 32) {
     const int h = q << 2;
     float4 res = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (MODE == M_BR) {
+    if (mode == M_BR) {
       res = ld4(cb + h);
       for (int a = 1; a < na; ++a) res = max4(res, ld4(cb + (size_t)a * c.vstride + h));
     } else {
-      const float* W = MODE == M_DCFR ? R : S;
+      const float* W = mode == M_DCFR ? R : S;
       float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
       for (int a = 0; a < na; ++a) {
         float4 x = ld4(W + a * hsp + h);
-        if (MODE == M_DCFR) x = max0(x);
+        if (mode == M_DCFR) x = max0(x);
         d = a == 0 ? x : add4(d, x);
       }
       for (int a = 0; a < na; ++a) {
         float4 x = ld4(W + a * hsp + h);
-        if (MODE == M_DCFR) x = max0(x);
+        if (mode == M_DCFR) x = max0(x);
         const float4 s = sigma4(x, d, def);
         const float4 cv = ld4(cb + (size_t)a * c.vstride + h);
         const float4 t = mul4(s, cv);
         res = a == 0 ? t : add4(res, t);
-        if (MODE == M_DCFR) {
+        if (mode == M_DCFR) {
           const float4 g = make_float4(dc.gamma, dc.gamma, dc.gamma, dc.gamma);
           st4(S + a * hsp + h, add4(mul4(ld4(S + a * hsp + h), g), s));
-        } else if (MODE == M_AVG_SAVE) {
+        } else if (mode == M_AVG_SAVE) {
           st4(R + a * hsp + h, cv);
         }
       }
-      if (MODE == M_DCFR) {
+      if (mode == M_DCFR) {
         for (int a = 0; a < na; ++a) {
           const float4 r = ld4(R + a * hsp + h);
           const float4 cv = ld4(cb + (size_t)a * c.vstride + h);
@@ -203,7 +201,7 @@ __device__ void op_bwd_trav(const Ctx& c, const Op& op, int p, const Discount dc
       }
     }
     st4(dst + h, res);
-    if (MODE == M_AVG_SAVE && p == 1 && nd.ip_off != 0xFFFFFFFFu) {
+    if (mode == M_AVG_SAVE && p == 1 && nd.ip_off != 0xFFFFFFFFu) {
       const float v[4] = {res.x, res.y, res.z, res.w};
       for (int k = 0; k < 4; ++k)
         if (h + k < sp.H[1]) sp.ipcfv[nd.ip_off + h + k] = v[k];
@@ -212,8 +210,7 @@ __device__ void op_bwd_trav(const Ctx& c, const Op& op, int p, const Discount dc
 }
 
 // Opponent decision node: cfv = sum_a cfv_a (solver.rs:471).
-template <int MODE>
-__device__ void op_bwd_opp(const Ctx& c, const Op& op, int p) {
+__device__ __noinline__ void op_bwd_opp(const Ctx& c, const Op& op, int p, int mode) {
   const SpotDev& sp = *c.sp;
   const int q4 = sp.hs[p] >> 2, na = op.na;
   const NodeDev& nd = sp.nodes[op.node];
@@ -224,7 +221,7 @@ __device__ void op_bwd_opp(const Ctx& c, const Op& op, int p) {
     float4 res = ld4(cb + h);
     for (int a = 1; a < na; ++a) res = add4(res, ld4(cb + (size_t)a * c.vstride + h));
     st4(dst + h, res);
-    if (MODE == M_AVG_SAVE && p == 1 && nd.ip_off != 0xFFFFFFFFu) {
+    if (mode == M_AVG_SAVE && p == 1 && nd.ip_off != 0xFFFFFFFFu) {
       const float v[4] = {res.x, res.y, res.z, res.w};
       for (int k = 0; k < 4; ++k)
         if (h + k < sp.H[1]) sp.ipcfv[nd.ip_off + h + k] = v[k];
@@ -234,8 +231,7 @@ __device__ void op_bwd_opp(const Ctx& c, const Op& op, int p) {
 
 // Chance node: cfv = sum over dealt cards, plus the suit-swapped rows of the
 // isomorphic cards that were not dealt (solver.rs:291-325).
-template <int MODE>
-__device__ void op_bwd_chance(const Ctx& c, const Op& op, int p) {
+__device__ __noinline__ void op_bwd_chance(const Ctx& c, const Op& op, int p, int mode) {
   const SpotDev& sp = *c.sp;
   const int hsp = sp.hs[p], na = op.na;
   const NodeDev& nd = sp.nodes[op.node];
@@ -255,7 +251,7 @@ __device__ void op_bwd_chance(const Ctx& c, const Op& op, int p) {
       res = __fadd_rn(res, cb[(size_t)ref * c.vstride + hh]);
     }
     dst[h] = res;
-    if (MODE == M_AVG_SAVE && nd.ch_player == p && h < sp.H[p]) sp.chcfv[nd.ch_off + h] = res;
+    if (mode == M_AVG_SAVE && nd.ch_player == p && h < sp.H[p]) sp.chcfv[nd.ch_off + h] = res;
   }
 }
 
@@ -294,7 +290,7 @@ __device__ __forceinline__ void board_tables(const Ctx& c, int b, Tables& t) {
 // scanned as one segmented inclusive scan, 128 entries per row (four per
 // lane), the running value carried from row to row; segment starts come from
 // the per-board bitmap.  The lookups then read the scan from shared memory.
-__device__ void warp_terms(const Ctx& c, const Op* ops, int n, int p) {
+__device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int p) {
   const SpotDev& sp = *c.sp;
   const int o = p ^ 1;
   const int Hp = sp.H[p], hsp = sp.hs[p];
@@ -402,8 +398,7 @@ __device__ void warp_terms(const Ctx& c, const Op* ops, int n, int p) {
 // ---------------------------------------------------------------------------
 // Pass driver and root reductions
 // ---------------------------------------------------------------------------
-template <int MODE>
-__device__ void run_pass(const Ctx& c, int p, const Discount dc) {
+__device__ __noinline__ void run_pass(const Ctx& c, int p, const Discount dc, int mode) {
   const SpotDev& sp = *c.sp;
   const Step* steps = sp.steps[p];
   const Op* ops = sp.ops[p];
@@ -420,11 +415,11 @@ __device__ void run_pass(const Ctx& c, int p, const Discount dc) {
       } else {
         const Op op = ops[st.begin + (it - st.n_groups)];
         switch (op.type) {
-          case OP_FWD_OPP: op_fwd_opp<MODE>(c, op, o); break;
+          case OP_FWD_OPP: op_fwd_opp(c, op, o, mode); break;
           case OP_FWD_CHANCE: op_fwd_chance(c, op, o); break;
-          case OP_BWD_TRAV: op_bwd_trav<MODE>(c, op, p, dc); break;
-          case OP_BWD_OPP: op_bwd_opp<MODE>(c, op, p); break;
-          case OP_BWD_CHANCE: op_bwd_chance<MODE>(c, op, p); break;
+          case OP_BWD_TRAV: op_bwd_trav(c, op, p, dc, mode); break;
+          case OP_BWD_OPP: op_bwd_opp(c, op, p, mode); break;
+          case OP_BWD_CHANCE: op_bwd_chance(c, op, p, mode); break;
           default: break;
         }
       }
@@ -457,14 +452,14 @@ __device__ float spot_exploitability(Ctx& c) {
   float mes[2];
   for (int p = 0; p < 2; ++p) {
     c.root_reach = sp.w[p ^ 1];
-    run_pass<M_BR>(c, p, dz);
+    run_pass(c, p, dz, M_BR);
     mes[p] = (float)block_dot_f64(c, sp.w[p], slot_at(c, sp.root_slot[p]), sp.H[p]);
   }
   if (!sp.raked) return (mes[0] + mes[1]) * 0.5f;
   float cur[2];
   for (int p = 0; p < 2; ++p) {
     c.root_reach = sp.w[p ^ 1];
-    run_pass<M_AVG>(c, p, dz);
+    run_pass(c, p, dz, M_AVG);
     cur[p] = (float)block_dot_f64(c, sp.w[p], slot_at(c, sp.root_slot[p]), sp.H[p]);
   }
   return ((mes[0] - cur[0]) + (mes[1] - cur[1])) * 0.5f;
@@ -474,7 +469,7 @@ __device__ void dcfr_iteration(Ctx& c, const Discount dc) {
   const SpotDev& sp = *c.sp;
   for (int p = 0; p < 2; ++p) {  // alternating updates (solver.rs:144-155)
     c.root_reach = sp.w[p ^ 1];
-    run_pass<M_DCFR>(c, p, dc);
+    run_pass(c, p, dc, M_DCFR);
   }
 }
 
@@ -613,11 +608,11 @@ __global__ void PS_SOLVE_BOUNDS k_average(const SpotDev* __restrict__ spots, int
     if (save) {
       for (int p = 0; p < 2; ++p) {
         c.root_reach = sp.w[p ^ 1];
-        run_pass<M_AVG_SAVE>(c, p, dz);
+        run_pass(c, p, dz, M_AVG_SAVE);
       }
     } else {
       c.root_reach = root_reach ? root_reach : sp.w[player ^ 1];
-      run_pass<M_AVG>(c, player, dz);
+      run_pass(c, player, dz, M_AVG);
       const float* r = slot_at(c, sp.root_slot[player]);
       for (int h = threadIdx.x; h < sp.H[player]; h += blockDim.x) out[(size_t)si * sp.hs[player] + h] = r[h];
     }
