@@ -98,6 +98,22 @@ __device__ __forceinline__ float warp_incl_scan(float x, int lane) {
   return x;
 }
 
+// Asks L2 for the n floats at p, one 128-byte line per lane at a time, without
+// waiting: an op issues this for every row it will stream before its first
+// load, so its dependent loop iterations find the rows in L2 instead of each
+// paying a DRAM round trip.
+#ifndef PS_PREFETCH
+#define PS_PREFETCH 1
+#endif
+__device__ __forceinline__ void prefetch_l2_bytes(const void* p, int bytes) {
+#if PS_PREFETCH
+  const char* b = static_cast<const char*>(p);
+  for (int i = (threadIdx.x & 31) * 128; i < bytes; i += 32 * 128)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(__cvta_generic_to_global(b + i)));
+#endif
+}
+__device__ __forceinline__ void prefetch_l2(const float* p, int n) { prefetch_l2_bytes(p, 4 * n); }
+
 // ---------------------------------------------------------------------------
 // Forward ops
 // ---------------------------------------------------------------------------
@@ -113,6 +129,7 @@ __device__ __noinline__ void op_fwd_opp(const Ctx& c, const Op& op, int o, int m
   const float* src = slot_in(c, op.src);
   float* dst = slot_at(c, op.blk);
   const float def = 1.0f / (float)na;
+  prefetch_l2(base, na * hso);
   for (int q = (threadIdx.x & 31); q < q4; q += 32) {
     const int h = q << 2;
     float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -161,6 +178,11 @@ __device__ __noinline__ void op_bwd_trav(const Ctx& c, const Op& op, int p, cons
   const float* cb = slot_at(c, op.blk);
   float* dst = slot_at(c, op.dst);
   const float def = 1.0f / (float)na;
+  if (mode != M_BR) {
+    prefetch_l2(mode == M_DCFR ? R : S, na * hsp);
+    if (mode == M_DCFR) prefetch_l2(S, na * hsp);
+  }
+  for (int a = 0; a < na; ++a) prefetch_l2(cb + (size_t)a * c.vstride, hsp);
   for (int q = (threadIdx.x & 31); q < q4; q += 32) {
     const int h = q << 2;
     float4 res = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -216,6 +238,7 @@ __device__ __noinline__ void op_bwd_opp(const Ctx& c, const Op& op, int p, int m
   const NodeDev& nd = sp.nodes[op.node];
   const float* cb = slot_at(c, op.blk);
   float* dst = slot_at(c, op.dst);
+  for (int a = 0; a < na; ++a) prefetch_l2(cb + (size_t)a * c.vstride, sp.hs[p]);
   for (int q = (threadIdx.x & 31); q < q4; q += 32) {
     const int h = q << 2;
     float4 res = ld4(cb + h);
@@ -301,6 +324,9 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
   const uint16_t* g = T.gidx[o];
   const uint32_t* hd = T.heads[o];
   const float* rch = slot_in(c, ops[0].src);
+  prefetch_l2_bytes(g, 2 * n3);
+  prefetch_l2_bytes(T.thr[p], 16 * Hp);
+  prefetch_l2(rch, sp.hs[o]);
   float* buf = c.buf;
   float carry = 0.f;
   for (int base = 0; base < n3; base += 128) {
