@@ -38,6 +38,28 @@ constexpr int ERR_SETUP = 2;    // setup tables exceeded their bounds
 
 constexpr uint32_t THR_INVALID = 0xFFFFFFFFu;
 
+// Optional per-phase cycle counters (build with -DPS_PHASE_TIMERS): lane 0 of
+// every warp adds the clock64 cycles it spent in each phase, so the totals
+// split the warps' time between terminal scans and lookups, node ops and
+// barrier waits.  Read and cleared by ps_debug_phase_cycles in such builds.
+enum Phase { PH_SCAN = 0, PH_LOOKUP, PH_FWD_OPP, PH_FWD_CHANCE, PH_BWD_TRAV, PH_BWD_OPP, PH_BWD_CHANCE, PH_BARRIER,
+             PH_ROOT, PH_COUNT };
+#ifdef PS_PHASE_TIMERS
+__device__ unsigned long long g_phase[16];
+#define PHASE_T0(v) const long long v = clock64()
+#define PHASE_ADD(k, v)                                                                           \
+  do {                                                                                            \
+    if ((threadIdx.x & 31) == 0) atomicAdd(&g_phase[k], (unsigned long long)(clock64() - (v))); \
+  } while (0)
+#else
+#define PHASE_T0(v) \
+  do {              \
+  } while (0)
+#define PHASE_ADD(k, v) \
+  do {                  \
+  } while (0)
+#endif
+
 struct Tables {  // board tables of one board, in shared or global memory
   const uint16_t* gidx[2];   // opponent-indexed gather lists
   const uint32_t* heads[2];  // opponent-indexed segment-start bitmaps
@@ -307,13 +329,20 @@ __device__ __forceinline__ void board_tables(const Ctx& c, int b, Tables& t) {
 }
 
 // Evaluates a run of n terminals that read the same reach on the same board,
-// for traverser p, with the calling warp alone.
-//
-// The gather list (3V entries: strength order, then per-card groups) is
-// scanned as one segmented inclusive scan, 128 entries per row (four per
-// lane), the running value carried from row to row; segment starts come from
-// the per-board bitmap.  The lookups then read the scan from shared memory.
+// for traverser p, with the calling warp alone, in three phases whose memory
+// accesses are issued as independent batches:
+//  1. gather: every lane reads four gather indices at a time (16 entries per
+//     batch) and the opponent reach at those indices; a segment start is
+//     stored as -x (reach values are >= +0, so the sign bit flags a start even
+//     for a zero);
+//  2. scan: each lane scans a contiguous chunk of the 3V-entry list of odd
+//     length (the lanes' strided shared-memory accesses then fall in distinct
+//     banks), a segmented warp scan of the chunk totals gives each chunk its
+//     carry-in, and the chunk's entries before its first segment start add it;
+//  3. lookups: per terminal, every hand reads its 16-byte record and its
+//     win / lose / blocked sums at the recorded positions of the scan.
 __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int p) {
+  PHASE_T0(t_scan);
   const SpotDev& sp = *c.sp;
   const int o = p ^ 1;
   const int Hp = sp.H[p], hsp = sp.hs[p];
@@ -324,53 +353,75 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
   const uint16_t* g = T.gidx[o];
   const uint32_t* hd = T.heads[o];
   const float* rch = slot_in(c, ops[0].src);
-  prefetch_l2_bytes(g, 2 * n3);
   prefetch_l2_bytes(T.thr[p], 16 * Hp);
-  prefetch_l2(rch, sp.hs[o]);
   float* buf = c.buf;
-  float carry = 0.f;
-  for (int base = 0; base < n3; base += 128) {
-    const int k = base + 4 * lane;
-    const uint32_t word = k < n3 ? hd[k >> 5] : 0u;
-    const uint32_t f4 = (word >> (k & 31)) & 0xFu;
-    float x0 = k < n3 ? rch[g[k]] : 0.f;
-    float x1 = k + 1 < n3 ? rch[g[k + 1]] : 0.f;
-    float x2 = k + 2 < n3 ? rch[g[k + 2]] : 0.f;
-    float x3 = k + 3 < n3 ? rch[g[k + 3]] : 0.f;
-    x1 = (f4 & 2) ? x1 : x0 + x1;  // in-lane segmented scan
-    x2 = (f4 & 4) ? x2 : x1 + x2;
-    x3 = (f4 & 8) ? x3 : x2 + x3;
-    bool F = f4 != 0;
-    float v = x3;
+  {  // 1. gather
+    const int n4 = (n3 + 3) >> 2;  // groups of four entries
+    for (int w0 = lane; w0 < n4; w0 += 32 * 4) {
+      uint2 ix[4];
+      uint32_t hb[4];
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {  // segmented warp scan of the lane totals
-      const float vv = __shfl_up_sync(0xffffffffu, v, d);
-      const bool ff = __shfl_up_sync(0xffffffffu, (int)F, d) != 0;
-      if (lane >= d) {
-        if (!F) v += vv;
-        F = F || ff;
+      for (int u = 0; u < 4; ++u) {
+        const int w = w0 + 32 * u;
+        ix[u] = w < n4 ? *reinterpret_cast<const uint2*>(g + 4 * w) : make_uint2(0u, 0u);
+        hb[u] = w < n4 ? hd[w >> 3] >> ((4 * w) & 31) : 0u;
+      }
+      float x[4][4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int k = 4 * (w0 + 32 * u);
+        const uint32_t id[4] = {ix[u].x & 0xFFFFu, ix[u].x >> 16, ix[u].y & 0xFFFFu, ix[u].y >> 16};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) x[u][e] = k + e < n3 ? rch[id[e]] : 0.f;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int k = 4 * (w0 + 32 * u);
+        if (k >= n3) continue;
+        float4 v;
+        v.x = (hb[u] & 1u) ? -x[u][0] : x[u][0];
+        v.y = (hb[u] & 2u) ? -x[u][1] : x[u][1];
+        v.z = (hb[u] & 4u) ? -x[u][2] : x[u][2];
+        v.w = (hb[u] & 8u) ? -x[u][3] : x[u][3];
+        st4(buf + k, v);  // entries past n3 are never read
       }
     }
-    float ev = __shfl_up_sync(0xffffffffu, v, 1);  // lanes before this one
-    bool eF = __shfl_up_sync(0xffffffffu, (int)F, 1) != 0;
-    if (lane == 0) {
-      ev = 0.f;
-      eF = false;
-    }
-    const float in = eF ? ev : carry + ev;  // value flowing into this lane's first entry
-    if (!(f4 & 1)) x0 += in;
-    if (!(f4 & 3)) x1 += in;
-    if (!(f4 & 7)) x2 += in;
-    if (!(f4 & 15)) x3 += in;
-    if (k < n3) buf[k] = x0;
-    if (k + 1 < n3) buf[k + 1] = x1;
-    if (k + 2 < n3) buf[k + 2] = x2;
-    if (k + 3 < n3) buf[k + 3] = x3;
-    const float vl = __shfl_sync(0xffffffffu, v, 31);
-    const bool Fl = __shfl_sync(0xffffffffu, (int)F, 31) != 0;
-    carry = Fl ? vl : carry + vl;
   }
   __syncwarp();
+  {  // 2. chunked segmented scan
+    const int C = ((n3 + 31) >> 5) | 1;
+    const int lo = min(lane * C, n3), hi = min(lo + C, n3);
+    float run = 0.f;
+    int first = hi;
+    for (int j = lo; j < hi; ++j) {
+      const float x = buf[j];
+      if (signbit(x)) {
+        run = -x;
+        first = min(first, j);
+      } else {
+        run = __fadd_rn(run, x);
+      }
+      buf[j] = run;
+    }
+    float v = run;
+    bool f = first < hi;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const float vv = __shfl_up_sync(0xffffffffu, v, d);
+      const bool ff = __shfl_up_sync(0xffffffffu, (int)f, d) != 0;
+      if (lane >= d) {
+        if (!f) v = __fadd_rn(v, vv);
+        f = f || ff;
+      }
+    }
+    float in = __shfl_up_sync(0xffffffffu, v, 1);
+    if (lane == 0) in = 0.f;
+    for (int j = lo; j < first; ++j) buf[j] = __fadd_rn(buf[j], in);
+  }
+  __syncwarp();
+  PHASE_ADD(PH_SCAN, t_scan);
+  PHASE_T0(t_look);
+  // 3. lookups
   const uint4* thr = T.thr[p];
   const float* cp = buf + V;  // card-group part
   const float Tsum = V > 0 ? buf[V - 1] : 0.f;
@@ -419,6 +470,7 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
     }
   }
   __syncwarp();  // the buffer is free for this warp's next run
+  PHASE_ADD(PH_LOOKUP, t_look);
 }
 
 // ---------------------------------------------------------------------------
@@ -440,6 +492,7 @@ __device__ __noinline__ void run_pass(const Ctx& c, int p, const Discount dc, in
         warp_terms(c, lead, lead->na, p);
       } else {
         const Op op = ops[st.begin + (it - st.n_groups)];
+        PHASE_T0(t_op);
         switch (op.type) {
           case OP_FWD_OPP: op_fwd_opp(c, op, o, mode); break;
           case OP_FWD_CHANCE: op_fwd_chance(c, op, o); break;
@@ -448,9 +501,17 @@ __device__ __noinline__ void run_pass(const Ctx& c, int p, const Discount dc, in
           case OP_BWD_CHANCE: op_bwd_chance(c, op, p, mode); break;
           default: break;
         }
+        PHASE_ADD(op.type == OP_FWD_OPP      ? PH_FWD_OPP
+                  : op.type == OP_FWD_CHANCE ? PH_FWD_CHANCE
+                  : op.type == OP_BWD_TRAV   ? PH_BWD_TRAV
+                  : op.type == OP_BWD_OPP    ? PH_BWD_OPP
+                                             : PH_BWD_CHANCE,
+                  t_op);
       }
     }
+    PHASE_T0(t_bar);
     __syncthreads();
+    PHASE_ADD(PH_BARRIER, t_bar);
   }
 }
 
@@ -528,13 +589,13 @@ __device__ bool bind_ctx(Ctx& c, const SpotDev* sp, float* scratch, size_t scrat
     __syncthreads();  // the previous spot's users of the staged tables are done
     uint4* thr_s = reinterpret_cast<uint4*>(tables);
     uint32_t* hd_s = reinterpret_cast<uint32_t*>(tables + 16 * (sp->hs[0] + sp->hs[1]));
-    uint16_t* g_s = reinterpret_cast<uint16_t*>(hd_s + head_words(sp->hs[0]) + head_words(sp->hs[1]));
+    uint16_t* g_s = reinterpret_cast<uint16_t*>(hd_s + head_words16(sp->hs[0]) + head_words16(sp->hs[1]));
     for (int q = 0; q < 2; ++q) {
       const int hs = sp->hs[q];
       uint4* ts = thr_s + (q ? sp->hs[0] : 0);
       const uint4* tg = reinterpret_cast<const uint4*>(sp->thr[q]);
       for (int i = threadIdx.x; i < hs; i += blockDim.x) ts[i] = tg[i];
-      uint32_t* hs_ = hd_s + (q ? head_words(sp->hs[0]) : 0);
+      uint32_t* hs_ = hd_s + (q ? head_words16(sp->hs[0]) : 0);
       for (int i = threadIdx.x; i < head_words(hs); i += blockDim.x) hs_[i] = sp->heads[q][i];
       uint16_t* gs = g_s + (q ? 3 * sp->hs[0] : 0);
       for (int i = threadIdx.x; i < 3 * hs; i += blockDim.x) gs[i] = sp->gidx[q][i];
@@ -979,6 +1040,16 @@ cudaError_t launch_exploitability_fixed(const SpotDev* spot, size_t slot_floats,
   __builtin_memcpy(host_err, &head[1], sizeof(int));
   return cudaSuccess;
 }
+
+#ifdef PS_PHASE_TIMERS
+extern "C" int ps_debug_phase_cycles(unsigned long long* out, int n) {
+  unsigned long long z[16] = {};
+  if (n > 16) n = 16;
+  if (cudaMemcpyFromSymbol(out, g_phase, sizeof(unsigned long long) * n) != cudaSuccess) return -3;
+  if (cudaMemcpyToSymbol(g_phase, z, sizeof(z)) != cudaSuccess) return -3;
+  return n;
+}
+#endif
 
 int solve_occupancy(int block, const SmemPlan& plan) {
   int n = 0;

@@ -9,11 +9,13 @@
 namespace ps {
 
 __host__ __device__ inline int head_words(int hs) { return (3 * hs + 31) / 32; }
+// bitmap words rounded up to 16 bytes, so staged gather lists stay 16-byte aligned
+__host__ __device__ inline int head_words16(int hs) { return (head_words(hs) + 3) & ~3; }
 
 // Board tables of one board staged in shared memory: lookup records (16 bytes
-// per hand), gather lists (u16, 3 * hs per player) and segment-start bitmaps.
+// per hand), segment-start bitmaps and gather lists (u16, 3 * hs per player).
 __host__ __device__ inline int table_bytes_for(int hs0, int hs1) {
-  int b = 16 * (hs0 + hs1) + 4 * (head_words(hs0) + head_words(hs1)) + 2 * (3 * hs0 + 3 * hs1);
+  int b = 16 * (hs0 + hs1) + 4 * (head_words16(hs0) + head_words16(hs1)) + 2 * (3 * hs0 + 3 * hs1);
   return (b + 15) & ~15;
 }
 
