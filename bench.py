@@ -25,6 +25,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -102,6 +103,18 @@ class ClockSampler:
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def profiled_traffic_per_spot_iteration():
+    """DRAM read + write bytes per spot-iteration of the committed ncu capture
+    of k_solve (profiles/k_solve_river_datagen_1024.md), or None."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "k_solve_river_datagen_1024.md")
+    try:
+        with open(path) as f:
+            m = re.search(r"^traffic_bytes_per_spot_iteration:\s*([0-9.]+)", f.read(), re.M)
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
 
 
 def make_workload(n_spots: int, seed: int):
@@ -239,6 +252,8 @@ def main():
     kernel_s = statistics.median(solve_ms) / 1e3
     achieved = alg_bytes / kernel_s / 1e9
     peak, peak_kind = _peaks()
+    tps = profiled_traffic_per_spot_iteration()
+    traffic = float(tps * np.sum(iters)) if tps else None
 
     # ---- end to end through the public API (host buffers) ----
     e2e_ms = []
@@ -292,8 +307,10 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": 2 * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-                         "kernel": "k_solve", "alg_bytes_per_launch": alg_bytes},
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                         "kernel": "k_solve", "alg_bytes_per_launch": alg_bytes,
+                         "traffic_note": "DRAM bytes per launch, scaled from the 1024-spot ncu capture by "
+                                         "spot-iterations (profiles/k_solve_river_datagen_1024.md)"},
             "cpu_baseline": cpu,
             "plain_gpu": plain,
             "clocks": clocks,
