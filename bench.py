@@ -117,6 +117,24 @@ def profiled_traffic_per_spot_iteration():
         return None
 
 
+def rank_max(x: float, dist, device: str) -> float:
+    """Max of x over all ranks of the process group (x itself without one).
+    Every rank must call it at the same point: it is a collective."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_throughput(spots_per_rank: int, world: int, step_ms_max: float) -> float:
+    """Whole-job spots/s of `world` independent replicas, each solving
+    spots_per_rank spots per step, timed by the slowest rank."""
+    return world * spots_per_rank / (step_ms_max / 1e3)
+
+
 def make_workload(n_spots: int, seed: int):
     from tests import spots
 
@@ -219,11 +237,7 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(x: float) -> float:
-        if not dist:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(x, dist, "cuda")
 
     bs = ps.BatchSolver(cc, tcs, block_threads=args.block, ctas_per_sm=args.ctas_per_sm, stage_tables=args.stage)
     for _ in range(args.warmup):
@@ -243,7 +257,7 @@ def main():
     clocks = clk.stop()
     step_ms = max_over_ranks(sum(solve_ms) / args.steps + sum(setup_ms) / args.steps)
     expl, iters = bs.results()
-    value = world * args.spots / (step_ms / 1e3)
+    value = replicas_throughput(args.spots, world, step_ms)
 
     # roofline of the persistent solve kernel: algorithmic bytes / kernel time
     sbytes = np.array([bs.iteration_bytes(i) / 20.0 for i in range(args.spots)])
@@ -270,7 +284,7 @@ def main():
         h2d, d2h = b2.io_bytes()
         del b2
     e2e_step = max_over_ranks(statistics.median(e2e_ms)) if e2e_ms else float("nan")
-    e2e_value = world * args.spots / (e2e_step / 1e3) if e2e_ms else None
+    e2e_value = replicas_throughput(args.spots, world, e2e_step) if e2e_ms else None
 
     # ---- plain per-instance GPU path on a sample (one game, one launch per spot) ----
     plain = None
