@@ -97,6 +97,22 @@ int ps_finalize(ps_game* g);
 /* root_cfvalues_with_reach (utility.rs:422); opp_reach NULL = initial weights (root_cfvalues, :407) */
 int ps_root_cfvalues_with_reach(ps_game* g, int player, const float* opp_reach, float* out);
 
+/* ---- fixed-strategy evaluation and its adjoint ----
+ * No counterpart in the reference, which has no gradients.  With the average
+ * strategy held fixed, cfv_p (root cfvalues of player p, the values of
+ * root_cfvalues_with_reach, utility.rs:422) is linear in the opponent's
+ * initial weights and in p's boundary values.  These entry points take the
+ * weights as arguments (solver hand order, H_p values each) instead of the
+ * game's; games with isomorphic chance pruning get PS_ERR_UNSUPPORTED. */
+/* forward: cfv0 = cfv_0(w1, B), cfv1 = cfv_1(w0, B) */
+int ps_eval_fixed_strategy(ps_game* g, const float* w0, const float* w1, float* cfv0, float* cfv1);
+/* vector-Jacobian product for cotangents g0, g1 on cfv0, cfv1 (NULL = zero):
+ * dw0 = g1 . dcfv1/dw0, dw1 = g0 . dcfv0/dw1 (cfv_p does not depend on w_p), and
+ * dbcfv = d(g0 . cfv0 + g1 . cfv1)/dB laid out per boundary ordinal k as
+ * [H0 values for player 0][H1 values for player 1] (NULL = not wanted) */
+int ps_eval_fixed_strategy_adjoint(ps_game* g, const float* w0, const float* w1, const float* g0, const float* g1,
+                                   float* dw0, float* dw1, float* dbcfv);
+
 /* ---- game data (game/mod.rs, interpreter.rs) ---- */
 int ps_num_private_hands(ps_game* g, int player);
 int ps_private_cards(ps_game* g, int player, uint8_t* out_pairs);  /* private_cards(): [H][2] */

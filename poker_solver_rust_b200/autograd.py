@@ -1,0 +1,65 @@
+"""torch.autograd.Function over fixed-strategy evaluation of a solved game.
+
+With the average strategy held fixed, the root cfvalues of each player are
+linear in the opponent's initial weights and in the player's depth-boundary
+values.  `FixedStrategyValues` exposes that map to PyTorch: forward runs the
+C-ABI evaluation (ps_eval_fixed_strategy), backward the hand-written adjoint
+kernels (ps_eval_fixed_strategy_adjoint), so a boundary-value model can be
+trained through a solved depth-limited tree.  Tensors may live on any device;
+the library is called with host copies.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import game as G
+
+
+class FixedStrategyValues(torch.autograd.Function):
+    """(w0, w1, B0, B1) -> (cfv0, cfv1).
+
+    w_p: [H_p] initial weights in solver hand order; B_p: [n_boundary, H_p]
+    boundary values of player p (ps_set_boundary_cfvs); cfv_p: [H_p] root
+    cfvalues of player p under the average strategy.
+    """
+
+    @staticmethod
+    def forward(ctx, game, w0, w1, b0, b1):
+        nb = game.num_boundary_nodes()
+        for k in range(nb):
+            game.set_boundary_cfvs(k, 0, b0[k].detach().cpu().numpy().astype(np.float32))
+            game.set_boundary_cfvs(k, 1, b1[k].detach().cpu().numpy().astype(np.float32))
+        a = w0.detach().cpu().numpy()
+        b = w1.detach().cpu().numpy()
+        c0, c1 = G.eval_fixed_strategy(game, a, b)
+        ctx.game = game
+        ctx.save_for_backward(w0, w1, b0, b1)
+        dev, dt = w0.device, w0.dtype
+        return torch.from_numpy(c0).to(dev, dt), torch.from_numpy(c1).to(dev, dt)
+
+    @staticmethod
+    def backward(ctx, g0, g1):
+        w0, w1, b0, b1 = ctx.saved_tensors
+        game = ctx.game
+        nb = game.num_boundary_nodes()
+        for k in range(nb):  # the values the forward pass saw
+            game.set_boundary_cfvs(k, 0, b0[k].detach().cpu().numpy().astype(np.float32))
+            game.set_boundary_cfvs(k, 1, b1[k].detach().cpu().numpy().astype(np.float32))
+        dw0, dw1, db = G.eval_fixed_strategy_adjoint(
+            game, w0.detach().cpu().numpy(), w1.detach().cpu().numpy(),
+            None if g0 is None else g0.detach().cpu().numpy(), None if g1 is None else g1.detach().cpu().numpy())
+        dev, dt = w0.device, w0.dtype
+        db0 = torch.from_numpy(np.stack([db[k][0] for k in range(nb)]) if nb else np.zeros((0, w0.shape[0]),
+                                                                                           np.float32))
+        db1 = torch.from_numpy(np.stack([db[k][1] for k in range(nb)]) if nb else np.zeros((0, w1.shape[0]),
+                                                                                           np.float32))
+        return (None, torch.from_numpy(dw0).to(dev, dt), torch.from_numpy(dw1).to(dev, dt), db0.to(dev, dt),
+                db1.to(dev, dt))
+
+
+def fixed_strategy_values(game, w0, w1, b0, b1):
+    """Root cfvalues (cfv0, cfv1) of `game` as a differentiable function of
+    the initial weights and boundary values (see FixedStrategyValues)."""
+    return FixedStrategyValues.apply(game, w0, w1, b0, b1)

@@ -255,6 +255,15 @@ struct Batch {
         s.heads[p] = (uint32_t*)(dU + L.heads[p]);
       }
       NodeDev* nd = (NodeDev*)(h_static + L.nodes);
+      // reach scale of every node: the product of the rounded 1 / chance_factor
+      // of the chance nodes above it, in the order the forward sweep applies them
+      std::vector<float> pscale(g.arena.size(), 1.0f);
+      for (size_t k = 0; k < g.arena.size(); ++k) {
+        const ArenaNode& a = g.arena[k];
+        if (a.terminal()) continue;
+        const float f = a.chance() ? (float)(1.0f / (float)g.chance_factor(a)) : 1.0f;
+        for (int ch = 0; ch < a.nch; ++ch) pscale[k + a.child_off + ch] = a.chance() ? pscale[k] * f : pscale[k];
+      }
       for (size_t k = 0; k < g.arena.size(); ++k) {
         const ArenaNode& a = g.arena[k];
         NodeDev& d = nd[k];
@@ -275,6 +284,7 @@ struct Batch {
         d.amount_lose = (float)(-half / g.num_combinations);
         d.amount_tie = (float)(-0.5 * rake / g.num_combinations);
         d.payoff_scale = (float)(half / g.num_combinations);
+        d.path_scale = pscale[k];
       }
       uint8_t* bc = (uint8_t*)(h_static + L.board_cards);
       for (size_t b = 0; b < g.boards.size(); ++b) {
@@ -718,6 +728,75 @@ int ps_root_cfvalues_with_reach(ps_game* G, int player, const float* opp_reach, 
   cudaFree(d_reach);
   cudaFree(d_out);
   return B.check_err();
+}
+
+// Fixed-strategy evaluation and its adjoint (no reference counterpart: the
+// reference has no gradients).  Both passes use the average strategy, the
+// boundary values as set, and the given initial weights instead of the game's.
+static int fixed_strategy_run(ps_game* G, const float* w0, const float* w1, const float* g0, const float* g1,
+                              float* cfv0, float* cfv1, float* dw0, float* dw1, float* dbcfv) {
+  if (!G || !w0 || !w1) return fail(PS_ERR_INVALID, "null argument");
+  if (G->state == GState::TreeBuilt) return fail(PS_ERR_STATE, "Game is not ready");
+  int rc = need_boundaries(G);
+  if (rc) return rc;
+  Batch& B = *G->b;
+  Game& g = *G->g;
+  if (!g.iso_list.empty())
+    return fail(PS_ERR_UNSUPPORTED, "fixed-strategy evaluation with arbitrary weights needs a game without "
+                                    "isomorphic chance pruning (its suit swaps assume the game's own ranges)");
+  const bool adjoint = dw0 || dw1 || dbcfv;
+  const size_t hs0 = g.hs[0], hs1 = g.hs[1], nb = (size_t)g.num_boundary;
+  // one device block: w0 w1 c0 c1 (g0 g1 a0 a1 when adjoint) then the boundary gradients
+  const size_t nvec = adjoint ? 8 : 4;
+  const size_t vec = std::max(hs0, hs1);
+  const size_t nbg = adjoint ? nb * 2 * (size_t)g.vstride : 0;
+  float* d = nullptr;
+  CU(cudaMalloc(&d, 4 * (nvec * vec + nbg + 4)));
+  std::unique_ptr<float, decltype(&cudaFree)> keep(d, &cudaFree);
+  float* dv[8];
+  for (size_t k = 0; k < nvec; ++k) dv[k] = d + k * vec;
+  float* d_bg = nbg ? d + nvec * vec : nullptr;
+  CU(cudaMemsetAsync(d, 0, 4 * (nvec * vec + nbg), B.stream));
+  CU(cudaMemcpyAsync(dv[0], w0, 4 * (size_t)g.H[0], cudaMemcpyHostToDevice, B.stream));
+  CU(cudaMemcpyAsync(dv[1], w1, 4 * (size_t)g.H[1], cudaMemcpyHostToDevice, B.stream));
+  if (adjoint) {
+    if (g0) CU(cudaMemcpyAsync(dv[4], g0, 4 * (size_t)g.H[0], cudaMemcpyHostToDevice, B.stream));
+    if (g1) CU(cudaMemcpyAsync(dv[5], g1, 4 * (size_t)g.H[1], cudaMemcpyHostToDevice, B.stream));
+  }
+  CU(cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream));
+  // forward: cfv_p from the opponent's weights (utility.rs:422-443)
+  CU(launch_average(B.d_spots, 1, 0, 0, dv[1], B.d_scratch, B.scratch_floats, dv[2], B.d_err, 1, B.block, B.plan,
+                    B.stream, -1, d_bg));
+  CU(launch_average(B.d_spots, 1, 0, 1, dv[0], B.d_scratch, B.scratch_floats, dv[3], B.d_err, 1, B.block, B.plan,
+                    B.stream, -1, d_bg));
+  if (adjoint) {
+    // cotangent of cfv_0 flows into player 1's weights and player 0's boundary values, and vice versa
+    CU(launch_average(B.d_spots, 1, 0, 1, dv[4], B.d_scratch, B.scratch_floats, dv[7], B.d_err, 1, B.block, B.plan,
+                      B.stream, 0, d_bg));
+    CU(launch_average(B.d_spots, 1, 0, 0, dv[5], B.d_scratch, B.scratch_floats, dv[6], B.d_err, 1, B.block, B.plan,
+                      B.stream, 1, d_bg));
+  }
+  if (cfv0) CU(cudaMemcpyAsync(cfv0, dv[2], 4 * (size_t)g.H[0], cudaMemcpyDeviceToHost, B.stream));
+  if (cfv1) CU(cudaMemcpyAsync(cfv1, dv[3], 4 * (size_t)g.H[1], cudaMemcpyDeviceToHost, B.stream));
+  if (dw0) CU(cudaMemcpyAsync(dw0, dv[6], 4 * (size_t)g.H[0], cudaMemcpyDeviceToHost, B.stream));
+  if (dw1) CU(cudaMemcpyAsync(dw1, dv[7], 4 * (size_t)g.H[1], cudaMemcpyDeviceToHost, B.stream));
+  if (dbcfv)
+    for (size_t k = 0; k < nb; ++k)
+      for (int p = 0; p < 2; ++p)
+        CU(cudaMemcpyAsync(dbcfv + k * (g.H[0] + g.H[1]) + (p ? g.H[0] : 0), d_bg + (k * 2 + p) * g.vstride,
+                           4 * (size_t)g.H[p], cudaMemcpyDeviceToHost, B.stream));
+  CU(cudaStreamSynchronize(B.stream));
+  return B.check_err();
+}
+
+int ps_eval_fixed_strategy(ps_game* G, const float* w0, const float* w1, float* cfv0, float* cfv1) {
+  return fixed_strategy_run(G, w0, w1, nullptr, nullptr, cfv0, cfv1, nullptr, nullptr, nullptr);
+}
+
+int ps_eval_fixed_strategy_adjoint(ps_game* G, const float* w0, const float* w1, const float* g0, const float* g1,
+                                   float* dw0, float* dw1, float* dbcfv) {
+  if (!dw0 || !dw1) return fail(PS_ERR_INVALID, "null argument");
+  return fixed_strategy_run(G, w0, w1, g0, g1, nullptr, nullptr, dw0, dw1, dbcfv);
 }
 
 int ps_num_private_hands(ps_game* G, int p) { return G ? G->g->H[p & 1] : fail(PS_ERR_INVALID, "null game"); }

@@ -58,7 +58,7 @@ struct NodeDev {
   float amount_lose;     //   (game/evaluation.rs:64-68, :430)
   float amount_tie;
   float payoff_scale;    // half_pot / num_combinations (depth boundary)
-  int32_t pad;
+  float path_scale;      // product of 1 / chance_factor over the chance nodes above
 };
 static_assert(sizeof(NodeDev) == 48, "NodeDev layout");
 

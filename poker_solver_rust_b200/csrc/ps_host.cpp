@@ -763,7 +763,11 @@ void Game::compile(int p) {
     for (int i = 0; i < nt;) {
       int j = i + 1;
       Op& lead = P.ops[begin + ne + i];
-      while (j < nt && j - i < 255 && P.ops[begin + ne + j].board == lead.board && P.ops[begin + ne + j].src == lead.src) ++j;
+      // a depth-boundary terminal always forms a run of its own: the adjoint
+      // pass weights its reach by that node's boundary values
+      while (j < nt && j - i < 255 && lead.term != TERM_BOUNDARY && P.ops[begin + ne + j].term != TERM_BOUNDARY &&
+             P.ops[begin + ne + j].board == lead.board && P.ops[begin + ne + j].src == lead.src)
+        ++j;
       lead.na = (uint8_t)(j - i);
       P.groups.push_back((uint16_t)i);
       i = j;

@@ -73,6 +73,9 @@ struct Ctx {
   int vstride;
   const float* root_reach;
   float* buf;    // smem: this warp's scan buffer [3 * vstride]
+  int owner;     // >= 0: adjoint pass, terminal values are player owner's payoffs (see warp_terms)
+  int signed_reach;  // reach may be negative: terminal scans take segment starts from the bitmap
+  float* bgrad;  // boundary gradient buffer [num_boundary][2][vstride], or null
   double* red;   // smem: reduction scratch       [32]
   Tables t0;     // board-0 tables (shared memory when staged, else global)
 };
@@ -355,6 +358,16 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
   const float* rch = slot_in(c, ops[0].src);
   prefetch_l2_bytes(T.thr[p], 16 * Hp);
   float* buf = c.buf;
+  // adjoint pass at a depth boundary: the reach is weighted by the payoff
+  // owner's boundary values.  Where the gathered values may be negative
+  // (caller-given reach, boundary weights) segment starts come from the
+  // bitmap; solve passes mark them in the sign bit of the non-negative reach.
+  const bool adjm = c.owner >= 0;
+  const NodeDev& nd0 = sp.nodes[ops[0].node];
+  const float* bw = adjm && ops[0].term == TERM_BOUNDARY
+                        ? sp.bcfv + ((size_t)nd0.boundary * 2 + c.owner) * c.vstride
+                        : nullptr;
+  const bool bits = bw != nullptr || c.signed_reach != 0;
   {  // 1. gather
     const int n4 = (n3 + 3) >> 2;  // groups of four entries
     for (int w0 = lane; w0 < n4; w0 += 32 * 4) {
@@ -372,17 +385,18 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
         const int k = 4 * (w0 + 32 * u);
         const uint32_t id[4] = {ix[u].x & 0xFFFFu, ix[u].x >> 16, ix[u].y & 0xFFFFu, ix[u].y >> 16};
 #pragma unroll
-        for (int e = 0; e < 4; ++e) x[u][e] = k + e < n3 ? rch[id[e]] : 0.f;
+        for (int e = 0; e < 4; ++e) x[u][e] = k + e < n3 ? (bw ? rch[id[e]] * bw[id[e]] : rch[id[e]]) : 0.f;
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         const int k = 4 * (w0 + 32 * u);
         if (k >= n3) continue;
+        const uint32_t m = bits ? 0u : hb[u];
         float4 v;
-        v.x = (hb[u] & 1u) ? -x[u][0] : x[u][0];
-        v.y = (hb[u] & 2u) ? -x[u][1] : x[u][1];
-        v.z = (hb[u] & 4u) ? -x[u][2] : x[u][2];
-        v.w = (hb[u] & 8u) ? -x[u][3] : x[u][3];
+        v.x = (m & 1u) ? -x[u][0] : x[u][0];
+        v.y = (m & 2u) ? -x[u][1] : x[u][1];
+        v.z = (m & 4u) ? -x[u][2] : x[u][2];
+        v.w = (m & 8u) ? -x[u][3] : x[u][3];
         st4(buf + k, v);  // entries past n3 are never read
       }
     }
@@ -394,9 +408,16 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
     float run = 0.f;
     int first = hi;
     for (int j = lo; j < hi; ++j) {
-      const float x = buf[j];
-      if (signbit(x)) {
-        run = -x;
+      float x = buf[j];
+      bool head;
+      if (bits) {
+        head = (hd[j >> 5] >> (j & 31)) & 1u;
+      } else {
+        head = signbit(x);
+        if (head) x = -x;
+      }
+      if (head) {
+        run = x;
         first = min(first, j);
       } else {
         run = __fadd_rn(run, x);
@@ -425,11 +446,18 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
   const uint4* thr = T.thr[p];
   const float* cp = buf + V;  // card-group part
   const float Tsum = V > 0 ? buf[V - 1] : 0.f;
+  const int pay = adjm ? c.owner : p;  // whose payoffs the values are
   for (int j = 0; j < n; ++j) {
     const Op& op = ops[j];
     const NodeDev& nd = sp.nodes[op.node];
     float* dst = slot_at(c, op.dst);
     const float aw = nd.amount_win, al = nd.amount_lose;
+    // showdown coefficients of the traverser's win / loss (swapped when the
+    // values are the opponent's payoffs)
+    const float cw = adjm ? al : aw, cl = adjm ? aw : al;
+    float* grow = c.bgrad && op.term == TERM_BOUNDARY && !adjm
+                      ? c.bgrad + ((size_t)nd.boundary * 2 + p) * c.vstride
+                      : nullptr;
     for (int h = lane; h < hsp; h += 32) {
       float v = 0.f;
       const uint4 t = h < Hp ? thr[h] : make_uint4(THR_INVALID, 0, 0, 0);
@@ -446,28 +474,37 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
           const float win = Plt - Q1lt - Q2lt;
           if (!sp.raked) {
             const float lose = (Tsum - Ple) - (M1 - Q1le) - (M2 - Q2le);
-            v = __fadd_rn(__fmul_rn(aw, win), __fmul_rn(al, lose));
+            v = __fadd_rn(__fmul_rn(cw, win), __fmul_rn(cl, lose));
           } else {
             const uint32_t si = t.w >> 16;
             const float rs = si != 0xFFFF ? rch[si] : 0.f;
             const float tie = Ple - Q1le - Q2le;
             const float tot = Tsum - M1 - M2;
-            v = aw * win + nd.amount_tie * (tie - win + rs) + al * (tot - tie);
+            v = cw * win + nd.amount_tie * (tie - win + rs) + cl * (tot - tie);
           }
         } else {
           const uint32_t si = t.w >> 16;
-          const float rs = si != 0xFFFF ? rch[si] : 0.f;
+          const float rs = si != 0xFFFF ? (bw ? rch[si] * bw[si] : rch[si]) : 0.f;
           const float adj = Tsum + rs - M1 - M2;
           if (op.term == TERM_FOLD) {
-            v = __fmul_rn(op.fold_pl != p ? aw : al, adj);
+            v = __fmul_rn(op.fold_pl != pay ? aw : al, adj);
+          } else if (adjm) {
+            v = __fmul_rn(nd.payoff_scale, adj);
           } else {
             const float bv = sp.bcfv[((size_t)nd.boundary * 2 + p) * c.vstride + h];
             v = __fmul_rn(__fmul_rn(bv, nd.payoff_scale), adj);
+            if (grow) grow[h] = __fmul_rn(nd.payoff_scale, adj);
           }
         }
       }
+      if (grow && !(t.x != THR_INVALID && V > 0)) grow[h] = 0.f;
       dst[h] = v;
     }
+  }
+  if (bw && c.bgrad) {  // dV/dB = (scale * blocked opponent reach) * own adjoint reach / chance path
+    float* grow = c.bgrad + ((size_t)nd0.boundary * 2 + c.owner) * c.vstride;
+    const float inv = __fdiv_rn(1.0f, nd0.path_scale);
+    for (int h = lane; h < sp.H[c.owner]; h += 32) grow[h] = __fmul_rn(__fmul_rn(grow[h], rch[h]), inv);
   }
   __syncwarp();  // the buffer is free for this warp's next run
   PHASE_ADD(PH_LOOKUP, t_look);
@@ -566,6 +603,9 @@ __device__ bool bind_ctx(Ctx& c, const SpotDev* sp, float* scratch, size_t scrat
                          const SmemPlan plan, int* err) {
   c.sp = sp;
   c.vstride = sp->vstride;
+  c.owner = -1;
+  c.signed_reach = 0;
+  c.bgrad = nullptr;
   c.slots = scratch;
   char* p = smem;
   const int tb = table_bytes_for(sp->hs[0], sp->hs[1]);
@@ -681,9 +721,18 @@ __global__ void PS_SOLVE_BOUNDS k_exploitability(const SpotDev* __restrict__ spo
 // Average-strategy values (utility.rs:552-795).  save != 0: finalize (stores
 // the per-node cfvalues for queries) for both players.  Otherwise one pass for
 // `player` from `root_reach` (root_cfvalues_with_reach), root values to out.
+//
+// owner >= 0 (with save == 0): the adjoint pass of fixed-strategy evaluation.
+// The pass runs player's tree program with the average strategy from
+// root_reach, but every terminal returns the payoffs of `owner` (the other
+// player): out is then the vector-Jacobian product of owner's root cfvalues
+// (cotangent root_reach) with respect to player's initial weights.  bgrad
+// (when not null) collects the boundary-value gradients: a plain pass stores
+// scale * blocked opponent reach at each boundary leaf, the adjoint pass for
+// the other player multiplies it by that player's adjoint reach.
 __global__ void PS_SOLVE_BOUNDS k_average(const SpotDev* __restrict__ spots, int nspots, int save, int player,
                                           const float* root_reach, float* scratch, size_t scratch_floats, float* out,
-                                          SmemPlan plan, int* err) {
+                                          int owner, float* bgrad, SmemPlan plan, int* err) {
   extern __shared__ float4 smem4[];
   char* smem = reinterpret_cast<char*>(smem4);
   float* my_scratch = scratch + (size_t)blockIdx.x * scratch_floats;
@@ -699,6 +748,9 @@ __global__ void PS_SOLVE_BOUNDS k_average(const SpotDev* __restrict__ spots, int
       }
     } else {
       c.root_reach = root_reach ? root_reach : sp.w[player ^ 1];
+      c.signed_reach = root_reach != nullptr;
+      c.owner = owner;
+      c.bgrad = bgrad;
       run_pass(c, player, dz, M_AVG);
       const float* r = slot_at(c, sp.root_slot[player]);
       for (int h = threadIdx.x; h < sp.H[player]; h += blockDim.x) out[(size_t)si * sp.hs[player] + h] = r[h];
@@ -964,11 +1016,12 @@ cudaError_t launch_exploitability(const SpotDev* spots, int nspots, float* scrat
 
 cudaError_t launch_average(const SpotDev* spots, int nspots, int save, int player, const float* root_reach,
                            float* scratch, size_t scratch_floats, float* out, int* err, int grid, int block,
-                           const SmemPlan& plan, cudaStream_t s) {
+                           const SmemPlan& plan, cudaStream_t s, int owner, float* bgrad) {
   size_t smem = plan.total();
   cudaError_t e = set_smem((const void*)k_average, smem);
   if (e != cudaSuccess) return e;
-  k_average<<<grid, block, smem, s>>>(spots, nspots, save, player, root_reach, scratch, scratch_floats, out, plan,
+  k_average<<<grid, block, smem, s>>>(spots, nspots, save, player, root_reach, scratch, scratch_floats, out, owner,
+                                       bgrad, plan,
                                        err);
   return cudaGetLastError();
 }

@@ -46,7 +46,8 @@ cudaError_t launch_exploitability(const SpotDev* spots, int nspots, float* scrat
                                   float* out, int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s);
 cudaError_t launch_average(const SpotDev* spots, int nspots, int save, int player, const float* root_reach,
                            float* scratch, size_t scratch_floats, float* out, int* err, int grid, int block,
-                           const SmemPlan& plan, cudaStream_t s);
+                           const SmemPlan& plan, cudaStream_t s, int owner = -1,
+                           float* bgrad = nullptr);
 cudaError_t launch_eval_terminal(const SpotDev* spots, Op op, int player, float* scratch, size_t scratch_floats,
                                  int* err, int block, const SmemPlan& plan, cudaStream_t s);
 

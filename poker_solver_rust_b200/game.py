@@ -367,6 +367,36 @@ def root_cfvalues(game: PostFlopGame, player: int) -> np.ndarray:
     return root_cfvalues_with_reach(game, player, None)
 
 
+def eval_fixed_strategy(game: PostFlopGame, w0, w1):
+    """Root cfvalues of both players under the average strategy, with initial
+    weights w0, w1 (solver hand order) in place of the game's: (cfv0, cfv1),
+    where cfv0 depends on w1 and the boundary values, cfv1 on w0."""
+    a = np.ascontiguousarray(w0, np.float32)
+    b = np.ascontiguousarray(w1, np.float32)
+    c0, c1 = _f32(game.num_private_hands(0)), _f32(game.num_private_hands(1))
+    N.check(N.lib().ps_eval_fixed_strategy(game._h, _fp(a), _fp(b), _fp(c0), _fp(c1)))
+    return c0, c1
+
+
+def eval_fixed_strategy_adjoint(game: PostFlopGame, w0, w1, g0, g1):
+    """Vector-Jacobian product of eval_fixed_strategy for cotangents g0, g1 on
+    (cfv0, cfv1): returns (dw0, dw1, dbcfv) with dbcfv[k][p] the gradient with
+    respect to the boundary values of ordinal k, player p."""
+    a = np.ascontiguousarray(w0, np.float32)
+    b = np.ascontiguousarray(w1, np.float32)
+    ga = None if g0 is None else np.ascontiguousarray(g0, np.float32)
+    gb = None if g1 is None else np.ascontiguousarray(g1, np.float32)
+    H0, H1 = game.num_private_hands(0), game.num_private_hands(1)
+    nb = game.num_boundary_nodes()
+    dw0, dw1 = _f32(H0), _f32(H1)
+    db = _f32(max(1, nb * (H0 + H1)))
+    N.check(N.lib().ps_eval_fixed_strategy_adjoint(game._h, _fp(a), _fp(b), None if ga is None else _fp(ga),
+                                                   None if gb is None else _fp(gb), _fp(dw0), _fp(dw1), _fp(db)))
+    dbcfv = [[db[k * (H0 + H1):k * (H0 + H1) + H0].copy(), db[k * (H0 + H1) + H0:(k + 1) * (H0 + H1)].copy()]
+             for k in range(nb)]
+    return dw0, dw1, dbcfv
+
+
 def compute_average(values, weights) -> float:  # utility.rs:127-136
     v = np.asarray(values, np.float64)
     w = np.asarray(weights, np.float64)
