@@ -198,7 +198,7 @@ def main():
     ap.add_argument("--ref-spots", type=int, default=32)
     ap.add_argument("--cpu-sample", type=int, default=32)
     ap.add_argument("--plain-sample", type=int, default=32)
-    ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--block", type=int, default=-1, help="threads per CTA; -1 = autotune, 0 = library default")
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--stage", type=int, default=-1)
@@ -317,7 +317,8 @@ def main():
                                    f"{MAX_ITER} iterations", "parallelism": f"replicas x{world}",
                        "l2": "state (regrets + strategy sums) exceeds L2; no flush needed",
                        "block_threads": cfg["block_threads"], "ctas_per_sm": cfg["ctas_per_sm"],
-                       "grid": cfg["grid"]},
+                       "grid": cfg["grid"],
+                       "autotune": [{"block_threads": b, "trial_ms": round(ms, 3)} for b, ms in bs.autotune_log()]},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": 2 * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

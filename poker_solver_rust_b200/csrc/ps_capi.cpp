@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -45,6 +46,8 @@ struct DeviceConsts {
   int nsm = 0;
 };
 std::mutex g_dev_mu;
+std::mutex g_tune_mu;
+std::map<long, int> g_tune;  // autotuned CTA size per (device, hand-count class, tree-size class)
 DeviceConsts g_dev[16];
 
 int device_consts(DeviceConsts** out) {
@@ -136,6 +139,7 @@ struct Batch {
   int block = 256, grid = 1, ctas_per_sm = 0;
   int max_vstride = 32;
   SmemPlan plan{};
+  std::vector<std::pair<int, float>> tune_log;  // (threads per CTA, trial ms) of the last autotune
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   float last_solve_ms = 0, last_setup_ms = 0;
   std::vector<float> h_expl;
@@ -329,6 +333,7 @@ struct Batch {
       hs_max = std::max(hs_max, std::max(gp->hs[0], gp->hs[1]));
       single_board &= gp->boards.size() == 1;
     }
+    const bool tune = opts && opts->block_threads < 0;
     block = opts && opts->block_threads > 0 ? opts->block_threads : 128;
     block = std::max(64, std::min(256, (block / 32) * 32));
     const int stage = opts ? opts->stage_tables : -1;
@@ -356,6 +361,108 @@ struct Batch {
     CU(cudaMemcpyAsync(d_spots, h_spots.data(), sizeof(SpotDev) * n, cudaMemcpyHostToDevice, stream));
     CU(cudaMemcpyAsync(d_work, work.data(), sizeof(int2) * nwork, cudaMemcpyHostToDevice, stream));
     CU(cudaMemcpyAsync(d_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
+    CU(cudaStreamSynchronize(stream));
+    if (tune) return autotune(order, opts ? opts->ctas_per_sm : 0);
+    return PS_OK;
+  }
+
+  // Launch shape for a CTA of `b` threads: shared-memory plan, CTAs per SM
+  // and grid for `nspots` spots.
+  void shape_for(int b, int cap_ctas, int nspots, SmemPlan& pl, int& occ, int& g) const {
+    pl = plan;
+    pl.warps = b / 32;
+    occ = solve_occupancy(b, pl);
+    if (cap_ctas > 0) occ = std::min(occ, cap_ctas);
+    g = std::max(1, std::min(nspots, dc->nsm * occ));
+  }
+
+  // Autotuner: times a fixed amount of work (a few DCFR iterations of a
+  // sample of this batch's spots, taken evenly from the cost order) with every
+  // CTA size from 64 to the compiled maximum in steps of one warp, each with
+  // as many CTAs as fit, and keeps the fastest.  The choice is cached per
+  // device and tree-size class, and the state the trial runs touched is
+  // cleared afterwards.
+  int autotune(const std::vector<int>& order, int cap_ctas) {
+    const int n = (int)games.size();
+    int hs_max = 4;
+    double nodes = 0;
+    for (auto& gp : games) {
+      hs_max = std::max(hs_max, std::max(gp->hs[0], gp->hs[1]));
+      nodes += (double)gp->arena.size();
+    }
+    const long key = ((long)dc->device << 40) | ((long)(hs_max / 64) << 20) |
+                     (long)std::min(1 << 19, (int)std::lround(std::log2(1.0 + nodes / n) * 4));
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tune.find(key);
+      if (it != g_tune.end()) return adopt_block(it->second, cap_ctas);
+    }
+    std::vector<int> cands;
+    for (int b = 64; b <= kMaxSolveBlock; b += 32) cands.push_back(b);
+    int max_grid = 1;
+    for (int b : cands) {
+      SmemPlan pl;
+      int occ, g;
+      shape_for(b, cap_ctas, n, pl, occ, g);
+      max_grid = std::max(max_grid, g);
+    }
+    const int ns = std::min(n, max_grid);
+    std::vector<SpotDev> sample(ns);
+    for (int i = 0; i < ns; ++i) sample[i] = h_spots[order[(size_t)i * n / ns]];
+    int rc = run_setup();
+    if (rc) return rc;
+    if ((rc = ensure_disc(16))) return rc;
+    SpotDev* d_sample = nullptr;
+    float* d_tscratch = nullptr;
+    CU(cudaMalloc(&d_sample, sizeof(SpotDev) * ns));
+    std::unique_ptr<SpotDev, decltype(&cudaFree)> k1(d_sample, &cudaFree);
+    CU(cudaMalloc(&d_tscratch, sizeof(float) * scratch_floats * ns));
+    std::unique_ptr<float, decltype(&cudaFree)> k2(d_tscratch, &cudaFree);
+    CU(cudaMemcpyAsync(d_sample, sample.data(), sizeof(SpotDev) * ns, cudaMemcpyHostToDevice, stream));
+    int best = block;
+    float best_ms = 0;
+    for (int b : cands) {
+      SmemPlan pl;
+      int occ, g;
+      shape_for(b, cap_ctas, ns, pl, occ, g);
+      CU(launch_iterate(d_sample, ns, d_disc, 0, 2, d_tscratch, scratch_floats, d_err, g, b, pl, stream));
+      CU(cudaEventRecord(ev[2], stream));
+      CU(launch_iterate(d_sample, ns, d_disc, 2, 8, d_tscratch, scratch_floats, d_err, g, b, pl, stream));
+      CU(cudaEventRecord(ev[3], stream));
+      CU(cudaStreamSynchronize(stream));
+      float ms = 0;
+      CU(cudaEventElapsedTime(&ms, ev[2], ev[3]));
+      tune_log.push_back({b, ms});
+      if (best_ms == 0 || ms < best_ms) {
+        best_ms = ms;
+        best = b;
+      }
+    }
+    if ((rc = check_err())) return rc;
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      g_tune[key] = best;
+    }
+    CU(cudaMemsetAsync(pool + static_bytes + setup_bytes, 0, state_bytes, stream));
+    return adopt_block(best, cap_ctas);
+  }
+
+  // Switches the batch to CTAs of `b` threads (scratch sized for the new grid).
+  int adopt_block(int b, int cap_ctas) {
+    const int n = (int)games.size();
+    SmemPlan pl;
+    int occ, g;
+    shape_for(b, cap_ctas, n, pl, occ, g);
+    if (g > scratch_ctas) {
+      cudaFree(d_scratch);
+      d_scratch = nullptr;
+      CU(cudaMalloc(&d_scratch, sizeof(float) * scratch_floats * g));
+      scratch_ctas = g;
+    }
+    block = b;
+    plan = pl;
+    ctas_per_sm = occ;
+    grid = g;
     CU(cudaStreamSynchronize(stream));
     return PS_OK;
   }
@@ -1405,6 +1512,16 @@ int ps_batch_config(ps_batch* pb, int32_t* block, int32_t* grid, int32_t* cps) {
   if (grid) *grid = pb->b->grid;
   if (cps) *cps = pb->b->ctas_per_sm;
   return PS_OK;
+}
+
+int ps_batch_autotune_log(ps_batch* pb, int32_t* block_threads, float* trial_ms, int cap) {
+  if (!pb) return fail(PS_ERR_INVALID, "null batch");
+  const auto& L = pb->b->tune_log;
+  for (int i = 0; i < (int)L.size() && i < cap; ++i) {
+    if (block_threads) block_threads[i] = L[i].first;
+    if (trial_ms) trial_ms[i] = L[i].second;
+  }
+  return (int)L.size();
 }
 
 }  // extern "C"

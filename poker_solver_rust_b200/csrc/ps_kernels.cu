@@ -344,6 +344,10 @@ __device__ __forceinline__ void board_tables(const Ctx& c, int b, Tables& t) {
 //     carry-in, and the chunk's entries before its first segment start add it;
 //  3. lookups: per terminal, every hand reads its 16-byte record and its
 //     win / lose / blocked sums at the recorded positions of the scan.
+// GEN = false is the copy the solve passes use (non-negative reach, the
+// traverser's own payoffs, no boundary gradients); GEN = true adds what the
+// average-strategy passes of root_cfvalues_with_reach and the adjoint need.
+template <bool GEN>
 __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int p) {
   PHASE_T0(t_scan);
   const SpotDev& sp = *c.sp;
@@ -362,12 +366,12 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
   // owner's boundary values.  Where the gathered values may be negative
   // (caller-given reach, boundary weights) segment starts come from the
   // bitmap; solve passes mark them in the sign bit of the non-negative reach.
-  const bool adjm = c.owner >= 0;
+  const bool adjm = GEN && c.owner >= 0;
   const NodeDev& nd0 = sp.nodes[ops[0].node];
   const float* bw = adjm && ops[0].term == TERM_BOUNDARY
                         ? sp.bcfv + ((size_t)nd0.boundary * 2 + c.owner) * c.vstride
                         : nullptr;
-  const bool bits = bw != nullptr || c.signed_reach != 0;
+  const bool bits = GEN && (bw != nullptr || c.signed_reach != 0);
   {  // 1. gather
     const int n4 = (n3 + 3) >> 2;  // groups of four entries
     for (int w0 = lane; w0 < n4; w0 += 32 * 4) {
@@ -385,7 +389,7 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
         const int k = 4 * (w0 + 32 * u);
         const uint32_t id[4] = {ix[u].x & 0xFFFFu, ix[u].x >> 16, ix[u].y & 0xFFFFu, ix[u].y >> 16};
 #pragma unroll
-        for (int e = 0; e < 4; ++e) x[u][e] = k + e < n3 ? (bw ? rch[id[e]] * bw[id[e]] : rch[id[e]]) : 0.f;
+        for (int e = 0; e < 4; ++e) x[u][e] = k + e < n3 ? (GEN && bw ? rch[id[e]] * bw[id[e]] : rch[id[e]]) : 0.f;
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
@@ -455,7 +459,7 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
     // showdown coefficients of the traverser's win / loss (swapped when the
     // values are the opponent's payoffs)
     const float cw = adjm ? al : aw, cl = adjm ? aw : al;
-    float* grow = c.bgrad && op.term == TERM_BOUNDARY && !adjm
+    float* grow = GEN && c.bgrad && op.term == TERM_BOUNDARY && !adjm
                       ? c.bgrad + ((size_t)nd.boundary * 2 + p) * c.vstride
                       : nullptr;
     for (int h = lane; h < hsp; h += 32) {
@@ -484,24 +488,24 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
           }
         } else {
           const uint32_t si = t.w >> 16;
-          const float rs = si != 0xFFFF ? (bw ? rch[si] * bw[si] : rch[si]) : 0.f;
+          const float rs = si != 0xFFFF ? (GEN && bw ? rch[si] * bw[si] : rch[si]) : 0.f;
           const float adj = Tsum + rs - M1 - M2;
           if (op.term == TERM_FOLD) {
             v = __fmul_rn(op.fold_pl != pay ? aw : al, adj);
-          } else if (adjm) {
+          } else if (GEN && adjm) {
             v = __fmul_rn(nd.payoff_scale, adj);
           } else {
             const float bv = sp.bcfv[((size_t)nd.boundary * 2 + p) * c.vstride + h];
             v = __fmul_rn(__fmul_rn(bv, nd.payoff_scale), adj);
-            if (grow) grow[h] = __fmul_rn(nd.payoff_scale, adj);
+            if (GEN && grow) grow[h] = __fmul_rn(nd.payoff_scale, adj);
           }
         }
       }
-      if (grow && !(t.x != THR_INVALID && V > 0)) grow[h] = 0.f;
+      if (GEN && grow && !(t.x != THR_INVALID && V > 0)) grow[h] = 0.f;
       dst[h] = v;
     }
   }
-  if (bw && c.bgrad) {  // dV/dB = (scale * blocked opponent reach) * own adjoint reach / chance path
+  if (GEN && bw && c.bgrad) {  // dV/dB = (scale * blocked opponent reach) * own adjoint reach / chance path
     float* grow = c.bgrad + ((size_t)nd0.boundary * 2 + c.owner) * c.vstride;
     const float inv = __fdiv_rn(1.0f, nd0.path_scale);
     for (int h = lane; h < sp.H[c.owner]; h += 32) grow[h] = __fmul_rn(__fmul_rn(grow[h], rch[h]), inv);
@@ -526,7 +530,10 @@ __device__ __noinline__ void run_pass(const Ctx& c, int p, const Discount dc, in
     for (int it = warp; it < items; it += nw) {
       if (it < st.n_groups) {
         const Op* lead = ops + st.begin + st.n_elem + groups[st.gbegin + it];
-        warp_terms(c, lead, lead->na, p);
+        if (c.owner >= 0 || c.signed_reach || c.bgrad)
+          warp_terms<true>(c, lead, lead->na, p);
+        else
+          warp_terms<false>(c, lead, lead->na, p);
       } else {
         const Op op = ops[st.begin + (it - st.n_groups)];
         PHASE_T0(t_op);
@@ -651,7 +658,7 @@ __device__ bool bind_ctx(Ctx& c, const SpotDev* sp, float* scratch, size_t scrat
 // ---------------------------------------------------------------------------
 // Kernels
 // ---------------------------------------------------------------------------
-#define PS_SOLVE_BOUNDS __launch_bounds__(256, 3)
+#define PS_SOLVE_BOUNDS __launch_bounds__(kMaxSolveBlock, 3)
 
 // Batched persistent solve: CTAs pull spots from `counter` (in `order`), and
 // run the full reference solve loop (solver.rs:108-176) per spot:
@@ -769,7 +776,7 @@ __global__ void k_eval_terminal(const SpotDev* __restrict__ spots, Op op, int pl
   if (!bind_ctx(c, &spots[0], scratch, scratch_floats, smem, plan, err)) return;
   c.root_reach = nullptr;
   op.na = 1;
-  if (threadIdx.x < 32) warp_terms(c, &op, 1, player);
+  if (threadIdx.x < 32) warp_terms<false>(c, &op, 1, player);
 }
 
 // ---------------------------------------------------------------------------

@@ -32,6 +32,7 @@ struct SmemPlan {
   }
 };
 
+constexpr int kMaxSolveBlock = 256;  // threads per CTA the solve kernels are compiled for (launch bounds)
 size_t setup_smem_bytes();
 int solve_occupancy(int block, const SmemPlan& plan);
 cudaError_t launch_setup(const SpotDev* spots, const int2* work, int nwork, const int32_t* table, int* err,

@@ -491,6 +491,13 @@ class BatchSolver:
         N.check(N.lib().ps_batch_io_bytes(self._h, C.byref(a), C.byref(b)))
         return int(a.value), int(b.value)
 
+    def autotune_log(self):
+        """[(threads per CTA, trial ms)] of the autotune run by block_threads=-1."""
+        b = (C.c_int32 * 16)()
+        t = (C.c_float * 16)()
+        n = N.check(N.lib().ps_batch_autotune_log(self._h, b, t, 16))
+        return [(int(b[i]), float(t[i])) for i in range(min(n, 16))]
+
     def config(self):
         a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
         N.check(N.lib().ps_batch_config(self._h, C.byref(a), C.byref(b), C.byref(c)))

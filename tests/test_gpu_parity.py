@@ -373,6 +373,29 @@ def test_batch_matches_single_and_oracle():
     _report("batch", rows)
 
 
+def test_batch_autotune_keeps_results():
+    """block_threads=-1 times every CTA size on a sample of the batch and keeps
+    the fastest; the spots' arithmetic does not depend on the CTA size."""
+    sp = spots.datagen_spots(48, seed=33)
+    cc = [spots.card_config(r, b) for r, b, _ in sp]
+    tcs = [t for _, _, t in sp]
+    targets = np.array([0.003 * t.starting_pot for t in tcs], np.float32)
+    ref = ps.BatchSolver(cc, tcs)
+    ref.solve(300, targets)
+    e0, it0 = ref.results()
+    tuned = ps.BatchSolver(cc, tcs, block_threads=-1)
+    cands = list(range(64, 257, 32))
+    log = tuned.autotune_log()
+    assert [b for b, _ in log] in ([], cands) and all(ms > 0 for _, ms in log)
+    assert tuned.config()["block_threads"] in cands
+    if log:
+        assert tuned.config()["block_threads"] == min(log, key=lambda x: x[1])[0]
+    tuned.solve(300, targets)
+    e1, it1 = tuned.results()
+    assert np.array_equal(it0, it1)
+    assert np.allclose(e0, e1, rtol=1e-5, atol=0)
+
+
 def test_state_export_import():
     r, board, tc = spots.river_spot(7)
     g = spots.product_game(r, board, tc)
