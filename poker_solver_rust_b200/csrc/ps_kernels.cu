@@ -462,9 +462,13 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
     float* grow = GEN && c.bgrad && op.term == TERM_BOUNDARY && !adjm
                       ? c.bgrad + ((size_t)nd.boundary * 2 + p) * c.vstride
                       : nullptr;
+    // the next hand's record is requested before this hand's value is stored:
+    // the store may alias it, so the compiler would not issue it earlier
+    uint4 tn = lane < Hp ? thr[lane] : make_uint4(THR_INVALID, 0, 0, 0);
     for (int h = lane; h < hsp; h += 32) {
       float v = 0.f;
-      const uint4 t = h < Hp ? thr[h] : make_uint4(THR_INVALID, 0, 0, 0);
+      const uint4 t = tn;
+      tn = h + 32 < Hp ? thr[h + 32] : make_uint4(THR_INVALID, 0, 0, 0);
       if (t.x != THR_INVALID && V > 0) {
         const int s1 = t.z & 0xFFFF, s2 = t.z >> 16, n1 = t.w & 0xFF, n2 = (t.w >> 8) & 0xFF;
         const float M1 = n1 ? cp[s1 + n1 - 1] : 0.f;
