@@ -202,6 +202,7 @@ def main():
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--stage", type=int, default=-1)
+    ap.add_argument("--bufs", type=int, default=0, help="terminal scan buffers per CTA (0 = one per warp)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -239,7 +240,8 @@ def main():
     def max_over_ranks(x: float) -> float:
         return rank_max(x, dist, "cuda")
 
-    bs = ps.BatchSolver(cc, tcs, block_threads=args.block, ctas_per_sm=args.ctas_per_sm, stage_tables=args.stage)
+    bs = ps.BatchSolver(cc, tcs, block_threads=args.block, ctas_per_sm=args.ctas_per_sm, stage_tables=args.stage,
+                        scan_buffers=args.bufs)
     for _ in range(args.warmup):
         bs.solve(MAX_ITER, targets)
 
@@ -276,7 +278,7 @@ def main():
         barrier()
         t0 = time.perf_counter()
         b2 = ps.BatchSolver(cc, tcs, block_threads=args.block, ctas_per_sm=args.ctas_per_sm,
-                            stage_tables=args.stage)
+                            stage_tables=args.stage, scan_buffers=args.bufs)
         b2.solve(MAX_ITER, targets)
         e2, _ = b2.results()
         torch.cuda.synchronize()
@@ -318,7 +320,9 @@ def main():
                        "l2": "state (regrets + strategy sums) exceeds L2; no flush needed",
                        "block_threads": cfg["block_threads"], "ctas_per_sm": cfg["ctas_per_sm"],
                        "grid": cfg["grid"],
-                       "autotune": [{"block_threads": b, "trial_ms": round(ms, 3)} for b, ms in bs.autotune_log()]},
+                       "scan_buffers": cfg["scan_buffers"],
+                       "autotune": [{"block_threads": b, "scan_buffers": u, "trial_ms": round(ms, 3)}
+                                    for b, u, ms in bs.autotune_log()]},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": 2 * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

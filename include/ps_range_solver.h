@@ -165,12 +165,15 @@ int ps_state_import(ps_game* g, const void* buf, uint64_t size);
  *      crates/gpu-range-solver/src/batch.rs:79-610) ---- */
 typedef struct ps_batch ps_batch;
 typedef struct ps_batch_opts {
-  int32_t block_threads;  /* threads per CTA, a multiple of 32 up to 256 (0 = default 128,
-                             -1 = autotune: time each size on a sample of the batch) */
+  int32_t block_threads;  /* threads per CTA, a multiple of 32 up to 256 (0 = default 256,
+                             -1 = autotune: time each shape on a sample of the batch) */
   int32_t ctas_per_sm;    /* 0 = as many as fit */
   int32_t sort_by_cost;   /* 1 = hand out the largest spots first */
   int32_t stage_tables;   /* 1 = copy a spot's board tables to shared memory, 0 = read them
                              from global memory, -1 = default (0) */
+  int32_t scan_buffers;   /* warps per CTA that evaluate terminal runs, each with a shared-memory
+                             scan buffer of 12 bytes per hand (0 = half the warps; the
+                             autotuner then also tries all of them) */
 } ps_batch_opts;
 int ps_batch_new(const ps_card_config* cards, const ps_tree_config* trees, int32_t n,
                  const ps_batch_opts* opts, ps_batch** out);
@@ -184,10 +187,12 @@ int ps_batch_last_timing(ps_batch* b, float* solve_ms, float* setup_ms);
 /* algorithmic bytes of one DCFR iteration of spot i: 20 * sum_edges H_actor */
 double ps_batch_iteration_bytes(ps_batch* b, int32_t spot);
 int ps_batch_config(ps_batch* b, int32_t* block_threads, int32_t* grid, int32_t* ctas_per_sm);
-/* the trials of the last autotune (block_threads = -1): CTA size and device ms of
- * the fixed trial work each; returns the count (0 when the choice came from the
- * cache or was given) */
-int ps_batch_autotune_log(ps_batch* b, int32_t* block_threads, float* trial_ms, int cap);
+/* the trials of the last autotune (block_threads = -1): CTA size, scan-buffer warps
+ * and device ms of the fixed trial work each; returns the count (0 when the choice
+ * came from the cache or was given) */
+int ps_batch_autotune_log(ps_batch* b, int32_t* block_threads, int32_t* scan_buffers, float* trial_ms, int cap);
+/* scan-buffer warps per CTA the batch runs with */
+int ps_batch_scan_buffers(ps_batch* b);
 /* bytes copied host->device by ps_batch_new and device->host by ps_batch_results */
 int ps_batch_io_bytes(ps_batch* b, uint64_t* h2d, uint64_t* d2h);
 

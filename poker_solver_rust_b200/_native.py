@@ -53,6 +53,7 @@ class PsBatchOpts(C.Structure):
         ("ctas_per_sm", C.c_int32),
         ("sort_by_cost", C.c_int32),
         ("stage_tables", C.c_int32),
+        ("scan_buffers", C.c_int32),
     ]
 
 
@@ -122,7 +123,8 @@ _sig("ps_batch_root_strategy", i32, vp, i32, P(f32))
 _sig("ps_batch_last_timing", i32, vp, P(f32), P(f32))
 _sig("ps_batch_iteration_bytes", f64, vp, i32)
 _sig("ps_batch_config", i32, vp, P(i32), P(i32), P(i32))
-_sig("ps_batch_autotune_log", i32, vp, P(i32), P(f32), i32)
+_sig("ps_batch_autotune_log", i32, vp, P(i32), P(i32), P(f32), i32)
+_sig("ps_batch_scan_buffers", i32, vp)
 _sig("ps_batch_io_bytes", i32, vp, P(u64), P(u64))
 
 EXPORTED = sorted(_SIGS)

@@ -47,7 +47,8 @@ struct DeviceConsts {
 };
 std::mutex g_dev_mu;
 std::mutex g_tune_mu;
-std::map<long, int> g_tune;  // autotuned CTA size per (device, hand-count class, tree-size class)
+std::map<long, std::pair<int, int>> g_tune;  // autotuned (CTA size, scan-buffer warps) per
+                                             // (device, hand-count class, tree-size class)
 DeviceConsts g_dev[16];
 
 int device_consts(DeviceConsts** out) {
@@ -139,7 +140,12 @@ struct Batch {
   int block = 256, grid = 1, ctas_per_sm = 0;
   int max_vstride = 32;
   SmemPlan plan{};
-  std::vector<std::pair<int, float>> tune_log;  // (threads per CTA, trial ms) of the last autotune
+  int req_bufs = 0;  // scan buffers per CTA asked for (0 = one per warp)
+  struct Trial {
+    int block, bufs;
+    float ms;
+  };
+  std::vector<Trial> tune_log;  // trials of the last autotune
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   float last_solve_ms = 0, last_setup_ms = 0;
   std::vector<float> h_expl;
@@ -334,12 +340,15 @@ struct Batch {
       single_board &= gp->boards.size() == 1;
     }
     const bool tune = opts && opts->block_threads < 0;
-    block = opts && opts->block_threads > 0 ? opts->block_threads : 128;
+    req_bufs = opts ? opts->scan_buffers : 0;
+    block = opts && opts->block_threads > 0 ? opts->block_threads : 256;
     block = std::max(64, std::min(256, (block / 32) * 32));
     const int stage = opts ? opts->stage_tables : -1;
     plan.vstride = max_vstride;
     plan.hs_max = hs_max;
     plan.warps = block / 32;
+    plan.bufs = opts && opts->scan_buffers > 0 ? std::min(opts->scan_buffers, plan.warps)
+                                               : std::max(1, plan.warps / 2);
     plan.tables = (single_board && stage == 1) ? table_bytes_for(hs_max, hs_max) : 0;
     int occ = solve_occupancy(block, plan);
     ctas_per_sm = opts && opts->ctas_per_sm > 0 ? std::min(opts->ctas_per_sm, occ) : occ;
@@ -368,9 +377,10 @@ struct Batch {
 
   // Launch shape for a CTA of `b` threads: shared-memory plan, CTAs per SM
   // and grid for `nspots` spots.
-  void shape_for(int b, int cap_ctas, int nspots, SmemPlan& pl, int& occ, int& g) const {
+  void shape_for(int b, int bufs, int cap_ctas, int nspots, SmemPlan& pl, int& occ, int& g) const {
     pl = plan;
     pl.warps = b / 32;
+    pl.bufs = std::max(1, std::min(pl.warps, bufs));
     occ = solve_occupancy(b, pl);
     if (cap_ctas > 0) occ = std::min(occ, cap_ctas);
     g = std::max(1, std::min(nspots, dc->nsm * occ));
@@ -390,20 +400,30 @@ struct Batch {
       hs_max = std::max(hs_max, std::max(gp->hs[0], gp->hs[1]));
       nodes += (double)gp->arena.size();
     }
-    const long key = ((long)dc->device << 40) | ((long)(hs_max / 64) << 20) |
+    const long key = ((long)dc->device << 40) | ((long)(req_bufs & 0xFF) << 32) | ((long)(hs_max / 64) << 20) |
                      (long)std::min(1 << 19, (int)std::lround(std::log2(1.0 + nodes / n) * 4));
     {
       std::lock_guard<std::mutex> lk(g_tune_mu);
       auto it = g_tune.find(key);
-      if (it != g_tune.end()) return adopt_block(it->second, cap_ctas);
+      if (it != g_tune.end()) return adopt_block(it->second.first, it->second.second, cap_ctas);
     }
-    std::vector<int> cands;
-    for (int b = 64; b <= kMaxSolveBlock; b += 32) cands.push_back(b);
+    // candidates: CTA size x warps that own a terminal scan buffer (half or
+    // all of them, or the count the caller fixed)
+    std::vector<std::pair<int, int>> cands;
+    for (int b = 128; b <= kMaxSolveBlock; b += 32) {
+      const int w = b / 32;
+      if (req_bufs > 0) {
+        cands.push_back({b, std::min(w, req_bufs)});
+      } else {
+        cands.push_back({b, std::max(1, w / 2)});
+        cands.push_back({b, w});
+      }
+    }
     int max_grid = 1;
-    for (int b : cands) {
+    for (auto [b, nb] : cands) {
       SmemPlan pl;
       int occ, g;
-      shape_for(b, cap_ctas, n, pl, occ, g);
+      shape_for(b, nb, cap_ctas, n, pl, occ, g);
       max_grid = std::max(max_grid, g);
     }
     const int ns = std::min(n, max_grid);
@@ -419,12 +439,12 @@ struct Batch {
     CU(cudaMalloc(&d_tscratch, sizeof(float) * scratch_floats * ns));
     std::unique_ptr<float, decltype(&cudaFree)> k2(d_tscratch, &cudaFree);
     CU(cudaMemcpyAsync(d_sample, sample.data(), sizeof(SpotDev) * ns, cudaMemcpyHostToDevice, stream));
-    int best = block;
+    std::pair<int, int> best{block, plan.bufs};
     float best_ms = 0;
-    for (int b : cands) {
+    for (auto [b, nb] : cands) {
       SmemPlan pl;
       int occ, g;
-      shape_for(b, cap_ctas, ns, pl, occ, g);
+      shape_for(b, nb, cap_ctas, ns, pl, occ, g);
       CU(launch_iterate(d_sample, ns, d_disc, 0, 2, d_tscratch, scratch_floats, d_err, g, b, pl, stream));
       CU(cudaEventRecord(ev[2], stream));
       CU(launch_iterate(d_sample, ns, d_disc, 2, 8, d_tscratch, scratch_floats, d_err, g, b, pl, stream));
@@ -432,10 +452,10 @@ struct Batch {
       CU(cudaStreamSynchronize(stream));
       float ms = 0;
       CU(cudaEventElapsedTime(&ms, ev[2], ev[3]));
-      tune_log.push_back({b, ms});
+      tune_log.push_back({b, nb, ms});
       if (best_ms == 0 || ms < best_ms) {
         best_ms = ms;
-        best = b;
+        best = {b, nb};
       }
     }
     if ((rc = check_err())) return rc;
@@ -444,15 +464,16 @@ struct Batch {
       g_tune[key] = best;
     }
     CU(cudaMemsetAsync(pool + static_bytes + setup_bytes, 0, state_bytes, stream));
-    return adopt_block(best, cap_ctas);
+    return adopt_block(best.first, best.second, cap_ctas);
   }
 
-  // Switches the batch to CTAs of `b` threads (scratch sized for the new grid).
-  int adopt_block(int b, int cap_ctas) {
+  // Switches the batch to CTAs of `b` threads with `bufs` scan-buffer warps
+  // (scratch sized for the new grid).
+  int adopt_block(int b, int bufs, int cap_ctas) {
     const int n = (int)games.size();
     SmemPlan pl;
     int occ, g;
-    shape_for(b, cap_ctas, n, pl, occ, g);
+    shape_for(b, bufs, cap_ctas, n, pl, occ, g);
     if (g > scratch_ctas) {
       cudaFree(d_scratch);
       d_scratch = nullptr;
@@ -1506,6 +1527,8 @@ int ps_batch_io_bytes(ps_batch* pb, uint64_t* h2d, uint64_t* d2h) {
   return PS_OK;
 }
 
+int ps_batch_scan_buffers(ps_batch* pb) { return pb ? pb->b->plan.bufs : fail(PS_ERR_INVALID, "null batch"); }
+
 int ps_batch_config(ps_batch* pb, int32_t* block, int32_t* grid, int32_t* cps) {
   if (!pb) return fail(PS_ERR_INVALID, "null batch");
   if (block) *block = pb->b->block;
@@ -1514,12 +1537,13 @@ int ps_batch_config(ps_batch* pb, int32_t* block, int32_t* grid, int32_t* cps) {
   return PS_OK;
 }
 
-int ps_batch_autotune_log(ps_batch* pb, int32_t* block_threads, float* trial_ms, int cap) {
+int ps_batch_autotune_log(ps_batch* pb, int32_t* block_threads, int32_t* scan_buffers, float* trial_ms, int cap) {
   if (!pb) return fail(PS_ERR_INVALID, "null batch");
   const auto& L = pb->b->tune_log;
   for (int i = 0; i < (int)L.size() && i < cap; ++i) {
-    if (block_threads) block_threads[i] = L[i].first;
-    if (trial_ms) trial_ms[i] = L[i].second;
+    if (block_threads) block_threads[i] = L[i].block;
+    if (scan_buffers) scan_buffers[i] = L[i].bufs;
+    if (trial_ms) trial_ms[i] = L[i].ms;
   }
   return (int)L.size();
 }

@@ -72,7 +72,8 @@ struct Ctx {
   float* slots;
   int vstride;
   const float* root_reach;
-  float* buf;    // smem: this warp's scan buffer [3 * vstride]
+  float* buf;    // smem: this warp's scan buffer [3 * vstride] (null for warps >= bufs)
+  int bufs;      // warps 0 .. bufs-1 own a scan buffer
   int owner;     // >= 0: adjoint pass, terminal values are player owner's payoffs (see warp_terms)
   int signed_reach;  // reach may be negative: terminal scans take segment starts from the bitmap
   float* bgrad;  // boundary gradient buffer [num_boundary][2][vstride], or null
@@ -530,34 +531,35 @@ __device__ __noinline__ void run_pass(const Ctx& c, int p, const Discount dc, in
   const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int s = 0; s < sp.nsteps[p]; ++s) {
     const Step st = steps[s];
-    const int items = st.n_groups + st.n_elem;  // terminal runs first: they are the longest items
-    for (int it = warp; it < items; it += nw) {
-      if (it < st.n_groups) {
-        const Op* lead = ops + st.begin + st.n_elem + groups[st.gbegin + it];
+    // terminal runs go round robin to the warps that own a scan buffer; node
+    // ops go round robin to all warps, starting at the first warp without a run
+    if (warp < c.bufs)
+      for (int j = warp; j < st.n_groups; j += c.bufs) {
+        const Op* lead = ops + st.begin + st.n_elem + groups[st.gbegin + j];
         if (c.owner >= 0 || c.signed_reach || c.bgrad)
           warp_terms<true>(c, lead, lead->na, p);
         else
           warp_terms<false>(c, lead, lead->na, p);
-      } else {
-        const Op op = ops[st.begin + (it - st.n_groups)];
-        PHASE_T0(t_op);
-        switch (op.type) {
-          case OP_FWD_OPP: op_fwd_opp(c, op, o, mode); break;
-          case OP_FWD_CHANCE: op_fwd_chance(c, op, o); break;
-          case OP_BWD_TRAV: op_bwd_trav(c, op, p, dc, mode); break;
-          case OP_BWD_OPP: op_bwd_opp(c, op, p, mode); break;
-          case OP_BWD_CHANCE: op_bwd_chance(c, op, p, mode); break;
-          default: break;
-        }
-        PHASE_ADD(op.type == OP_FWD_OPP      ? PH_FWD_OPP
-                  : op.type == OP_FWD_CHANCE ? PH_FWD_CHANCE
-                  : op.type == OP_BWD_TRAV   ? PH_BWD_TRAV
-                  : op.type == OP_BWD_OPP    ? PH_BWD_OPP
-                                             : PH_BWD_CHANCE,
-                  t_op);
       }
+    const int start = min(st.n_groups, c.bufs) % nw;
+    for (int i = (warp - start + nw) % nw; i < st.n_elem; i += nw) {
+      const Op op = ops[st.begin + i];
+      PHASE_T0(t_op);
+      switch (op.type) {
+        case OP_FWD_OPP: op_fwd_opp(c, op, o, mode); break;
+        case OP_FWD_CHANCE: op_fwd_chance(c, op, o); break;
+        case OP_BWD_TRAV: op_bwd_trav(c, op, p, dc, mode); break;
+        case OP_BWD_OPP: op_bwd_opp(c, op, p, mode); break;
+        case OP_BWD_CHANCE: op_bwd_chance(c, op, p, mode); break;
+        default: break;
+      }
+      PHASE_ADD(op.type == OP_FWD_OPP      ? PH_FWD_OPP
+                : op.type == OP_FWD_CHANCE ? PH_FWD_CHANCE
+                : op.type == OP_BWD_TRAV   ? PH_BWD_TRAV
+                : op.type == OP_BWD_OPP    ? PH_BWD_OPP
+                                           : PH_BWD_CHANCE,
+                t_op);
     }
-    PHASE_T0(t_bar);
     __syncthreads();
     PHASE_ADD(PH_BARRIER, t_bar);
   }
@@ -623,8 +625,10 @@ __device__ bool bind_ctx(Ctx& c, const SpotDev* sp, float* scratch, size_t scrat
   const bool staged = sp->num_boards == 1 && tb <= plan.tables;
   char* tables = p;
   p += plan.tables;
-  c.buf = reinterpret_cast<float*>(p) + (size_t)(threadIdx.x >> 5) * 3 * plan.vstride;
-  p += (size_t)plan.warps * 3 * plan.vstride * 4;
+  const int warp_id = threadIdx.x >> 5;
+  c.buf = warp_id < plan.bufs ? reinterpret_cast<float*>(p) + (size_t)warp_id * 3 * plan.vstride : nullptr;
+  c.bufs = plan.bufs;
+  p += (size_t)plan.bufs * 3 * plan.vstride * 4;
   c.red = reinterpret_cast<double*>(p);
   if ((size_t)sp->num_slots * sp->vstride > scratch_floats || sp->vstride > plan.vstride) {
     if (threadIdx.x == 0) atomicOr(err, ERR_SCRATCH);
@@ -662,7 +666,10 @@ __device__ bool bind_ctx(Ctx& c, const SpotDev* sp, float* scratch, size_t scrat
 // ---------------------------------------------------------------------------
 // Kernels
 // ---------------------------------------------------------------------------
-#define PS_SOLVE_BOUNDS __launch_bounds__(kMaxSolveBlock, 3)
+#ifndef PS_LB_MIN
+#define PS_LB_MIN 4  // CTAs of kMaxSolveBlock threads per SM the register budget is sized for (64 registers)
+#endif
+#define PS_SOLVE_BOUNDS __launch_bounds__(kMaxSolveBlock, PS_LB_MIN)
 
 // Batched persistent solve: CTAs pull spots from `counter` (in `order`), and
 // run the full reference solve loop (solver.rs:108-176) per spot:

@@ -25,10 +25,11 @@ __host__ __device__ inline int table_bytes_for(int hs0, int hs1) {
 struct SmemPlan {
   int vstride;  // max slot stride of the launch (floats)
   int hs_max;   // max padded hand count
-  int warps;    // warps per CTA (one scan buffer each)
+  int warps;    // warps per CTA
+  int bufs;     // warps 0 .. bufs-1 own a terminal scan buffer and evaluate the terminal runs
   int tables;   // bytes reserved for staged board tables (0 = tables stay in global memory)
   __host__ __device__ size_t total() const {
-    return (size_t)tables + (size_t)warps * 3 * vstride * 4 + 32 * 8;
+    return (size_t)tables + (size_t)bufs * 3 * vstride * 4 + 32 * 8;
   }
 };
 

@@ -439,7 +439,7 @@ class BatchSolver:
 
     def __init__(self, card_configs: Sequence[CardConfig], tree_configs: Sequence[TreeConfig],
                  block_threads: int = 0, ctas_per_sm: int = 0, sort_by_cost: bool = True,
-                 stage_tables: int = -1):
+                 stage_tables: int = -1, scan_buffers: int = 0):
         n = len(card_configs)
         cc = (N.PsCardConfig * n)()
         tc = (N.PsTreeConfig * n)()
@@ -450,7 +450,7 @@ class BatchSolver:
             keep.append((c._keep, t._keep))
             cc[i] = c
             tc[i] = t
-        opts = N.PsBatchOpts(block_threads, ctas_per_sm, int(sort_by_cost), stage_tables)
+        opts = N.PsBatchOpts(block_threads, ctas_per_sm, int(sort_by_cost), stage_tables, scan_buffers)
         h = C.c_void_p()
         N.check(N.lib().ps_batch_new(cc, tc, n, C.byref(opts), C.byref(h)))
         self._h = h
@@ -492,13 +492,16 @@ class BatchSolver:
         return int(a.value), int(b.value)
 
     def autotune_log(self):
-        """[(threads per CTA, trial ms)] of the autotune run by block_threads=-1."""
-        b = (C.c_int32 * 16)()
-        t = (C.c_float * 16)()
-        n = N.check(N.lib().ps_batch_autotune_log(self._h, b, t, 16))
-        return [(int(b[i]), float(t[i])) for i in range(min(n, 16))]
+        """[(threads per CTA, scan-buffer warps, trial ms)] of the autotune run by
+        block_threads=-1."""
+        b = (C.c_int32 * 32)()
+        u = (C.c_int32 * 32)()
+        t = (C.c_float * 32)()
+        n = N.check(N.lib().ps_batch_autotune_log(self._h, b, u, t, 32))
+        return [(int(b[i]), int(u[i]), float(t[i])) for i in range(min(n, 32))]
 
     def config(self):
         a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
         N.check(N.lib().ps_batch_config(self._h, C.byref(a), C.byref(b), C.byref(c)))
-        return {"block_threads": a.value, "grid": b.value, "ctas_per_sm": c.value}
+        return {"block_threads": a.value, "grid": b.value, "ctas_per_sm": c.value,
+                "scan_buffers": N.check(N.lib().ps_batch_scan_buffers(self._h))}

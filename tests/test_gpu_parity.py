@@ -384,12 +384,14 @@ def test_batch_autotune_keeps_results():
     ref.solve(300, targets)
     e0, it0 = ref.results()
     tuned = ps.BatchSolver(cc, tcs, block_threads=-1)
-    cands = list(range(64, 257, 32))
+    cands = [(b, u) for b in range(128, 257, 32) for u in (max(1, b // 64), b // 32)]
     log = tuned.autotune_log()
-    assert [b for b, _ in log] in ([], cands) and all(ms > 0 for _, ms in log)
-    assert tuned.config()["block_threads"] in cands
+    assert [(b, u) for b, u, _ in log] in ([], cands) and all(ms > 0 for _, _, ms in log)
+    cfg = tuned.config()
+    assert (cfg["block_threads"], cfg["scan_buffers"]) in cands
     if log:
-        assert tuned.config()["block_threads"] == min(log, key=lambda x: x[1])[0]
+        best = min(log, key=lambda x: x[2])
+        assert (cfg["block_threads"], cfg["scan_buffers"]) == best[:2]
     tuned.solve(300, targets)
     e1, it1 = tuned.results()
     assert np.array_equal(it0, it1)
