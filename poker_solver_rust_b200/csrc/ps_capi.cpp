@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -141,6 +142,11 @@ struct Batch {
   int max_vstride = 32;
   SmemPlan plan{};
   int req_bufs = 0;  // scan buffers per CTA asked for (0 = one per warp)
+  // grid mode: a single large spot runs on every CTA of a cooperative launch
+  bool grid_mode = false;
+  int grid_blocks = 0;
+  unsigned* d_bar = nullptr;
+  double* d_gred = nullptr;
   struct Trial {
     int block, bufs;
     float ms;
@@ -161,6 +167,8 @@ struct Batch {
     cudaFree(d_disc);
     cudaFree(d_target);
     cudaFree(d_expl);
+    cudaFree(d_bar);
+    cudaFree(d_gred);
     cudaFree(d_iters);
     cudaFree(d_counter);
     cudaFree(d_err);
@@ -357,6 +365,21 @@ struct Batch {
     scratch_floats = (scratch_floats + 63) & ~(size_t)63;
     scratch_ctas = grid;
     CU(cudaMalloc(&d_scratch, sizeof(float) * scratch_floats * scratch_ctas));
+    // a single tree of at least PS_GRID_NODES nodes (default 2000; 0 = never)
+    // is solved by all SMs at once
+    {
+      const char* env = std::getenv("PS_GRID_NODES");
+      const long thr = env ? std::atol(env) : 2000;
+      if (n == 1 && thr > 0 && (long)games[0]->arena.size() >= thr) {
+        const int gc = grid_ctas(block, plan);
+        if (gc >= 2) {
+          grid_mode = true;
+          grid_blocks = gc;
+          CU(cudaMalloc(&d_bar, 64));
+          CU(cudaMalloc(&d_gred, 64));
+        }
+      }
+    }
     // order: largest estimated cost first (longest-processing-time first)
     std::vector<int> order(n);
     for (int i = 0; i < n; ++i) order[i] = i;
@@ -530,6 +553,22 @@ struct Batch {
     const int n = (int)games.size();
     int rc = ensure_disc(max_iter + 1);
     if (rc) return rc;
+    if (grid_mode) {
+      if (fresh && (rc = run_setup())) return rc;
+      CU(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
+      CU(cudaEventRecord(ev[2], stream));
+      CU(launch_grid(d_spots, 0, d_disc, 0, (int)max_iter, target[0], d_scratch, scratch_floats, d_expl, d_iters,
+                     d_bar, d_gred, d_err, grid_blocks, block, plan, stream));
+      CU(cudaEventRecord(ev[3], stream));
+      h_expl.resize(1);
+      h_iters.resize(1);
+      CU(cudaMemcpyAsync(h_expl.data(), d_expl, sizeof(float), cudaMemcpyDeviceToHost, stream));
+      CU(cudaMemcpyAsync(h_iters.data(), d_iters, sizeof(int), cudaMemcpyDeviceToHost, stream));
+      CU(cudaStreamSynchronize(stream));
+      CU(cudaEventElapsedTime(&last_solve_ms, ev[2], ev[3]));
+      last_setup_ms = 0;
+      return check_err();
+    }
     CU(cudaMemcpyAsync(d_target, target, sizeof(float) * n, cudaMemcpyHostToDevice, stream));
     CU(cudaMemsetAsync(d_counter, 0, sizeof(int), stream));
     CU(cudaEventRecord(ev[1], stream));
@@ -610,7 +649,10 @@ float expl_run(ps_game* G, int* rc) {
   Batch& B = *G->b;
   float e = 0;
   cudaError_t ce = cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream);
-  if (ce == cudaSuccess)
+  if (ce == cudaSuccess && B.grid_mode)
+    ce = launch_grid(B.d_spots, 2, B.d_disc, 0, 0, 0.f, B.d_scratch, B.scratch_floats, B.d_expl, nullptr, B.d_bar,
+                     B.d_gred, B.d_err, B.grid_blocks, B.block, B.plan, B.stream);
+  else if (ce == cudaSuccess)
     ce = launch_exploitability(B.d_spots, 1, B.d_scratch, B.scratch_floats, B.d_expl, B.d_err, 1, B.block, B.plan,
                                B.stream);
   if (ce == cudaSuccess) ce = cudaMemcpyAsync(&e, B.d_expl, 4, cudaMemcpyDeviceToHost, B.stream);
@@ -780,8 +822,12 @@ int ps_solve_step(ps_game* G, uint32_t t) {
   Batch& B = *G->b;
   if ((rc = B.ensure_disc(t + 1))) return rc;
   CU(cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream));
-  CU(launch_iterate(B.d_spots, 1, B.d_disc, (int)t, (int)t + 1, B.d_scratch, B.scratch_floats, B.d_err, 1, B.block,
-                    B.plan, B.stream));
+  if (B.grid_mode)
+    CU(launch_grid(B.d_spots, 1, B.d_disc, (int)t, (int)t + 1, 0.f, B.d_scratch, B.scratch_floats, B.d_expl,
+                   nullptr, B.d_bar, B.d_gred, B.d_err, B.grid_blocks, B.block, B.plan, B.stream));
+  else
+    CU(launch_iterate(B.d_spots, 1, B.d_disc, (int)t, (int)t + 1, B.d_scratch, B.scratch_floats, B.d_err, 1,
+                      B.block, B.plan, B.stream));
   G->host_dirty = true;
   return B.check_err();
 }

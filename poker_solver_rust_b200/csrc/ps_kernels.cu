@@ -19,6 +19,7 @@
 // k_setup), the warp scans that list segment by segment into its shared-memory
 // buffer, and every hand reads its win / lose / blocked sums at precomputed
 // positions - O(n) work per terminal, no CTA-wide barrier.
+#include <cuda/atomic>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -35,6 +36,7 @@ enum Mode { M_DCFR = 0, M_BR = 1, M_AVG = 2, M_AVG_SAVE = 3 };
 // Error bits reported through the error word of every launch.
 constexpr int ERR_SCRATCH = 1;  // a spot needed more scratch than its CTA owns
 constexpr int ERR_SETUP = 2;    // setup tables exceeded their bounds
+constexpr int ERR_WAIT = 4;     // a grid barrier gave up waiting for the other CTAs
 
 constexpr uint32_t THR_INVALID = 0xFFFFFFFFu;
 
@@ -72,6 +74,10 @@ struct Ctx {
   float* slots;
   int vstride;
   const float* root_reach;
+  int grid;      // 1: every CTA of the launch works on this one spot (steps end in a grid barrier)
+  unsigned* bar; // grid mode: barrier counter and generation
+  double* gred;  // grid mode: root reductions shared by all CTAs
+  int* err;
   float* buf;    // smem: this warp's scan buffer [3 * vstride] (null for warps >= bufs)
   int bufs;      // warps 0 .. bufs-1 own a scan buffer
   int owner;     // >= 0: adjoint pass, terminal values are player owner's payoffs (see warp_terms)
@@ -522,27 +528,65 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
 // ---------------------------------------------------------------------------
 // Pass driver and root reductions
 // ---------------------------------------------------------------------------
+// Grid barrier of a cooperative launch (all CTAs resident): a counter and a
+// generation word in global memory, device-scope release / acquire.  The wait
+// gives up after kGridSpin polls and reports ERR_WAIT, so a failed launch ends
+// with an error instead of a hung GPU.
+constexpr int kGridSpin = 1 << 24;  // polls of the generation word (~1 s with the back-off)
+__device__ void grid_barrier(const Ctx& c) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> count(c.bar[0]), gen(c.bar[1]);
+    const unsigned g = gen.load(cuda::memory_order_acquire);
+    if (count.fetch_add(1u, cuda::memory_order_acq_rel) == gridDim.x - 1) {
+      count.store(0u, cuda::memory_order_relaxed);
+      gen.store(g + 1u, cuda::memory_order_release);
+    } else {
+      for (int n = 0; gen.load(cuda::memory_order_acquire) == g; ++n) {
+        if (n >= kGridSpin) {
+          atomicOr(c.err, ERR_WAIT);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void step_barrier(const Ctx& c) {
+  if (c.grid)
+    grid_barrier(c);
+  else
+    __syncthreads();
+}
+
 __device__ __noinline__ void run_pass(const Ctx& c, int p, const Discount dc, int mode) {
   const SpotDev& sp = *c.sp;
   const Step* steps = sp.steps[p];
   const Op* ops = sp.ops[p];
   const uint16_t* groups = sp.groups[p];
   const int o = p ^ 1;
-  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5, nw0 = blockDim.x >> 5;
+  // in grid mode the items of a step are spread over the warps of all CTAs
+  const int nw = c.grid ? gridDim.x * nw0 : nw0;
+  const int gw = c.grid ? blockIdx.x * nw0 + warp : warp;
+  const int nb = c.grid ? gridDim.x * c.bufs : c.bufs;
+  const int gb = c.grid ? blockIdx.x * c.bufs + warp : warp;
   for (int s = 0; s < sp.nsteps[p]; ++s) {
     const Step st = steps[s];
     // terminal runs go round robin to the warps that own a scan buffer; node
     // ops go round robin to all warps, starting at the first warp without a run
     if (warp < c.bufs)
-      for (int j = warp; j < st.n_groups; j += c.bufs) {
+      for (int j = gb; j < st.n_groups; j += nb) {
         const Op* lead = ops + st.begin + st.n_elem + groups[st.gbegin + j];
         if (c.owner >= 0 || c.signed_reach || c.bgrad)
           warp_terms<true>(c, lead, lead->na, p);
         else
           warp_terms<false>(c, lead, lead->na, p);
       }
-    const int start = min(st.n_groups, c.bufs) % nw;
-    for (int i = (warp - start + nw) % nw; i < st.n_elem; i += nw) {
+    const int start = min(st.n_groups, nb) % nw;
+    for (int i = (gw - start + nw) % nw; i < st.n_elem; i += nw) {
       const Op op = ops[st.begin + i];
       PHASE_T0(t_op);
       switch (op.type) {
@@ -560,7 +604,8 @@ __device__ __noinline__ void run_pass(const Ctx& c, int p, const Discount dc, in
                                            : PH_BWD_CHANCE,
                 t_op);
     }
-    __syncthreads();
+    PHASE_T0(t_bar);
+    step_barrier(c);
     PHASE_ADD(PH_BARRIER, t_bar);
   }
 }
@@ -583,6 +628,18 @@ __device__ double block_dot_f64(const Ctx& c, const float* w, const float* v, in
 
 // Exploitability (utility.rs:380-392, :450-543): best-response passes for both
 // players, root values weighted by the initial ranges in f64.
+// Root value sum_h w[h] v[h] in f64 on every thread; in grid mode CTA 0
+// reduces and publishes it to the others through a grid barrier.
+__device__ double root_dot(const Ctx& c, const float* w, const float* v, int n, int slot) {
+  if (!c.grid) return block_dot_f64(c, w, v, n);
+  if (blockIdx.x == 0) {
+    const double d = block_dot_f64(c, w, v, n);
+    if (threadIdx.x == 0) c.gred[slot] = d;
+  }
+  grid_barrier(c);
+  return *reinterpret_cast<volatile double*>(c.gred + slot);
+}
+
 __device__ float spot_exploitability(Ctx& c) {
   const SpotDev& sp = *c.sp;
   const Discount dz{0.f, 0.f, 0.f, 0.f};
@@ -590,14 +647,14 @@ __device__ float spot_exploitability(Ctx& c) {
   for (int p = 0; p < 2; ++p) {
     c.root_reach = sp.w[p ^ 1];
     run_pass(c, p, dz, M_BR);
-    mes[p] = (float)block_dot_f64(c, sp.w[p], slot_at(c, sp.root_slot[p]), sp.H[p]);
+    mes[p] = (float)root_dot(c, sp.w[p], slot_at(c, sp.root_slot[p]), sp.H[p], p);
   }
   if (!sp.raked) return (mes[0] + mes[1]) * 0.5f;
   float cur[2];
   for (int p = 0; p < 2; ++p) {
     c.root_reach = sp.w[p ^ 1];
     run_pass(c, p, dz, M_AVG);
-    cur[p] = (float)block_dot_f64(c, sp.w[p], slot_at(c, sp.root_slot[p]), sp.H[p]);
+    cur[p] = (float)root_dot(c, sp.w[p], slot_at(c, sp.root_slot[p]), sp.H[p], 2 + p);
   }
   return ((mes[0] - cur[0]) + (mes[1] - cur[1])) * 0.5f;
 }
@@ -619,6 +676,10 @@ __device__ bool bind_ctx(Ctx& c, const SpotDev* sp, float* scratch, size_t scrat
   c.owner = -1;
   c.signed_reach = 0;
   c.bgrad = nullptr;
+  c.grid = 0;
+  c.bar = nullptr;
+  c.gred = nullptr;
+  c.err = err;
   c.slots = scratch;
   char* p = smem;
   const int tb = table_bytes_for(sp->hs[0], sp->hs[1]);
@@ -704,6 +765,40 @@ __global__ void PS_SOLVE_BOUNDS k_solve(const SpotDev* __restrict__ spots, int n
       out_expl[si] = expl;
       out_iters[si] = t;
     }
+  }
+}
+
+// One spot on every CTA of a cooperative launch (large trees): the solve loop
+// of k_solve, a fixed iteration range, or an exploitability evaluation
+// (kind 0 / 1 / 2).  All CTAs run the same loop and take the same decisions:
+// the exploitability reaches them through root_dot.
+__global__ void PS_SOLVE_BOUNDS k_grid(const SpotDev* __restrict__ spot, int kind, const Discount* __restrict__ disc,
+                                       int t0, int t1, float target, float* scratch, size_t scratch_floats,
+                                       float* out_expl, int* out_iters, unsigned* bar, double* gred, SmemPlan plan,
+                                       int* err) {
+  extern __shared__ float4 smem4[];
+  char* smem = reinterpret_cast<char*>(smem4);
+  Ctx c;
+  const bool ok = bind_ctx(c, spot, scratch, scratch_floats, smem, plan, err);
+  if (!ok) return;  // the check is the same on every CTA
+  c.grid = 1;
+  c.bar = bar;
+  c.gred = gred;
+  if (kind == 1) {
+    for (int t = t0; t < t1; ++t) dcfr_iteration(c, disc[t]);
+    return;
+  }
+  float expl = spot_exploitability(c);
+  int t = 0;
+  if (kind == 0)
+    for (; t < t1; ++t) {
+      if (expl <= target) break;
+      dcfr_iteration(c, disc[t]);
+      if ((t + 1) % 5 == 0 || t + 1 == t1) expl = spot_exploitability(c);
+    }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *out_expl = expl;
+    if (out_iters) *out_iters = t;
   }
 }
 
@@ -1011,6 +1106,30 @@ cudaError_t launch_solve(const SpotDev* spots, int nspots, const int* order, int
   k_solve<<<grid, block, smem, s>>>(spots, nspots, order, counter, disc, max_iter, target, scratch, scratch_floats,
                                      out_expl, out_iters, plan, err);
   return cudaGetLastError();
+}
+
+int grid_ctas(int block, const SmemPlan& plan) {
+  int dev = 0, nsm = 0, per_sm = 0;
+  size_t smem = plan.total();
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  if (set_smem((const void*)k_grid, smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grid, block, smem) != cudaSuccess) return 0;
+  return nsm * per_sm;
+}
+
+cudaError_t launch_grid(const SpotDev* spot, int kind, const Discount* disc, int t0, int t1, float target,
+                        float* scratch, size_t scratch_floats, float* out_expl, int* out_iters, unsigned* bar,
+                        double* gred, int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s) {
+  size_t smem = plan.total();
+  cudaError_t e = set_smem((const void*)k_grid, smem);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  void* args[] = {(void*)&spot, (void*)&kind,     (void*)&disc,      (void*)&t0,  (void*)&t1,
+                  (void*)&target, (void*)&scratch, (void*)&scratch_floats, (void*)&out_expl, (void*)&out_iters,
+                  (void*)&bar,  (void*)&gred,     (void*)&plan,      (void*)&err};
+  return cudaLaunchCooperativeKernel((const void*)k_grid, dim3(grid), dim3(block), args, smem, s);
 }
 
 cudaError_t launch_iterate(const SpotDev* spots, int nspots, const Discount* disc, int t0, int t1, float* scratch,

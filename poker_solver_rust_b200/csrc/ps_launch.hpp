@@ -36,6 +36,13 @@ struct SmemPlan {
 constexpr int kMaxSolveBlock = 256;  // threads per CTA the solve kernels are compiled for (launch bounds)
 size_t setup_smem_bytes();
 int solve_occupancy(int block, const SmemPlan& plan);
+// Grid mode for one large spot: CTAs that can be co-resident for k_grid, and
+// its cooperative launch (kind 0: solve loop to t1 iterations or `target`;
+// 1: iterations [t0, t1); 2: exploitability only).  bar: 2 unsigned, gred: 4 double.
+int grid_ctas(int block, const SmemPlan& plan);
+cudaError_t launch_grid(const SpotDev* spot, int kind, const Discount* disc, int t0, int t1, float target,
+                        float* scratch, size_t scratch_floats, float* out_expl, int* out_iters, unsigned* bar,
+                        double* gred, int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s);
 cudaError_t launch_setup(const SpotDev* spots, const int2* work, int nwork, const int32_t* table, int* err,
                          int grid, cudaStream_t s);
 cudaError_t launch_solve(const SpotDev* spots, int nspots, const int* order, int* counter, const Discount* disc,

@@ -398,6 +398,27 @@ def test_batch_autotune_keeps_results():
     assert np.allclose(e0, e1, rtol=1e-5, atol=0)
 
 
+def test_grid_mode_matches_single_cta(monkeypatch):
+    """A large single tree runs on every CTA of a cooperative launch; the
+    arithmetic of each item does not depend on which warp runs it, so the
+    state matches the one-CTA run bit for bit."""
+    r, b, t = spots.turn_spot(8, weights=_sparse)
+    grid = spots.product_game(r, b, t)            # default: grid mode for trees >= 2000 nodes
+    assert grid.num_nodes() >= 2000
+    monkeypatch.setenv("PS_GRID_NODES", "0")
+    one = spots.product_game(r, b, t)
+    for it in range(4):
+        ps.solve_step(grid, it)
+        ps.solve_step(one, it)
+    assert ps.compute_exploitability(grid) == ps.compute_exploitability(one)
+    for i in _decision_nodes(grid)[:50]:
+        assert np.array_equal(grid.node_storage(i, 2), one.node_storage(i, 2))
+        assert np.array_equal(grid.node_storage(i, 1), one.node_storage(i, 1))
+    e1 = ps.solve(grid, 12, 0.0)
+    e2 = ps.solve(one, 12, 0.0)
+    assert e1 == e2 and grid.last_iterations == one.last_iterations
+
+
 def test_state_export_import():
     r, board, tc = spots.river_spot(7)
     g = spots.product_game(r, board, tc)
