@@ -511,6 +511,21 @@ struct Batch {
     return PS_OK;
   }
 
+  // One grid-mode launch of this batch's single spot.
+  cudaError_t grid_launch(const GridJob& job) {
+    return launch_grid(d_spots, job, d_disc, d_scratch, scratch_floats, d_expl, d_iters, d_bar, d_gred, d_err,
+                       grid_blocks, block, plan, stream);
+  }
+
+  // Average-strategy pass(es) of the single spot: on every SM in grid mode,
+  // on one CTA otherwise (k_average).
+  cudaError_t average(int save, int player, const float* root_reach, float* out, int owner, float* bgrad) {
+    if (grid_mode)
+      return grid_launch({save ? GRID_FINALIZE : GRID_AVERAGE, 0, 0, 0.f, player, owner, root_reach, bgrad, out});
+    return launch_average(d_spots, 1, save, player, root_reach, d_scratch, scratch_floats, out, d_err, 1, block, plan,
+                          stream, owner, bgrad);
+  }
+
   // Zeroes the solver state and rebuilds the per-board tables on the device.
   int enqueue_setup() {
     CU(cudaMemsetAsync(pool + static_bytes + setup_bytes, 0, state_bytes, stream));
@@ -557,8 +572,9 @@ struct Batch {
       if (fresh && (rc = run_setup())) return rc;
       CU(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
       CU(cudaEventRecord(ev[2], stream));
-      CU(launch_grid(d_spots, 0, d_disc, 0, (int)max_iter, target[0], d_scratch, scratch_floats, d_expl, d_iters,
-                     d_bar, d_gred, d_err, grid_blocks, block, plan, stream));
+      GridJob job{GRID_SOLVE, 0, (int)max_iter, target[0], 0, -1, nullptr, nullptr, nullptr};
+      CU(launch_grid(d_spots, job, d_disc, d_scratch, scratch_floats, d_expl, d_iters, d_bar, d_gred, d_err,
+                     grid_blocks, block, plan, stream));
       CU(cudaEventRecord(ev[3], stream));
       h_expl.resize(1);
       h_iters.resize(1);
@@ -650,8 +666,7 @@ float expl_run(ps_game* G, int* rc) {
   float e = 0;
   cudaError_t ce = cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream);
   if (ce == cudaSuccess && B.grid_mode)
-    ce = launch_grid(B.d_spots, 2, B.d_disc, 0, 0, 0.f, B.d_scratch, B.scratch_floats, B.d_expl, nullptr, B.d_bar,
-                     B.d_gred, B.d_err, B.grid_blocks, B.block, B.plan, B.stream);
+    ce = B.grid_launch({GRID_EXPL, 0, 0, 0.f, 0, -1, nullptr, nullptr, nullptr});
   else if (ce == cudaSuccess)
     ce = launch_exploitability(B.d_spots, 1, B.d_scratch, B.scratch_floats, B.d_expl, B.d_err, 1, B.block, B.plan,
                                B.stream);
@@ -823,8 +838,7 @@ int ps_solve_step(ps_game* G, uint32_t t) {
   if ((rc = B.ensure_disc(t + 1))) return rc;
   CU(cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream));
   if (B.grid_mode)
-    CU(launch_grid(B.d_spots, 1, B.d_disc, (int)t, (int)t + 1, 0.f, B.d_scratch, B.scratch_floats, B.d_expl,
-                   nullptr, B.d_bar, B.d_gred, B.d_err, B.grid_blocks, B.block, B.plan, B.stream));
+    CU(B.grid_launch({GRID_ITERATE, (int)t, (int)t + 1, 0.f, 0, -1, nullptr, nullptr, nullptr}));
   else
     CU(launch_iterate(B.d_spots, 1, B.d_disc, (int)t, (int)t + 1, B.d_scratch, B.scratch_floats, B.d_err, 1,
                       B.block, B.plan, B.stream));
@@ -867,8 +881,7 @@ int ps_finalize(ps_game* G) {
   if ((rc = need_boundaries(G))) return rc;
   Batch& B = *G->b;
   CU(cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream));
-  CU(launch_average(B.d_spots, 1, 1, 0, nullptr, B.d_scratch, B.scratch_floats, nullptr, B.d_err, 1, B.block,
-                    B.plan, B.stream));
+  CU(B.average(1, 0, nullptr, nullptr, -1, nullptr));
   if ((rc = B.check_err())) return rc;
   G->state = GState::Solved;
   G->host_dirty = true;
@@ -895,8 +908,7 @@ int ps_root_cfvalues_with_reach(ps_game* G, int player, const float* opp_reach, 
   CU(cudaMalloc(&d_out, 4 * (size_t)g.hs[player]));
   CU(cudaMemcpyAsync(d_reach, r.data(), 4 * r.size(), cudaMemcpyHostToDevice, B.stream));
   CU(cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream));
-  CU(launch_average(B.d_spots, 1, 0, player, d_reach, B.d_scratch, B.scratch_floats, d_out, B.d_err, 1, B.block,
-                    B.plan, B.stream));
+  CU(B.average(0, player, d_reach, d_out, -1, nullptr));
   CU(cudaMemcpyAsync(out, d_out, 4 * (size_t)g.H[player], cudaMemcpyDeviceToHost, B.stream));
   CU(cudaStreamSynchronize(B.stream));
   cudaFree(d_reach);
@@ -939,16 +951,12 @@ static int fixed_strategy_run(ps_game* G, const float* w0, const float* w1, cons
   }
   CU(cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream));
   // forward: cfv_p from the opponent's weights (utility.rs:422-443)
-  CU(launch_average(B.d_spots, 1, 0, 0, dv[1], B.d_scratch, B.scratch_floats, dv[2], B.d_err, 1, B.block, B.plan,
-                    B.stream, -1, d_bg));
-  CU(launch_average(B.d_spots, 1, 0, 1, dv[0], B.d_scratch, B.scratch_floats, dv[3], B.d_err, 1, B.block, B.plan,
-                    B.stream, -1, d_bg));
+  CU(B.average(0, 0, dv[1], dv[2], -1, d_bg));
+  CU(B.average(0, 1, dv[0], dv[3], -1, d_bg));
   if (adjoint) {
     // cotangent of cfv_0 flows into player 1's weights and player 0's boundary values, and vice versa
-    CU(launch_average(B.d_spots, 1, 0, 1, dv[4], B.d_scratch, B.scratch_floats, dv[7], B.d_err, 1, B.block, B.plan,
-                      B.stream, 0, d_bg));
-    CU(launch_average(B.d_spots, 1, 0, 0, dv[5], B.d_scratch, B.scratch_floats, dv[6], B.d_err, 1, B.block, B.plan,
-                      B.stream, 1, d_bg));
+    CU(B.average(0, 1, dv[4], dv[7], 0, d_bg));
+    CU(B.average(0, 0, dv[5], dv[6], 1, d_bg));
   }
   if (cfv0) CU(cudaMemcpyAsync(cfv0, dv[2], 4 * (size_t)g.H[0], cudaMemcpyDeviceToHost, B.stream));
   if (cfv1) CU(cudaMemcpyAsync(cfv1, dv[3], 4 * (size_t)g.H[1], cudaMemcpyDeviceToHost, B.stream));

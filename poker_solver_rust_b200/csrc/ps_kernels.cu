@@ -768,14 +768,17 @@ __global__ void PS_SOLVE_BOUNDS k_solve(const SpotDev* __restrict__ spots, int n
   }
 }
 
-// One spot on every CTA of a cooperative launch (large trees): the solve loop
-// of k_solve, a fixed iteration range, or an exploitability evaluation
-// (kind 0 / 1 / 2).  All CTAs run the same loop and take the same decisions:
-// the exploitability reaches them through root_dot.
-__global__ void PS_SOLVE_BOUNDS k_grid(const SpotDev* __restrict__ spot, int kind, const Discount* __restrict__ disc,
-                                       int t0, int t1, float target, float* scratch, size_t scratch_floats,
-                                       float* out_expl, int* out_iters, unsigned* bar, double* gred, SmemPlan plan,
-                                       int* err) {
+// One spot on every CTA of a cooperative launch (large trees).  All CTAs run
+// the same loop and take the same decisions: the exploitability reaches them
+// through root_dot.  job.kind:
+//   GRID_SOLVE    the solve loop of k_solve to job.t1 iterations or job.target
+//   GRID_ITERATE  iterations [job.t0, job.t1), no checks
+//   GRID_EXPL     exploitability only
+//   GRID_FINALIZE the average-strategy passes that store the query values
+//   GRID_AVERAGE  one average pass of job.player (k_average with save == 0)
+__global__ void PS_SOLVE_BOUNDS k_grid(const SpotDev* __restrict__ spot, const Discount* __restrict__ disc,
+                                       float* scratch, size_t scratch_floats, float* out_expl, int* out_iters,
+                                       unsigned* bar, double* gred, GridJob job, SmemPlan plan, int* err) {
   extern __shared__ float4 smem4[];
   char* smem = reinterpret_cast<char*>(smem4);
   Ctx c;
@@ -784,17 +787,40 @@ __global__ void PS_SOLVE_BOUNDS k_grid(const SpotDev* __restrict__ spot, int kin
   c.grid = 1;
   c.bar = bar;
   c.gred = gred;
-  if (kind == 1) {
-    for (int t = t0; t < t1; ++t) dcfr_iteration(c, disc[t]);
-    return;
+  const SpotDev& sp = *spot;
+  const Discount dz{0.f, 0.f, 0.f, 0.f};
+  switch (job.kind) {
+    case GRID_ITERATE:
+      for (int t = job.t0; t < job.t1; ++t) dcfr_iteration(c, disc[t]);
+      return;
+    case GRID_FINALIZE:
+      for (int p = 0; p < 2; ++p) {
+        c.root_reach = sp.w[p ^ 1];
+        run_pass(c, p, dz, M_AVG_SAVE);
+      }
+      return;
+    case GRID_AVERAGE: {
+      c.root_reach = job.root_reach ? job.root_reach : sp.w[job.player ^ 1];
+      c.signed_reach = job.root_reach != nullptr;
+      c.owner = job.owner;
+      c.bgrad = job.bgrad;
+      run_pass(c, job.player, dz, M_AVG);
+      if (blockIdx.x == 0) {
+        const float* r = slot_at(c, sp.root_slot[job.player]);
+        for (int h = threadIdx.x; h < sp.H[job.player]; h += blockDim.x) job.out[h] = r[h];
+      }
+      return;
+    }
+    default:
+      break;
   }
   float expl = spot_exploitability(c);
   int t = 0;
-  if (kind == 0)
-    for (; t < t1; ++t) {
-      if (expl <= target) break;
+  if (job.kind == GRID_SOLVE)
+    for (; t < job.t1; ++t) {
+      if (expl <= job.target) break;
       dcfr_iteration(c, disc[t]);
-      if ((t + 1) % 5 == 0 || t + 1 == t1) expl = spot_exploitability(c);
+      if ((t + 1) % 5 == 0 || t + 1 == job.t1) expl = spot_exploitability(c);
     }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     *out_expl = expl;
@@ -1118,17 +1144,18 @@ int grid_ctas(int block, const SmemPlan& plan) {
   return nsm * per_sm;
 }
 
-cudaError_t launch_grid(const SpotDev* spot, int kind, const Discount* disc, int t0, int t1, float target,
-                        float* scratch, size_t scratch_floats, float* out_expl, int* out_iters, unsigned* bar,
-                        double* gred, int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s) {
+cudaError_t launch_grid(const SpotDev* spot, const GridJob& job, const Discount* disc, float* scratch,
+                        size_t scratch_floats, float* out_expl, int* out_iters, unsigned* bar, double* gred,
+                        int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s) {
   size_t smem = plan.total();
   cudaError_t e = set_smem((const void*)k_grid, smem);
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
-  void* args[] = {(void*)&spot, (void*)&kind,     (void*)&disc,      (void*)&t0,  (void*)&t1,
-                  (void*)&target, (void*)&scratch, (void*)&scratch_floats, (void*)&out_expl, (void*)&out_iters,
-                  (void*)&bar,  (void*)&gred,     (void*)&plan,      (void*)&err};
+  GridJob j = job;
+  SmemPlan pl = plan;
+  void* args[] = {(void*)&spot, (void*)&disc, (void*)&scratch, (void*)&scratch_floats, (void*)&out_expl,
+                  (void*)&out_iters, (void*)&bar, (void*)&gred, (void*)&j, (void*)&pl, (void*)&err};
   return cudaLaunchCooperativeKernel((const void*)k_grid, dim3(grid), dim3(block), args, smem, s);
 }
 

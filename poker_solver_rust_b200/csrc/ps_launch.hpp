@@ -36,13 +36,23 @@ struct SmemPlan {
 constexpr int kMaxSolveBlock = 256;  // threads per CTA the solve kernels are compiled for (launch bounds)
 size_t setup_smem_bytes();
 int solve_occupancy(int block, const SmemPlan& plan);
-// Grid mode for one large spot: CTAs that can be co-resident for k_grid, and
-// its cooperative launch (kind 0: solve loop to t1 iterations or `target`;
-// 1: iterations [t0, t1); 2: exploitability only).  bar: 2 unsigned, gred: 4 double.
+// Grid mode for one large spot: the work of one cooperative launch of k_grid
+// (every CTA on the same spot), the number of CTAs that can be co-resident for
+// it, and the launch.  bar: 2 unsigned, gred: 4 double, both device memory.
+enum GridKind { GRID_SOLVE = 0, GRID_ITERATE = 1, GRID_EXPL = 2, GRID_FINALIZE = 3, GRID_AVERAGE = 4 };
+struct GridJob {
+  int kind;
+  int t0, t1;              // iteration range (GRID_ITERATE) / max iterations (GRID_SOLVE)
+  float target;            // GRID_SOLVE: stop once exploitability <= target
+  int player, owner;       // GRID_AVERAGE: traverser and payoff owner (-1 = the traverser)
+  const float* root_reach; // GRID_AVERAGE: opponent reach at the root (null = initial weights)
+  float* bgrad;            // GRID_AVERAGE: boundary gradient buffer or null
+  float* out;              // GRID_AVERAGE: root values [H_player]
+};
 int grid_ctas(int block, const SmemPlan& plan);
-cudaError_t launch_grid(const SpotDev* spot, int kind, const Discount* disc, int t0, int t1, float target,
-                        float* scratch, size_t scratch_floats, float* out_expl, int* out_iters, unsigned* bar,
-                        double* gred, int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s);
+cudaError_t launch_grid(const SpotDev* spot, const GridJob& job, const Discount* disc, float* scratch,
+                        size_t scratch_floats, float* out_expl, int* out_iters, unsigned* bar, double* gred,
+                        int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s);
 cudaError_t launch_setup(const SpotDev* spots, const int2* work, int nwork, const int32_t* table, int* err,
                          int grid, cudaStream_t s);
 cudaError_t launch_solve(const SpotDev* spots, int nspots, const int* order, int* counter, const Discount* disc,
