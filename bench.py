@@ -135,6 +135,37 @@ def replicas_throughput(spots_per_rank: int, world: int, step_ms_max: float) -> 
     return world * spots_per_rank / (step_ms_max / 1e3)
 
 
+def turn_game_measure(ps, spots, iters: int, cpu_iters: int):
+    """One turn subgame (4-card board, 48 river deals, U[0,1] ranges, pot 100,
+    stack 300, bets 33% / 75% / all-in, raise 60%) solved for a fixed number of
+    iterations on the whole GPU (grid mode), timed through ps.solve from host
+    to host (exploitability every 5 iterations and finalize included), beside
+    the oracle's time for `cpu_iters` iterations on one host thread."""
+    import torch
+
+    r, b, t = spots.turn_spot(2)
+    warm = spots.product_game(r, b, t)
+    ps.solve(warm, 5, 0.0)
+    g = spots.product_game(r, b, t)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e = ps.solve(g, iters, 0.0)
+    dt = time.perf_counter() - t0
+    out = {"workload": "turn subgame: 4-card board, 48 river deals, pot 100, stack 300, bets 33%/75%/a, raise 60%",
+           "nodes": g.num_nodes(), "hands": [g.num_private_hands(0), g.num_private_hands(1)],
+           "iterations": iters, "gpu_ms_per_iteration": dt / iters * 1e3,
+           "gpu_note": "ps.solve from host: iterations, exploitability every 5, finalize",
+           "exploitability_pct_pot": 100.0 * e / t.starting_pot}
+    if cpu_iters > 0:
+        o = spots.oracle_game(r, b, t)
+        t0 = time.perf_counter()
+        for it in range(cpu_iters):
+            o.solve_step(it)
+        out["cpu_ms_per_iteration"] = (time.perf_counter() - t0) / cpu_iters * 1e3
+        out["cpu"] = {"threads": 1, "kind": "port", "iterations_timed": cpu_iters}
+    return out
+
+
 def make_workload(n_spots: int, seed: int):
     from tests import spots
 
@@ -201,6 +232,8 @@ def main():
     ap.add_argument("--block", type=int, default=-1, help="threads per CTA; -1 = autotune, 0 = library default")
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--turn-iters", type=int, default=500, help="single turn game iterations (0 = skip)")
+    ap.add_argument("--turn-cpu-iters", type=int, default=1)
     ap.add_argument("--stage", type=int, default=-1)
     ap.add_argument("--bufs", type=int, default=0, help="terminal scan buffers per CTA (0 = one per warp)")
     args = ap.parse_args()
@@ -300,6 +333,11 @@ def main():
         plain = {"value": len(sample) / plain_s, "unit": UNIT, "sample": f"first {len(sample)} spots, one "
                  "game + single-CTA solve launch per spot, host-synchronised"}
 
+    # ---- single turn game (config 2 of the spec), grid mode ----
+    turn = None
+    if rank == 0 and args.turn_iters > 0:
+        turn = turn_game_measure(ps, spots, args.turn_iters, args.turn_cpu_iters)
+
     # ---- CPU baseline (oracle) on a bounded sample ----
     cpu = None
     if rank == 0 and args.cpu_sample > 0:
@@ -332,6 +370,7 @@ def main():
                                          "spot-iterations (profiles/k_solve_river_datagen_1024.md)"},
             "cpu_baseline": cpu,
             "plain_gpu": plain,
+            "turn_game": turn,
             "clocks": clocks,
             "detail": {"setup_ms": statistics.median(setup_ms), "solve_ms": statistics.median(solve_ms),
                        "mean_iterations": float(iters.mean()), "max_iterations": int(iters.max()),
