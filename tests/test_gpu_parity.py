@@ -419,6 +419,47 @@ def test_grid_mode_matches_single_cta(monkeypatch):
     assert e1 == e2 and grid.last_iterations == one.last_iterations
 
 
+@pytest.mark.parametrize("case", [0, 1, 2])
+def test_regret_matching_known_answers(case):
+    """solver.rs:724-750 on the device: one iteration at t = 0 (gamma_0 = 0)
+    leaves the strategy sum equal to the regret-matched seeded regrets."""
+    from tests.test_oracle_pins import REGRET_CASES, _decision_node, _fixture_oracle, _tile
+
+    pattern, na, expected = REGRET_CASES[case]
+    r, board, tc = _fixture_oracle()
+    g = spots.product_game(r, board, tc)
+    idx = _decision_node(g, na, 0)
+    H = g.num_private_hands(0)
+    g.seed_node_storage(idx, 2, _tile(pattern, na, H))
+    ps.solve_step(g, 0)
+    want = np.full(na * H, 1.0 / na) if expected is None else _tile(expected, na, H)
+    assert np.abs(g.node_storage(idx, 1) - want).max() < 1e-6
+
+
+def test_normalized_strategy_known_answers():
+    """utility.rs:1012-1036 through the product's strategy query."""
+    from tests.test_oracle_pins import _decision_node, _fixture_oracle, _tile
+
+    r, board, tc = _fixture_oracle()
+    g = spots.product_game(r, board, tc)
+    idx = _decision_node(g, 2, 1)
+    H = g.num_private_hands(1)
+    g.seed_node_storage(idx, 1, np.zeros(2 * H, np.float32))
+    assert np.abs(g.strategy_at_index(idx) - 0.5).max() < 1e-6
+    g.seed_node_storage(idx, 1, _tile([1.0, 3.0, 3.0, 1.0], 2, H))
+    assert np.abs(g.strategy_at_index(idx) - _tile([0.25, 0.75, 0.75, 0.25], 2, H)).max() < 1e-6
+
+
+def test_early_termination():
+    """solver.rs:808-838: a target above the starting exploitability stops at once."""
+    from tests.test_oracle_pins import _fixture_oracle
+
+    r, board, tc = _fixture_oracle()
+    g = spots.product_game(r, board, tc)
+    e = ps.solve(g, 1000, 1e10)
+    assert e >= 0.0 and g.last_iterations == 0
+
+
 def test_state_export_import():
     r, board, tc = spots.river_spot(7)
     g = spots.product_game(r, board, tc)

@@ -157,3 +157,108 @@ def test_oracle_evaluation_properties():
                 assert (v >= 0).all() if folded != p else (v <= 0).all()
                 z = g.evaluate_node(idx, p, np.zeros(g.num_private_hands(p ^ 1), np.float32))
                 assert (z == 0).all()
+
+
+# ---- known answers of the reference's own unit tests (restated here) ----
+
+def test_card_known_answers():
+    # card.rs:418-490 (encoding, pair index round trip, strings, flop parser)
+    import poker_solver_rust_b200 as ps
+
+    assert ps.card_from_str("2c") == 0 and ps.card_from_str("As") == 51
+    assert ps.card_to_string(0) == "2c" and ps.card_to_string(51) == "As"
+    assert [ps.card_to_string(c) for c in (5, 10)] == ["3d", "4h"]
+    with pytest.raises(ValueError):
+        ps.card_to_string(52)
+    k = 0
+    for i in range(52):
+        for j in range(i + 1, 52):
+            assert ps.card_pair_to_index(i, j) == k == ps.card_pair_to_index(j, i)
+            assert tuple(ps.index_to_card_pair(k)) == (i, j)
+            k += 1
+    assert k == 1326
+    assert ps.hole_to_string((0, 5)) == "3d2c" and ps.hole_to_string((10, 51)) == "As4h"
+    assert ps.holes_to_strings([(0, 5), (10, 51)]) == ["3d2c", "As4h"]
+    assert list(ps.flop_from_str("2c3d4h")) == [0, 5, 10]
+    assert list(ps.flop_from_str("As Ah Ks")) == [47, 50, 51]
+    for bad in ("2c3d4h5s", "2c2c3d"):
+        with pytest.raises(ValueError):
+            ps.flop_from_str(bad)
+
+
+def test_compute_average_known_answers():
+    # utility.rs:1054-1064
+    import poker_solver_rust_b200 as ps
+
+    assert ps.compute_average([1.0, 2.0, 3.0], [1.0, 1.0, 1.0]) == pytest.approx(2.0, abs=1e-6)
+    assert ps.compute_average([1.0, 2.0, 3.0], [0.0, 0.0, 1.0]) == pytest.approx(3.0, abs=1e-6)
+
+
+def _fixture_oracle():
+    import poker_solver_rust_b200 as ps
+    from poker_solver_rust_b200 import BetSizeOptions as B, BoardState, TreeConfig
+
+    r = [ps.Range.from_str("AA,KK,QQ,AKs").raw_data(), ps.Range.from_str("QQ-JJ,AQs,AJs").raw_data()]
+    board = ps.flop_from_str("Qs Jh 2c") + [ps.card_from_str("8d"), ps.card_from_str("3s")]
+    s = B("50%, a", "")
+    tc = TreeConfig(initial_state=BoardState.River, starting_pot=100, effective_stack=100, river_bet_sizes=[s, s])
+    return r, board, tc
+
+
+def _decision_node(g, actions, player):
+    for i in range(g.num_nodes()):
+        info = g.node_info(i)
+        if not info["player"] & (4 | 8) and info["num_children"] == actions and info["player"] == player:
+            return i
+    raise AssertionError("no such node")
+
+
+# (regrets per action-major row pattern, actions, expected strategy) of
+# solver.rs:724-750; the pattern covers two hands and is tiled over the node's hands
+REGRET_CASES = [
+    ([-1.0, -2.0, -3.0, -1.0, -2.0, -3.0], 3, None),  # all negative -> uniform
+    ([1.0, 0.0, 0.0, 3.0], 2, [1.0, 0.0, 0.0, 1.0]),
+    ([2.0, 2.0, 1.0, 1.0], 2, [2.0 / 3.0, 2.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0]),
+]
+
+
+def _tile(pattern, actions, hands):
+    per = len(pattern) // actions  # hands covered by the pattern
+    rows = np.asarray(pattern, np.float32).reshape(actions, per)
+    return np.concatenate([np.resize(rows[a], hands) for a in range(actions)]).astype(np.float32)
+
+
+@pytest.mark.parametrize("case", range(len(REGRET_CASES)))
+def test_oracle_regret_matching_known_answers(case):
+    # one pass at t = 0 (gamma_0 = 0) leaves the strategy sum equal to the
+    # regret-matched strategy of the seeded regrets
+    pattern, na, expected = REGRET_CASES[case]
+    r, board, tc = _fixture_oracle()
+    g = spots.oracle_game(r, board, tc)
+    idx = _decision_node(g, na, 0)
+    H = g.num_private_hands(0)
+    g.seed_node_storage(idx, 2, _tile(pattern, na, H))
+    g.solve_pass(0, 0)
+    got = g.node_storage(idx, 1)
+    want = np.full(na * H, 1.0 / na) if expected is None else _tile(expected, na, H)
+    assert np.abs(got - want).max() < 1e-6
+
+
+def test_oracle_normalized_strategy_known_answers():
+    # utility.rs:1012-1036: zero sums -> uniform; [1, 3 | 3, 1] -> [.25, .75 | .75, .25]
+    r, board, tc = _fixture_oracle()
+    g = spots.oracle_game(r, board, tc)
+    idx = _decision_node(g, 2, 1)
+    H = g.num_private_hands(1)
+    g.seed_node_storage(idx, 1, np.zeros(2 * H, np.float32))
+    assert np.abs(g.strategy_at_index(idx) - 0.5).max() < 1e-6
+    g.seed_node_storage(idx, 1, _tile([1.0, 3.0, 3.0, 1.0], 2, H))
+    assert np.abs(g.strategy_at_index(idx) - _tile([0.25, 0.75, 0.75, 0.25], 2, H)).max() < 1e-6
+
+
+def test_oracle_early_termination():
+    # solver.rs:808-838: a target above the starting exploitability stops before any iteration
+    r, board, tc = _fixture_oracle()
+    g = spots.oracle_game(r, board, tc)
+    e = g.solve(1000, 1e10)
+    assert e >= 0.0 and g.iterations_run == 0
