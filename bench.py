@@ -209,8 +209,9 @@ def run_reference(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded PCG64)",
-        "config": {"workload": f"batched river datagen, {per_step}-spot sample per step of the {args.spots}-spot job",
-                   "target": "0.3% pot", "max_iter": MAX_ITER},
+        "config": {"workload": f"batched river datagen: {args.spots} spots per GPU to <=0.3% pot or "
+                               f"{MAX_ITER} iterations", "parallelism": f"host threads x{threads}",
+                   "timed_sample": f"{per_step} spots of the same workload per step"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{per_step} spots per step, spot-parallel on {threads} threads"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
