@@ -182,6 +182,11 @@ void ps_batch_free(ps_batch* b);
 int ps_batch_solve(ps_batch* b, uint32_t max_iter, const float* target_chips);
 int ps_batch_results(ps_batch* b, float* exploitability, int32_t* iterations);
 int ps_batch_root_strategy(ps_batch* b, int32_t spot, float* out); /* returns count */
+/* root cfvalues of `player` under the average strategy after the last
+ * ps_batch_solve, computed on the device at the end of each spot's solve
+ * (replaces compute_evs_from_strategy_sum, gpu-range-solver batch.rs:799-933);
+ * H_player values, returns the count */
+int ps_batch_root_cfvalues(ps_batch* b, int32_t spot, int player, float* out);
 /* device time in ms of the last ps_batch_solve (setup excluded / included) */
 int ps_batch_last_timing(ps_batch* b, float* solve_ms, float* setup_ms);
 /* algorithmic bytes of one DCFR iteration of spot i: 20 * sum_edges H_actor */

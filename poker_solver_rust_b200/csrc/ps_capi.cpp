@@ -109,7 +109,7 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 struct Layout {  // byte offsets inside the pool
   size_t cards[2], w[2], same[2], ops[2], steps[2], groups[2], nodes, board_cards, iso_perm[2], iso_off, iso_ent;  // static
   size_t gidx[2], coff[2], thr[2], nvalid[2], heads[2];                                                       // setup
-  size_t R, S, ipcfv, chcfv, bcfv;                                                                    // state
+  size_t R, S, ipcfv, chcfv, bcfv, rootv[2];                                                          // state
 };
 
 // ---------------------------------------------------------------------------
@@ -219,6 +219,7 @@ struct Batch {
       L.ipcfv = take(st, g.num_storage_ip * 4 + 16);
       L.chcfv = take(st, g.num_storage_chance * 4 + 16);
       L.bcfv = take(st, (size_t)g.num_boundary * 2 * g.vstride * 4 + 16);
+      for (int p = 0; p < 2; ++p) L.rootv[p] = take(st, (size_t)g.hs[p] * 4);
       max_vstride = std::max(max_vstride, g.vstride);
     }
     static_bytes = so;
@@ -325,6 +326,7 @@ struct Batch {
       s.iso_off = (const int32_t*)(dS + L.iso_off);
       s.iso_ent = (const int32_t*)(dS + L.iso_ent);
       s.bcfv = (const float*)(dT + L.bcfv);
+      for (int p = 0; p < 2; ++p) s.root_out[p] = (float*)(dT + L.rootv[p]);
       s.R = (float*)(dT + L.R);
       s.S = (float*)(dT + L.S);
       s.ipcfv = (float*)(dT + L.ipcfv);
@@ -1554,6 +1556,15 @@ int ps_batch_root_strategy(ps_batch* pb, int32_t spot, float* out) {
     for (int a = 0; a < na; ++a) out[(size_t)a * H + h] = d == 0.0f ? def : S[(size_t)a * hs + h] / d;
   }
   return na * H;
+}
+
+int ps_batch_root_cfvalues(ps_batch* pb, int32_t spot, int player, float* out) {
+  if (!pb || !out || spot < 0 || spot >= (int)pb->b->games.size() || (player != 0 && player != 1))
+    return fail(PS_ERR_INVALID, "bad argument");
+  Batch& B = *pb->b;
+  const int H = B.games[spot]->H[player];
+  CU(cudaMemcpy(out, B.h_spots[spot].root_out[player], 4 * (size_t)H, cudaMemcpyDeviceToHost));
+  return H;
 }
 
 int ps_batch_last_timing(ps_batch* pb, float* solve_ms, float* setup_ms) {

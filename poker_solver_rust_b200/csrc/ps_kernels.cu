@@ -765,6 +765,19 @@ __global__ void PS_SOLVE_BOUNDS k_solve(const SpotDev* __restrict__ spots, int n
       out_expl[si] = expl;
       out_iters[si] = t;
     }
+    // root cfvalues of both players under the average strategy: the
+    // per-hand values a datagen record needs (the reference computes them on
+    // the host from the strategy sums)
+    const SpotDev& sp = spots[si];
+    const Discount dz{0.f, 0.f, 0.f, 0.f};
+    for (int p = 0; p < 2; ++p) {
+      if (!sp.root_out[p]) continue;
+      c.root_reach = sp.w[p ^ 1];
+      run_pass(c, p, dz, M_AVG);
+      const float* r = slot_at(c, sp.root_slot[p]);
+      for (int h = threadIdx.x; h < sp.hs[p]; h += blockDim.x) sp.root_out[p][h] = r[h];
+      __syncthreads();
+    }
   }
 }
 

@@ -478,6 +478,13 @@ class BatchSolver:
         n = N.check(N.lib().ps_batch_root_strategy(self._h, spot, _fp(out)))
         return out[:n].copy()
 
+    def root_cfvalues(self, spot: int, player: int) -> np.ndarray:
+        """Root cfvalues of `player` under the average strategy after the last
+        solve (computed on the device at the end of the spot's solve)."""
+        out = np.zeros(1326, np.float32)
+        n = N.check(N.lib().ps_batch_root_cfvalues(self._h, spot, player, _fp(out)))
+        return out[:n].copy()
+
     def last_timing(self):
         a, b = C.c_float(), C.c_float()
         N.check(N.lib().ps_batch_last_timing(self._h, C.byref(a), C.byref(b)))

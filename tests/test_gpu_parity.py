@@ -373,6 +373,22 @@ def test_batch_matches_single_and_oracle():
     _report("batch", rows)
 
 
+def test_batch_root_cfvalues_match_single_game():
+    """The batch's device-side root cfvalues equal the single game's
+    root_cfvalues after the same solve (same kernels, same arithmetic)."""
+    sp = spots.datagen_spots(5, seed=44)
+    cc = [spots.card_config(r, b) for r, b, _ in sp]
+    tcs = [t for _, _, t in sp]
+    targets = np.array([0.003 * t.starting_pot for t in tcs], np.float32)
+    bs = ps.BatchSolver(cc, tcs)
+    bs.solve(300, targets)
+    for i, (r, b, t) in enumerate(sp):
+        g = spots.product_game(r, b, t)
+        ps.solve(g, 300, float(targets[i]))
+        for p in range(2):
+            assert np.array_equal(bs.root_cfvalues(i, p), ps.root_cfvalues(g, p))
+
+
 def test_batch_autotune_keeps_results():
     """block_threads=-1 times every CTA size on a sample of the batch and keeps
     the fastest; the spots' arithmetic does not depend on the CTA size."""
