@@ -141,6 +141,27 @@ int ps_valid_indices(ps_game* g, int turn, int river, int player, uint16_t* out)
 int64_t ps_num_boundary_nodes(ps_game* g);
 int ps_boundary_node_indices(ps_game* g, int64_t* out);
 int ps_set_boundary_cfvs(ps_game* g, int64_t ordinal, int player, const float* cfvs, int64_t n);
+/* reach of each player at every boundary under the average strategy from the
+ * initial weights (compute_reach_at_nodes, gpu-range-solver batch.rs:765-790;
+ * the range solver's boundary_reach, evaluation.rs:97, holds the same vector
+ * after an average-strategy pass); laid out per ordinal k as [H0 values of
+ * player 0][H1 values of player 1] */
+int ps_boundary_reach(ps_game* g, float* out);
+
+/* ---- turn datagen: boundary values from network outputs ----
+ * The reach-weighted average over the 48 river cards with card blocking of
+ * cfvnet/src/datagen/gpu_boundary_eval.rs:207-269, on the device.  n boundary
+ * items (a request's boundaries, flattened), each with its 4-card board
+ * (host [n][4]), pot and effective stack (host [n]).  Device arrays:
+ *   net   [n][2][48][1326]  network outputs per player, river (the 48 cards not on
+ *                           the board, ascending) and combo (card_pair_to_index order)
+ *   reach [n][2][1326]      OOP and IP reach at the boundary, combo order
+ *   hands [H]               combo index of each output hand
+ *   out   [n][2][H]         player 0 averaged with IP-reach weights, player 1 with OOP
+ * stream: a cudaStream_t (NULL = the default stream); returns after the work is done. */
+int ps_boundary_river_reduce(int32_t n, const uint8_t* boards, const float* pots, const float* stacks,
+                             const float* net, const float* reach, const int32_t* hands, int32_t H, float* out,
+                             void* stream);
 
 /* ---- navigation and queries (game/query.rs) ---- */
 int ps_back_to_root(ps_game* g);

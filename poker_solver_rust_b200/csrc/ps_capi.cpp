@@ -521,11 +521,13 @@ struct Batch {
 
   // Average-strategy pass(es) of the single spot: on every SM in grid mode,
   // on one CTA otherwise (k_average).
-  cudaError_t average(int save, int player, const float* root_reach, float* out, int owner, float* bgrad) {
+  cudaError_t average(int save, int player, const float* root_reach, float* out, int owner, float* bgrad,
+                      float* breach = nullptr) {
     if (grid_mode)
-      return grid_launch({save ? GRID_FINALIZE : GRID_AVERAGE, 0, 0, 0.f, player, owner, root_reach, bgrad, out});
+      return grid_launch(
+          {save ? GRID_FINALIZE : GRID_AVERAGE, 0, 0, 0.f, player, owner, root_reach, bgrad, out, breach});
     return launch_average(d_spots, 1, save, player, root_reach, d_scratch, scratch_floats, out, d_err, 1, block, plan,
-                          stream, owner, bgrad);
+                          stream, owner, bgrad, breach);
   }
 
   // Zeroes the solver state and rebuilds the per-board tables on the device.
@@ -971,6 +973,62 @@ static int fixed_strategy_run(ps_game* G, const float* w0, const float* w1, cons
                            4 * (size_t)g.H[p], cudaMemcpyDeviceToHost, B.stream));
   CU(cudaStreamSynchronize(B.stream));
   return B.check_err();
+}
+
+int ps_boundary_reach(ps_game* G, float* out) {
+  if (!G || !out) return fail(PS_ERR_INVALID, "null argument");
+  if (G->state == GState::TreeBuilt) return fail(PS_ERR_STATE, "Game is not ready");
+  int rc = need_boundaries(G);
+  if (rc) return rc;
+  Batch& B = *G->b;
+  Game& g = *G->g;
+  const size_t nb = (size_t)g.num_boundary;
+  if (nb == 0) return PS_OK;
+  const size_t vec = std::max(g.hs[0], g.hs[1]);
+  float* d = nullptr;
+  CU(cudaMalloc(&d, 4 * (nb * 2 * (size_t)g.vstride + vec)));
+  std::unique_ptr<float, decltype(&cudaFree)> keep(d, &cudaFree);
+  float* d_root = d + nb * 2 * (size_t)g.vstride;
+  CU(cudaMemsetAsync(d, 0, 4 * nb * 2 * (size_t)g.vstride, B.stream));
+  CU(cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream));
+  // traverser 0 records player 1's reach at every boundary, traverser 1 player 0's
+  for (int p = 0; p < 2; ++p) CU(B.average(0, p, nullptr, d_root, -1, nullptr, d));
+  for (size_t k = 0; k < nb; ++k)
+    for (int p = 0; p < 2; ++p)
+      CU(cudaMemcpyAsync(out + k * (g.H[0] + g.H[1]) + (p ? g.H[0] : 0), d + (k * 2 + p) * g.vstride,
+                         4 * (size_t)g.H[p], cudaMemcpyDeviceToHost, B.stream));
+  CU(cudaStreamSynchronize(B.stream));
+  return B.check_err();
+}
+
+int ps_boundary_river_reduce(int32_t n, const uint8_t* boards, const float* pots, const float* stacks,
+                             const float* net, const float* reach, const int32_t* hands, int32_t H, float* out,
+                             void* stream) {
+  if (n < 0 || H < 0 || H > 1326 || (n > 0 && (!boards || !pots || !stacks || !net || !reach || !hands || !out)))
+    return fail(PS_ERR_INVALID, "bad argument");
+  if (n == 0 || H == 0) return PS_OK;
+  std::vector<uint8_t> hb((size_t)n * 4);
+  std::vector<float> dn(n);
+  for (int i = 0; i < n; ++i) {
+    uint64_t seen = 0;
+    for (int k = 0; k < 4; ++k) {
+      const uint8_t c = boards[4 * i + k];
+      if (c >= 52 || (seen >> c & 1)) return fail(PS_ERR_INVALID, "boards must hold 4 distinct cards below 52");
+      seen |= 1ull << c;
+      hb[4 * i + k] = c;
+    }
+    dn[i] = (float)((double)pots[i] + (double)stacks[i]);
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  char* d = nullptr;
+  CU(cudaMalloc(&d, hb.size() + 4 * dn.size() + 16));
+  std::unique_ptr<char, decltype(&cudaFree)> keep(d, &cudaFree);
+  float* d_dn = (float*)(d + ((hb.size() + 15) & ~(size_t)15));
+  CU(cudaMemcpyAsync(d, hb.data(), hb.size(), cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(d_dn, dn.data(), 4 * dn.size(), cudaMemcpyHostToDevice, s));
+  CU(launch_boundary_river_reduce(n, (const uint8_t*)d, d_dn, net, reach, hands, H, out, s));
+  CU(cudaStreamSynchronize(s));
+  return PS_OK;
 }
 
 int ps_eval_fixed_strategy(ps_game* G, const float* w0, const float* w1, float* cfv0, float* cfv1) {

@@ -83,6 +83,7 @@ struct Ctx {
   int owner;     // >= 0: adjoint pass, terminal values are player owner's payoffs (see warp_terms)
   int signed_reach;  // reach may be negative: terminal scans take segment starts from the bitmap
   float* bgrad;  // boundary gradient buffer [num_boundary][2][vstride], or null
+  float* breach; // boundary reach buffer [num_boundary][2][vstride] (reach of each player), or null
   double* red;   // smem: reduction scratch       [32]
   Tables t0;     // board-0 tables (shared memory when staged, else global)
 };
@@ -453,6 +454,10 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
   __syncwarp();
   PHASE_ADD(PH_SCAN, t_scan);
   PHASE_T0(t_look);
+  if (GEN && c.breach && ops[0].term == TERM_BOUNDARY && !adjm) {  // the opponent's reach at this boundary
+    float* row = c.breach + ((size_t)nd0.boundary * 2 + o) * c.vstride;
+    for (int h = lane; h < sp.H[o]; h += 32) row[h] = rch[h];
+  }
   // 3. lookups
   const uint4* thr = T.thr[p];
   const float* cp = buf + V;  // card-group part
@@ -580,7 +585,7 @@ __device__ __noinline__ void run_pass(const Ctx& c, int p, const Discount dc, in
     if (warp < c.bufs)
       for (int j = gb; j < st.n_groups; j += nb) {
         const Op* lead = ops + st.begin + st.n_elem + groups[st.gbegin + j];
-        if (c.owner >= 0 || c.signed_reach || c.bgrad)
+        if (c.owner >= 0 || c.signed_reach || c.bgrad || c.breach)
           warp_terms<true>(c, lead, lead->na, p);
         else
           warp_terms<false>(c, lead, lead->na, p);
@@ -676,6 +681,7 @@ __device__ bool bind_ctx(Ctx& c, const SpotDev* sp, float* scratch, size_t scrat
   c.owner = -1;
   c.signed_reach = 0;
   c.bgrad = nullptr;
+  c.breach = nullptr;
   c.grid = 0;
   c.bar = nullptr;
   c.gred = nullptr;
@@ -817,6 +823,7 @@ __global__ void PS_SOLVE_BOUNDS k_grid(const SpotDev* __restrict__ spot, const D
       c.signed_reach = job.root_reach != nullptr;
       c.owner = job.owner;
       c.bgrad = job.bgrad;
+      c.breach = job.breach;
       run_pass(c, job.player, dz, M_AVG);
       if (blockIdx.x == 0) {
         const float* r = slot_at(c, sp.root_slot[job.player]);
@@ -884,7 +891,7 @@ __global__ void PS_SOLVE_BOUNDS k_exploitability(const SpotDev* __restrict__ spo
 // the other player multiplies it by that player's adjoint reach.
 __global__ void PS_SOLVE_BOUNDS k_average(const SpotDev* __restrict__ spots, int nspots, int save, int player,
                                           const float* root_reach, float* scratch, size_t scratch_floats, float* out,
-                                          int owner, float* bgrad, SmemPlan plan, int* err) {
+                                          int owner, float* bgrad, float* breach, SmemPlan plan, int* err) {
   extern __shared__ float4 smem4[];
   char* smem = reinterpret_cast<char*>(smem4);
   float* my_scratch = scratch + (size_t)blockIdx.x * scratch_floats;
@@ -903,6 +910,7 @@ __global__ void PS_SOLVE_BOUNDS k_average(const SpotDev* __restrict__ spots, int
       c.signed_reach = root_reach != nullptr;
       c.owner = owner;
       c.bgrad = bgrad;
+      c.breach = breach;
       run_pass(c, player, dz, M_AVG);
       const float* r = slot_at(c, sp.root_slot[player]);
       for (int h = threadIdx.x; h < sp.H[player]; h += blockDim.x) out[(size_t)si * sp.hs[player] + h] = r[h];
@@ -1193,12 +1201,12 @@ cudaError_t launch_exploitability(const SpotDev* spots, int nspots, float* scrat
 
 cudaError_t launch_average(const SpotDev* spots, int nspots, int save, int player, const float* root_reach,
                            float* scratch, size_t scratch_floats, float* out, int* err, int grid, int block,
-                           const SmemPlan& plan, cudaStream_t s, int owner, float* bgrad) {
+                           const SmemPlan& plan, cudaStream_t s, int owner, float* bgrad, float* breach) {
   size_t smem = plan.total();
   cudaError_t e = set_smem((const void*)k_average, smem);
   if (e != cudaSuccess) return e;
   k_average<<<grid, block, smem, s>>>(spots, nspots, save, player, root_reach, scratch, scratch_floats, out, owner,
-                                       bgrad, plan,
+                                       bgrad, breach, plan,
                                        err);
   return cudaGetLastError();
 }

@@ -48,8 +48,15 @@ struct GridJob {
   const float* root_reach; // GRID_AVERAGE: opponent reach at the root (null = initial weights)
   float* bgrad;            // GRID_AVERAGE: boundary gradient buffer or null
   float* out;              // GRID_AVERAGE: root values [H_player]
+  float* breach = nullptr; // GRID_AVERAGE: boundary reach buffer or null
 };
 int grid_ctas(int block, const SmemPlan& plan);
+// Reach-weighted 48-river average of boundary-network outputs (ps_datagen.cu):
+// boards [n][4], denorm [n] (pot + stack), net [n][2][48][1326], reach
+// [n][2][1326], hands [H] combo indices, out [n][2][H]; all device pointers.
+cudaError_t launch_boundary_river_reduce(int n, const uint8_t* boards, const float* denorm, const float* net,
+                                         const float* reach, const int32_t* hands, int H, float* out,
+                                         cudaStream_t s);
 cudaError_t launch_grid(const SpotDev* spot, const GridJob& job, const Discount* disc, float* scratch,
                         size_t scratch_floats, float* out_expl, int* out_iters, unsigned* bar, double* gred,
                         int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s);
@@ -66,7 +73,7 @@ cudaError_t launch_exploitability(const SpotDev* spots, int nspots, float* scrat
 cudaError_t launch_average(const SpotDev* spots, int nspots, int save, int player, const float* root_reach,
                            float* scratch, size_t scratch_floats, float* out, int* err, int grid, int block,
                            const SmemPlan& plan, cudaStream_t s, int owner = -1,
-                           float* bgrad = nullptr);
+                           float* bgrad = nullptr, float* breach = nullptr);
 cudaError_t launch_eval_terminal(const SpotDev* spots, Op op, int player, float* scratch, size_t scratch_floats,
                                  int* err, int block, const SmemPlan& plan, cudaStream_t s);
 
