@@ -236,7 +236,8 @@ def main():
     ap.add_argument("--turn-iters", type=int, default=500, help="single turn game iterations (0 = skip)")
     ap.add_argument("--turn-cpu-iters", type=int, default=1)
     ap.add_argument("--stage", type=int, default=-1)
-    ap.add_argument("--bufs", type=int, default=0, help="terminal scan buffers per CTA (0 = one per warp)")
+    ap.add_argument("--bufs", type=int, default=0, help="terminal scan buffers per CTA (0 = half the warps)")
+    ap.add_argument("--inst", type=int, default=0, help="spots per CTA in lockstep (0 = library default)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -275,7 +276,7 @@ def main():
         return rank_max(x, dist, "cuda")
 
     bs = ps.BatchSolver(cc, tcs, block_threads=args.block, ctas_per_sm=args.ctas_per_sm, stage_tables=args.stage,
-                        scan_buffers=args.bufs)
+                        scan_buffers=args.bufs, instances_per_cta=args.inst)
     for _ in range(args.warmup):
         bs.solve(MAX_ITER, targets)
 
@@ -312,7 +313,7 @@ def main():
         barrier()
         t0 = time.perf_counter()
         b2 = ps.BatchSolver(cc, tcs, block_threads=args.block, ctas_per_sm=args.ctas_per_sm,
-                            stage_tables=args.stage, scan_buffers=args.bufs)
+                            stage_tables=args.stage, scan_buffers=args.bufs, instances_per_cta=args.inst)
         b2.solve(MAX_ITER, targets)
         e2, _ = b2.results()
         torch.cuda.synchronize()

@@ -195,6 +195,8 @@ typedef struct ps_batch_opts {
   int32_t scan_buffers;   /* warps per CTA that evaluate terminal runs, each with a shared-memory
                              scan buffer of 12 bytes per hand (0 = half the warps; the
                              autotuner then also tries all of them) */
+  int32_t instances_per_cta; /* spots of one tree shape a CTA solves in lockstep, 1..4
+                                (0 = 1); they share each step's barrier */
 } ps_batch_opts;
 int ps_batch_new(const ps_card_config* cards, const ps_tree_config* trees, int32_t n,
                  const ps_batch_opts* opts, ps_batch** out);

@@ -54,6 +54,7 @@ class PsBatchOpts(C.Structure):
         ("sort_by_cost", C.c_int32),
         ("stage_tables", C.c_int32),
         ("scan_buffers", C.c_int32),
+        ("instances_per_cta", C.c_int32),
     ]
 
 

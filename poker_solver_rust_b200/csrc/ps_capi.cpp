@@ -138,6 +138,10 @@ struct Batch {
   int* d_counter = nullptr;
   int* d_err = nullptr;
   int* d_order = nullptr;
+  int inst_k = 1;            // spots per CTA solved in lockstep
+  int ninst = 0;             // instances
+  std::vector<int> inst;     // [ninst][inst_k] spot ids, -1 = empty
+  int* d_inst = nullptr;
   int block = 256, grid = 1, ctas_per_sm = 0;
   int max_vstride = 32;
   SmemPlan plan{};
@@ -173,6 +177,7 @@ struct Batch {
     cudaFree(d_counter);
     cudaFree(d_err);
     cudaFree(d_order);
+    cudaFree(d_inst);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
@@ -350,6 +355,7 @@ struct Batch {
       single_board &= gp->boards.size() == 1;
     }
     const bool tune = opts && opts->block_threads < 0;
+    inst_k = opts && opts->instances_per_cta > 0 ? std::min(opts->instances_per_cta, 4) : 1;
     req_bufs = opts ? opts->scan_buffers : 0;
     block = opts && opts->block_threads > 0 ? opts->block_threads : 256;
     block = std::max(64, std::min(256, (block / 32) * 32));
@@ -366,7 +372,7 @@ struct Batch {
     for (auto& gp : games) scratch_floats = std::max(scratch_floats, (size_t)gp->num_slots * gp->vstride);
     scratch_floats = (scratch_floats + 63) & ~(size_t)63;
     scratch_ctas = grid;
-    CU(cudaMalloc(&d_scratch, sizeof(float) * scratch_floats * scratch_ctas));
+    CU(cudaMalloc(&d_scratch, sizeof(float) * scratch_floats * scratch_ctas * inst_k));
     // a single tree of at least PS_GRID_NODES nodes (default 2000; 0 = never)
     // is solved by all SMs at once
     {
@@ -384,17 +390,59 @@ struct Batch {
     }
     // order: largest estimated cost first (longest-processing-time first)
     std::vector<int> order(n);
-    for (int i = 0; i < n; ++i) order[i] = i;
-    if (!opts || opts->sort_by_cost) {
-      std::vector<double> cost(n);
-      for (int i = 0; i < n; ++i) cost[i] = (double)games[i]->num_storage + 4.0 * games[i]->arena.size() * games[i]->vstride;
+    std::vector<double> cost(n);
+    for (int i = 0; i < n; ++i) {
+      order[i] = i;
+      cost[i] = (double)games[i]->num_storage + 4.0 * games[i]->arena.size() * games[i]->vstride;
+    }
+    if (!opts || opts->sort_by_cost)
       std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    // instances: up to inst_k spots of one tree shape (and rake setting),
+    // which share their step structure and are solved in lockstep by one CTA
+    {
+      std::map<std::string, std::vector<int>> by_shape;
+      std::vector<std::string> shape_order;
+      for (int i : order) {
+        const Game& g = *games[i];
+        std::string key;
+        key.reserve(g.arena.size() * 3 + 8);
+        for (const auto& a : g.arena) {
+          key += (char)a.player;
+          key += (char)(a.nch & 0xFF);
+          key += (char)(a.nch >> 8);
+        }
+        key += (g.cfg.rake_rate > 0.0 && g.cfg.rake_cap > 0.0) ? 'r' : 'u';
+        key += std::to_string(g.boards.size());
+        auto& v = by_shape[key];
+        if (v.empty()) shape_order.push_back(key);
+        v.push_back(i);
+      }
+      std::vector<std::pair<double, std::vector<int>>> insts;
+      for (const auto& key : shape_order) {
+        const auto& v = by_shape[key];
+        for (size_t j = 0; j < v.size(); j += inst_k) {
+          std::vector<int> ids(inst_k, -1);
+          double c = 0;
+          for (int k = 0; k < inst_k && j + k < v.size(); ++k) {
+            ids[k] = v[j + k];
+            c += cost[v[j + k]];
+          }
+          insts.push_back({c, ids});
+        }
+      }
+      if (!opts || opts->sort_by_cost)
+        std::stable_sort(insts.begin(), insts.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+      ninst = (int)insts.size();
+      inst.clear();
+      for (auto& it : insts) inst.insert(inst.end(), it.second.begin(), it.second.end());
+      CU(cudaMalloc(&d_inst, sizeof(int) * std::max<size_t>(1, inst.size())));
     }
     // ---- upload ----
     CU(cudaMemcpyAsync(pool, h_static, static_bytes, cudaMemcpyHostToDevice, stream));
     CU(cudaMemcpyAsync(d_spots, h_spots.data(), sizeof(SpotDev) * n, cudaMemcpyHostToDevice, stream));
     CU(cudaMemcpyAsync(d_work, work.data(), sizeof(int2) * nwork, cudaMemcpyHostToDevice, stream));
     CU(cudaMemcpyAsync(d_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
+    CU(cudaMemcpyAsync(d_inst, inst.data(), sizeof(int) * inst.size(), cudaMemcpyHostToDevice, stream));
     CU(cudaStreamSynchronize(stream));
     if (tune) return autotune(order, opts ? opts->ctas_per_sm : 0);
     return PS_OK;
@@ -502,7 +550,7 @@ struct Batch {
     if (g > scratch_ctas) {
       cudaFree(d_scratch);
       d_scratch = nullptr;
-      CU(cudaMalloc(&d_scratch, sizeof(float) * scratch_floats * g));
+      CU(cudaMalloc(&d_scratch, sizeof(float) * scratch_floats * g * inst_k));
       scratch_ctas = g;
     }
     block = b;
@@ -595,7 +643,8 @@ struct Batch {
     if (fresh && (rc = enqueue_setup())) return rc;
     if (!fresh) CU(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
     CU(cudaEventRecord(ev[2], stream));
-    CU(launch_solve(d_spots, n, d_order, d_counter, d_disc, (int)max_iter, d_target, d_scratch, scratch_floats,
+    CU(launch_solve(d_spots, ninst, inst_k, d_inst, d_counter, d_disc, (int)max_iter, d_target, d_scratch,
+                    scratch_floats,
                     d_expl, d_iters, d_err, grid, block, plan, stream));
     CU(cudaEventRecord(ev[3], stream));
     h_expl.resize(n);

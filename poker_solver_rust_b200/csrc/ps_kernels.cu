@@ -566,11 +566,19 @@ __device__ __forceinline__ void step_barrier(const Ctx& c) {
     __syncthreads();
 }
 
-__device__ __noinline__ void run_pass(const Ctx& c, int p, const Discount dc, int mode) {
+// One pass for traverser p over the K spots cs[0..K) in lockstep (spots of
+// one tree shape share the step structure; only the spots in `active` take
+// part).  A step's items of all spots are interleaved over the warps, so one
+// barrier per step serves K spots.
+constexpr int kMaxInst = 4;  // spots per CTA at most
+
+__device__ __noinline__ void run_pass_multi(Ctx* cs, int K, unsigned active, int p, const Discount dc, int mode) {
+  int first = 0;
+  while (first < K && !(active >> first & 1u)) ++first;
+  if (first == K) return;
+  const Ctx& c = cs[first];
   const SpotDev& sp = *c.sp;
   const Step* steps = sp.steps[p];
-  const Op* ops = sp.ops[p];
-  const uint16_t* groups = sp.groups[p];
   const int o = p ^ 1;
   const int warp = threadIdx.x >> 5, nw0 = blockDim.x >> 5;
   // in grid mode the items of a step are spread over the warps of all CTAs
@@ -578,28 +586,37 @@ __device__ __noinline__ void run_pass(const Ctx& c, int p, const Discount dc, in
   const int gw = c.grid ? blockIdx.x * nw0 + warp : warp;
   const int nb = c.grid ? gridDim.x * c.bufs : c.bufs;
   const int gb = c.grid ? blockIdx.x * c.bufs + warp : warp;
+  const bool gen = c.owner >= 0 || c.signed_reach || c.bgrad || c.breach;
   for (int s = 0; s < sp.nsteps[p]; ++s) {
     const Step st = steps[s];
     // terminal runs go round robin to the warps that own a scan buffer; node
-    // ops go round robin to all warps, starting at the first warp without a run
+    // ops go round robin to all warps, starting at the first warp without a
+    // run.  Item j belongs to spot j % K.
+    const int ng = K * st.n_groups, ne = K * st.n_elem;
     if (warp < c.bufs)
-      for (int j = gb; j < st.n_groups; j += nb) {
-        const Op* lead = ops + st.begin + st.n_elem + groups[st.gbegin + j];
-        if (c.owner >= 0 || c.signed_reach || c.bgrad || c.breach)
-          warp_terms<true>(c, lead, lead->na, p);
+      for (int j = gb; j < ng; j += nb) {
+        const int k = j % K;
+        if (!(active >> k & 1u)) continue;
+        const Ctx& ck = cs[k];
+        const Op* lead = ck.sp->ops[p] + st.begin + st.n_elem + ck.sp->groups[p][st.gbegin + j / K];
+        if (gen)
+          warp_terms<true>(ck, lead, lead->na, p);
         else
-          warp_terms<false>(c, lead, lead->na, p);
+          warp_terms<false>(ck, lead, lead->na, p);
       }
-    const int start = min(st.n_groups, nb) % nw;
-    for (int i = (gw - start + nw) % nw; i < st.n_elem; i += nw) {
-      const Op op = ops[st.begin + i];
+    const int start = min(ng, nb) % nw;
+    for (int i = (gw - start + nw) % nw; i < ne; i += nw) {
+      const int k = i % K;
+      if (!(active >> k & 1u)) continue;
+      const Ctx& ck = cs[k];
+      const Op op = ck.sp->ops[p][st.begin + i / K];
       PHASE_T0(t_op);
       switch (op.type) {
-        case OP_FWD_OPP: op_fwd_opp(c, op, o, mode); break;
-        case OP_FWD_CHANCE: op_fwd_chance(c, op, o); break;
-        case OP_BWD_TRAV: op_bwd_trav(c, op, p, dc, mode); break;
-        case OP_BWD_OPP: op_bwd_opp(c, op, p, mode); break;
-        case OP_BWD_CHANCE: op_bwd_chance(c, op, p, mode); break;
+        case OP_FWD_OPP: op_fwd_opp(ck, op, o, mode); break;
+        case OP_FWD_CHANCE: op_fwd_chance(ck, op, o); break;
+        case OP_BWD_TRAV: op_bwd_trav(ck, op, p, dc, mode); break;
+        case OP_BWD_OPP: op_bwd_opp(ck, op, p, mode); break;
+        case OP_BWD_CHANCE: op_bwd_chance(ck, op, p, mode); break;
         default: break;
       }
       PHASE_ADD(op.type == OP_FWD_OPP      ? PH_FWD_OPP
@@ -613,6 +630,10 @@ __device__ __noinline__ void run_pass(const Ctx& c, int p, const Discount dc, in
     step_barrier(c);
     PHASE_ADD(PH_BARRIER, t_bar);
   }
+}
+
+__device__ void run_pass(const Ctx& c, int p, const Discount dc, int mode) {
+  run_pass_multi(const_cast<Ctx*>(&c), 1, 1u, p, dc, mode);
 }
 
 // sum_h w[h] * v[h] accumulated in f64 (utility.rs:118-122), result on all threads.
@@ -643,6 +664,43 @@ __device__ double root_dot(const Ctx& c, const float* w, const float* v, int n, 
   }
   grid_barrier(c);
   return *reinterpret_cast<volatile double*>(c.gred + slot);
+}
+
+// Exploitability of the active spots of cs (same as spot_exploitability,
+// passes shared by the K spots); results in out[k].
+__device__ void exploitability_multi(Ctx* cs, int K, unsigned active, float* out) {
+  const Discount dz{0.f, 0.f, 0.f, 0.f};
+  float mes[kMaxInst][2], cur[kMaxInst][2];
+  const bool raked = cs[0].sp->raked != 0;  // an instance holds spots of one rake setting
+  for (int p = 0; p < 2; ++p) {
+    for (int k = 0; k < K; ++k) cs[k].root_reach = cs[k].sp->w[p ^ 1];
+    run_pass_multi(cs, K, active, p, dz, M_BR);
+    for (int k = 0; k < K; ++k)
+      if (active >> k & 1u) {
+        const SpotDev& sp = *cs[k].sp;
+        mes[k][p] = (float)block_dot_f64(cs[k], sp.w[p], slot_at(cs[k], sp.root_slot[p]), sp.H[p]);
+      }
+  }
+  if (raked)
+    for (int p = 0; p < 2; ++p) {
+      for (int k = 0; k < K; ++k) cs[k].root_reach = cs[k].sp->w[p ^ 1];
+      run_pass_multi(cs, K, active, p, dz, M_AVG);
+      for (int k = 0; k < K; ++k)
+        if (active >> k & 1u) {
+          const SpotDev& sp = *cs[k].sp;
+          cur[k][p] = (float)block_dot_f64(cs[k], sp.w[p], slot_at(cs[k], sp.root_slot[p]), sp.H[p]);
+        }
+    }
+  for (int k = 0; k < K; ++k)
+    if (active >> k & 1u)
+      out[k] = raked ? ((mes[k][0] - cur[k][0]) + (mes[k][1] - cur[k][1])) * 0.5f : (mes[k][0] + mes[k][1]) * 0.5f;
+}
+
+__device__ void dcfr_iteration_multi(Ctx* cs, int K, unsigned active, const Discount dc) {
+  for (int p = 0; p < 2; ++p) {  // alternating updates (solver.rs:144-155)
+    for (int k = 0; k < K; ++k) cs[k].root_reach = cs[k].sp->w[p ^ 1];
+    run_pass_multi(cs, K, active, p, dc, M_DCFR);
+  }
 }
 
 __device__ float spot_exploitability(Ctx& c) {
@@ -742,46 +800,81 @@ __device__ bool bind_ctx(Ctx& c, const SpotDev* sp, float* scratch, size_t scrat
 // run the full reference solve loop (solver.rs:108-176) per spot:
 //   expl = exploitability; for t < max_iter { if expl <= target break;
 //   iterate(t); if (t+1) % 5 == 0 || t+1 == max_iter: expl = exploitability }.
-__global__ void PS_SOLVE_BOUNDS k_solve(const SpotDev* __restrict__ spots, int nspots, const int* __restrict__ order,
-                                        int* counter, const Discount* __restrict__ disc, int max_iter,
-                                        const float* __restrict__ target, float* scratch, size_t scratch_floats,
-                                        float* out_expl, int* out_iters, SmemPlan plan, int* err) {
+__global__ void PS_SOLVE_BOUNDS k_solve(const SpotDev* __restrict__ spots, int ninst, int K,
+                                        const int* __restrict__ inst, int* counter, const Discount* __restrict__ disc,
+                                        int max_iter, const float* __restrict__ target, float* scratch,
+                                        size_t scratch_floats, float* out_expl, int* out_iters, SmemPlan plan,
+                                        int* err) {
   extern __shared__ float4 smem4[];
   char* smem = reinterpret_cast<char*>(smem4);
-  __shared__ int s_spot;
-  float* my_scratch = scratch + (size_t)blockIdx.x * scratch_floats;
+  __shared__ int s_inst;
+  float* my_scratch = scratch + (size_t)blockIdx.x * K * scratch_floats;
   for (;;) {
     __syncthreads();
-    if (threadIdx.x == 0) s_spot = atomicAdd(counter, 1);
+    if (threadIdx.x == 0) s_inst = atomicAdd(counter, 1);
     __syncthreads();
-    const int k = s_spot;
-    if (k >= nspots) return;
-    const int si = order ? order[k] : k;
-    Ctx c;
-    if (!bind_ctx(c, &spots[si], my_scratch, scratch_floats, smem, plan, err)) continue;
-    const float tgt = target[si];
-    float expl = spot_exploitability(c);
+    const int q = s_inst;
+    if (q >= ninst) return;
+    // an instance: up to K spots of one tree shape, solved in lockstep
+    Ctx cs[kMaxInst];
+    int ids[kMaxInst];
+    float tgt[kMaxInst], expl[kMaxInst];
+    int iters[kMaxInst];
+    unsigned active = 0;
+    for (int k = 0; k < K; ++k) {
+      ids[k] = inst[(size_t)q * K + k];
+      if (ids[k] >= 0 && bind_ctx(cs[k], &spots[ids[k]], my_scratch + (size_t)k * scratch_floats, scratch_floats,
+                                  smem, plan, err))
+        active |= 1u << k;
+      else
+        cs[k] = cs[0];  // placeholder; never active
+      tgt[k] = ids[k] >= 0 ? target[ids[k]] : 0.f;
+      expl[k] = 0.f;
+      iters[k] = 0;
+    }
+    if (!active) continue;
+    // the reference loop per spot (solver.rs:108-176): expl = exploitability;
+    // for t < max_iter { if expl <= target break; iterate(t); if (t+1) % 5 == 0
+    // || t+1 == max_iter: expl = exploitability }; a spot leaves the lockstep
+    // set at the first check that meets its target
+    exploitability_multi(cs, K, active, expl);
+    unsigned live = 0;
+    for (int k = 0; k < K; ++k)
+      if ((active >> k & 1u) && !(expl[k] <= tgt[k])) live |= 1u << k;
     int t = 0;
-    for (; t < max_iter; ++t) {
-      if (expl <= tgt) break;
-      dcfr_iteration(c, disc[t]);
-      if ((t + 1) % 5 == 0 || t + 1 == max_iter) expl = spot_exploitability(c);
+    for (; t < max_iter && live; ++t) {
+      dcfr_iteration_multi(cs, K, live, disc[t]);
+      if ((t + 1) % 5 == 0 || t + 1 == max_iter) {
+        exploitability_multi(cs, K, live, expl);
+        for (int k = 0; k < K; ++k)
+          if ((live >> k & 1u) && expl[k] <= tgt[k]) {
+            iters[k] = t + 1;
+            live &= ~(1u << k);
+          }
+      }
     }
-    if (threadIdx.x == 0) {
-      out_expl[si] = expl;
-      out_iters[si] = t;
-    }
+    for (int k = 0; k < K; ++k)
+      if (live >> k & 1u) iters[k] = t;
+    if (threadIdx.x == 0)
+      for (int k = 0; k < K; ++k)
+        if (active >> k & 1u) {
+          out_expl[ids[k]] = expl[k];
+          out_iters[ids[k]] = iters[k];
+        }
     // root cfvalues of both players under the average strategy: the
     // per-hand values a datagen record needs (the reference computes them on
     // the host from the strategy sums)
-    const SpotDev& sp = spots[si];
     const Discount dz{0.f, 0.f, 0.f, 0.f};
     for (int p = 0; p < 2; ++p) {
-      if (!sp.root_out[p]) continue;
-      c.root_reach = sp.w[p ^ 1];
-      run_pass(c, p, dz, M_AVG);
-      const float* r = slot_at(c, sp.root_slot[p]);
-      for (int h = threadIdx.x; h < sp.hs[p]; h += blockDim.x) sp.root_out[p][h] = r[h];
+      for (int k = 0; k < K; ++k) cs[k].root_reach = cs[k].sp->w[p ^ 1];
+      run_pass_multi(cs, K, active, p, dz, M_AVG);
+      for (int k = 0; k < K; ++k) {
+        if (!(active >> k & 1u)) continue;
+        const SpotDev& sp = *cs[k].sp;
+        if (!sp.root_out[p]) continue;
+        const float* r = slot_at(cs[k], sp.root_slot[p]);
+        for (int h = threadIdx.x; h < sp.hs[p]; h += blockDim.x) sp.root_out[p][h] = r[h];
+      }
       __syncthreads();
     }
   }
@@ -1144,13 +1237,15 @@ cudaError_t launch_setup(const SpotDev* spots, const int2* work, int nwork, cons
   return cudaGetLastError();
 }
 
-cudaError_t launch_solve(const SpotDev* spots, int nspots, const int* order, int* counter, const Discount* disc,
-                         int max_iter, const float* target, float* scratch, size_t scratch_floats, float* out_expl,
-                         int* out_iters, int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s) {
+cudaError_t launch_solve(const SpotDev* spots, int ninst, int K, const int* inst, int* counter,
+                         const Discount* disc, int max_iter, const float* target, float* scratch,
+                         size_t scratch_floats, float* out_expl, int* out_iters, int* err, int grid, int block,
+                         const SmemPlan& plan, cudaStream_t s) {
+  if (K < 1 || K > kMaxInst) return cudaErrorInvalidValue;
   size_t smem = plan.total();
   cudaError_t e = set_smem((const void*)k_solve, smem);
   if (e != cudaSuccess) return e;
-  k_solve<<<grid, block, smem, s>>>(spots, nspots, order, counter, disc, max_iter, target, scratch, scratch_floats,
+  k_solve<<<grid, block, smem, s>>>(spots, ninst, K, inst, counter, disc, max_iter, target, scratch, scratch_floats,
                                      out_expl, out_iters, plan, err);
   return cudaGetLastError();
 }

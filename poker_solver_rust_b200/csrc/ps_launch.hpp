@@ -62,9 +62,12 @@ cudaError_t launch_grid(const SpotDev* spot, const GridJob& job, const Discount*
                         int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s);
 cudaError_t launch_setup(const SpotDev* spots, const int2* work, int nwork, const int32_t* table, int* err,
                          int grid, cudaStream_t s);
-cudaError_t launch_solve(const SpotDev* spots, int nspots, const int* order, int* counter, const Discount* disc,
-                         int max_iter, const float* target, float* scratch, size_t scratch_floats, float* out_expl,
-                         int* out_iters, int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s);
+// Persistent batched solve over `ninst` instances of K spots (inst: [ninst][K]
+// spot ids, -1 = empty); scratch holds K * scratch_floats floats per CTA.
+cudaError_t launch_solve(const SpotDev* spots, int ninst, int K, const int* inst, int* counter,
+                         const Discount* disc, int max_iter, const float* target, float* scratch,
+                         size_t scratch_floats, float* out_expl, int* out_iters, int* err, int grid, int block,
+                         const SmemPlan& plan, cudaStream_t s);
 cudaError_t launch_iterate(const SpotDev* spots, int nspots, const Discount* disc, int t0, int t1,
                            float* scratch, size_t scratch_floats, int* err, int grid, int block,
                            const SmemPlan& plan, cudaStream_t s);

@@ -439,7 +439,7 @@ class BatchSolver:
 
     def __init__(self, card_configs: Sequence[CardConfig], tree_configs: Sequence[TreeConfig],
                  block_threads: int = 0, ctas_per_sm: int = 0, sort_by_cost: bool = True,
-                 stage_tables: int = -1, scan_buffers: int = 0):
+                 stage_tables: int = -1, scan_buffers: int = 0, instances_per_cta: int = 0):
         n = len(card_configs)
         cc = (N.PsCardConfig * n)()
         tc = (N.PsTreeConfig * n)()
@@ -450,7 +450,8 @@ class BatchSolver:
             keep.append((c._keep, t._keep))
             cc[i] = c
             tc[i] = t
-        opts = N.PsBatchOpts(block_threads, ctas_per_sm, int(sort_by_cost), stage_tables, scan_buffers)
+        opts = N.PsBatchOpts(block_threads, ctas_per_sm, int(sort_by_cost), stage_tables, scan_buffers,
+                             instances_per_cta)
         h = C.c_void_p()
         N.check(N.lib().ps_batch_new(cc, tc, n, C.byref(opts), C.byref(h)))
         self._h = h

@@ -389,6 +389,27 @@ def test_batch_root_cfvalues_match_single_game():
             assert np.array_equal(bs.root_cfvalues(i, p), ps.root_cfvalues(g, p))
 
 
+@pytest.mark.parametrize("inst", [2, 3])
+def test_batch_lockstep_instances_keep_results(inst):
+    """Spots of one tree shape solved in lockstep by one CTA: every spot's
+    iteration count, exploitability and root values equal the one-spot-per-CTA
+    solve (a spot that meets its target leaves the lockstep set)."""
+    sp = spots.datagen_spots(48, seed=35)
+    cc = [spots.card_config(r, b) for r, b, _ in sp]
+    tcs = [t for _, _, t in sp]
+    targets = np.array([0.003 * t.starting_pot for t in tcs], np.float32)
+    one = ps.BatchSolver(cc, tcs)
+    one.solve(300, targets)
+    many = ps.BatchSolver(cc, tcs, instances_per_cta=inst)
+    many.solve(300, targets)
+    e0, i0 = one.results()
+    e1, i1 = many.results()
+    assert np.array_equal(i0, i1) and np.array_equal(e0, e1)
+    for k in range(0, 48, 7):
+        for p in range(2):
+            assert np.array_equal(one.root_cfvalues(k, p), many.root_cfvalues(k, p))
+
+
 def test_batch_autotune_keeps_results():
     """block_threads=-1 times every CTA size on a sample of the batch and keeps
     the fastest; the spots' arithmetic does not depend on the CTA size."""
