@@ -48,6 +48,35 @@ struct DeviceConsts {
 };
 std::mutex g_dev_mu;
 std::mutex g_tune_mu;
+
+// Pinned host staging buffers, kept for reuse: a batch fills one, uploads it
+// and hands it back, so back-to-back batches pay for page-locking once.
+struct PinnedPool {
+  std::mutex mu;
+  std::vector<std::pair<char*, size_t>> free_;
+  cudaError_t acquire(size_t bytes, char** out) {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      for (size_t i = 0; i < free_.size(); ++i)
+        if (free_[i].second >= bytes) {
+          *out = free_[i].first;
+          free_.erase(free_.begin() + (long)i);
+          return cudaSuccess;
+        }
+    }
+    return cudaMallocHost(out, bytes);
+  }
+  void release(char* p, size_t bytes) {
+    std::lock_guard<std::mutex> lk(mu);
+    free_.push_back({p, bytes});
+    if (free_.size() > 2) {  // keep the two largest
+      std::sort(free_.begin(), free_.end(), [](const auto& a, const auto& b) { return a.second > b.second; });
+      cudaFreeHost(free_.back().first);
+      free_.pop_back();
+    }
+  }
+};
+PinnedPool g_pinned;
 std::map<long, std::pair<int, int>> g_tune;  // autotuned (CTA size, scan-buffer warps) per
                                              // (device, hand-count class, tree-size class)
 DeviceConsts g_dev[16];
@@ -122,7 +151,8 @@ struct Batch {
   cudaStream_t stream = nullptr;
   char* pool = nullptr;
   size_t static_bytes = 0, setup_bytes = 0, state_bytes = 0;
-  char* h_static = nullptr;  // pinned staging of the static region
+  char* h_static = nullptr;  // pinned staging of the static region (from g_pinned, during build only)
+  size_t h_static_cap = 0;
   SpotDev* d_spots = nullptr;
   std::vector<SpotDev> h_spots;
   int2* d_work = nullptr;
@@ -164,7 +194,7 @@ struct Batch {
   ~Batch() {
     if (stream) cudaStreamSynchronize(stream);
     cudaFree(pool);
-    cudaFreeHost(h_static);
+    if (h_static) g_pinned.release(h_static, h_static_cap);
     cudaFree(d_spots);
     cudaFree(d_work);
     cudaFree(d_scratch);
@@ -231,14 +261,16 @@ struct Batch {
     setup_bytes = su;
     state_bytes = st;
     CU(cudaMalloc(&pool, static_bytes + setup_bytes + state_bytes));
-    CU(cudaMallocHost(&h_static, std::max<size_t>(static_bytes, 16)));
+    h_static_cap = std::max<size_t>(static_bytes, 16);
+    CU(g_pinned.acquire(h_static_cap, &h_static));
     // ---- fill static ----
     h_spots.resize(n);
     std::vector<int2> work;
     char* dS = pool;
     char* dU = pool + static_bytes;
     char* dT = pool + static_bytes + setup_bytes;
-    for (int i = 0; i < n; ++i) {
+    // every spot fills its own regions: spread over the host cores
+    auto fill = [&](int i) {
       Game& g = *games[i];
       Layout& L = lay[i];
       SpotDev& s = h_spots[i];
@@ -311,10 +343,7 @@ struct Batch {
         d.path_scale = pscale[k];
       }
       uint8_t* bc = (uint8_t*)(h_static + L.board_cards);
-      for (size_t b = 0; b < g.boards.size(); ++b) {
-        std::memcpy(bc + 5 * b, g.boards[b].data(), 5);
-        work.push_back(make_int2(i, (int)b));
-      }
+      for (size_t b = 0; b < g.boards.size(); ++b) std::memcpy(bc + 5 * b, g.boards[b].data(), 5);
       std::memcpy(h_static + L.iso_off, g.iso_list_off.data(), g.iso_list_off.size() * 4);
       std::memcpy(h_static + L.iso_ent, g.iso_list.data(), g.iso_list.size() * 8);
       s.vstride = g.vstride;
@@ -336,7 +365,18 @@ struct Batch {
       s.S = (float*)(dT + L.S);
       s.ipcfv = (float*)(dT + L.ipcfv);
       s.chcfv = (float*)(dT + L.chcfv);
+    };
+    {
+      const int nt = std::max(1, std::min<int>(n / 64 + 1, std::min(16, (int)std::thread::hardware_concurrency())));
+      std::vector<std::thread> th;
+      for (int k = 0; k < nt; ++k)
+        th.emplace_back([&, k] {
+          for (int i = k; i < n; i += nt) fill(i);
+        });
+      for (auto& t : th) t.join();
     }
+    for (int i = 0; i < n; ++i)
+      for (size_t b = 0; b < games[i]->boards.size(); ++b) work.push_back(make_int2(i, (int)b));
     nwork = (int)work.size();
     CU(cudaMalloc(&d_spots, sizeof(SpotDev) * n));
     CU(cudaMalloc(&d_work, sizeof(int2) * std::max(1, nwork)));
@@ -444,6 +484,8 @@ struct Batch {
     CU(cudaMemcpyAsync(d_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
     CU(cudaMemcpyAsync(d_inst, inst.data(), sizeof(int) * inst.size(), cudaMemcpyHostToDevice, stream));
     CU(cudaStreamSynchronize(stream));
+    g_pinned.release(h_static, h_static_cap);  // uploaded: the staging buffer goes back to the pool
+    h_static = nullptr;
     if (tune) return autotune(order, opts ? opts->ctas_per_sm : 0);
     return PS_OK;
   }

@@ -432,6 +432,68 @@ def hand_table() -> np.ndarray:
 
 
 # ---- batched datagen path ----
+def _pack_configs(card_configs, tree_configs):
+    """ps_card_config / ps_tree_config arrays for n spots, filled column by
+    column through numpy views at the structs' field offsets: the ranges are
+    stacked into one array and every distinct bet-size string is encoded once.
+    Returns the two ctypes arrays and the objects they point into."""
+    n = len(card_configs)
+    cc = (N.PsCardConfig * n)()
+    tc = (N.PsTreeConfig * n)()
+    ranges = np.empty((n, 2, 1326), np.float32)
+    for i, c in enumerate(card_configs):
+        ranges[i, 0] = c.range[0].raw_data()
+        ranges[i, 1] = c.range[1].raw_data()
+    craw = np.frombuffer(cc, np.uint8).reshape(n, C.sizeof(N.PsCardConfig))
+    traw = np.frombuffer(tc, np.uint8).reshape(n, C.sizeof(N.PsTreeConfig))
+
+    def col(raw, struct, field, dtype, count=1):
+        off = getattr(struct, field).offset
+        return raw[:, off:off + np.dtype(dtype).itemsize * count].view(dtype)
+
+    base = ranges.ctypes.data
+    ptrs = col(craw, N.PsCardConfig, "range", np.uint64, 2)
+    ptrs[:, 0] = base + np.arange(n, dtype=np.uint64) * (2 * 1326 * 4)
+    ptrs[:, 1] = ptrs[:, 0] + 1326 * 4
+    cards = np.array([[c.flop[0], c.flop[1], c.flop[2], c.turn, c.river] for c in card_configs], np.uint8)
+    col(craw, N.PsCardConfig, "flop", np.uint8, 3)[:] = cards[:, :3]
+    col(craw, N.PsCardConfig, "turn", np.uint8)[:, 0] = cards[:, 3]
+    col(craw, N.PsCardConfig, "river", np.uint8)[:, 0] = cards[:, 4]
+
+    strings = {}  # str -> bytes, kept alive with the arrays
+
+    def addr(sv):
+        if sv is None:
+            return 0
+        b = strings.get(sv)
+        if b is None:
+            b = strings[sv] = C.create_string_buffer(sv.encode())
+        return C.addressof(b)
+
+    T = tree_configs
+    col(traw, N.PsTreeConfig, "initial_state", np.int32)[:, 0] = [int(t.initial_state) for t in T]
+    col(traw, N.PsTreeConfig, "starting_pot", np.int32)[:, 0] = [int(t.starting_pot) for t in T]
+    col(traw, N.PsTreeConfig, "effective_stack", np.int32)[:, 0] = [int(t.effective_stack) for t in T]
+    col(traw, N.PsTreeConfig, "depth_limit", np.int32)[:, 0] = [-1 if t.depth_limit is None else int(t.depth_limit)
+                                                               for t in T]
+    for f in ("rake_rate", "rake_cap", "add_allin_threshold", "force_allin_threshold", "merging_threshold"):
+        col(traw, N.PsTreeConfig, f, np.float64)[:, 0] = [float(getattr(t, f)) for t in T]
+    col(traw, N.PsTreeConfig, "max_bets", np.int32)[:, 0] = [int(t.max_bets) for t in T]
+    sizes = col(traw, N.PsTreeConfig, "bet_sizes", np.uint64, 12)
+    menus = {}  # the per-street menus of one TreeConfig are usually shared objects
+    for i, t in enumerate(T):
+        key = (id(t.flop_bet_sizes), id(t.turn_bet_sizes), id(t.river_bet_sizes))
+        row = menus.get(key)
+        if row is None:
+            row = menus[key] = [addr(s) for st in (t.flop_bet_sizes, t.turn_bet_sizes, t.river_bet_sizes)
+                                for p in range(2) for s in (st[p].bet, st[p].raise_)]
+        sizes[i] = row
+    donk = col(traw, N.PsTreeConfig, "donk_sizes", np.uint64, 2)
+    donk[:, 0] = [addr(t.turn_donk_sizes) for t in T]
+    donk[:, 1] = [addr(t.river_donk_sizes) for t in T]
+    return cc, tc, (ranges, strings, menus, T)
+
+
 class BatchSolver:
     """Thousands of independent subgames solved by one persistent launch
     (replaces the per-spot GpuBatchSolver launches of the reference's GPU
@@ -441,15 +503,7 @@ class BatchSolver:
                  block_threads: int = 0, ctas_per_sm: int = 0, sort_by_cost: bool = True,
                  stage_tables: int = -1, scan_buffers: int = 0, instances_per_cta: int = 0):
         n = len(card_configs)
-        cc = (N.PsCardConfig * n)()
-        tc = (N.PsTreeConfig * n)()
-        keep = []
-        for i in range(n):
-            c = card_configs[i].to_c()
-            t = tree_configs[i].to_c()
-            keep.append((c._keep, t._keep))
-            cc[i] = c
-            tc[i] = t
+        cc, tc, keep = _pack_configs(card_configs, tree_configs)
         opts = N.PsBatchOpts(block_threads, ctas_per_sm, int(sort_by_cost), stage_tables, scan_buffers,
                              instances_per_cta)
         h = C.c_void_p()
@@ -460,7 +514,7 @@ class BatchSolver:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and N is not None and N.lib is not None:
             N.lib().ps_batch_free(h)
             self._h = None
 
