@@ -224,6 +224,61 @@ int ps_batch_scan_buffers(ps_batch* b);
 /* bytes copied host->device by ps_batch_new and device->host by ps_batch_results */
 int ps_batch_io_bytes(ps_batch* b, uint64_t* h2d, uint64_t* d2h);
 
+/* ---- batched depth-limited solving (turn datagen with boundary values:
+ *      gpu-range-solver batch.rs:279-585 set_leaf_injection / run_iterations /
+ *      download_reach / update_leaf_cfvs, driven by cfvnet
+ *      datagen/domain/pipeline.rs:648-700) ----
+ * A boundary item is one depth boundary of one spot: items are listed spot by
+ * spot, ordinals ascending.  Per-item arrays use the 1326-combo layout
+ * (card_pair_to_index, card.rs:50-55), [items][2][1326], row p = player p. */
+#define PS_EPI_ROOT 1 /* root cfvalues + boundary reach under the average strategy */
+#define PS_EPI_EXPL 2 /* exploitability of every spot (ps_batch_results) */
+/* DCFR iterations [t0, t1) of every spot from the current state, no
+ * exploitability checks (batch.rs:414 run_iterations), in one launch; then the
+ * epilogue bits.  The first call after ps_batch_new or ps_batch_reset starts
+ * from zero regrets and strategy sums. */
+int ps_batch_run_iterations(ps_batch* b, uint32_t t0, uint32_t t1, int32_t epilogue);
+/* the next ps_batch_run_iterations starts from zero state (boundary values stay) */
+int ps_batch_reset(ps_batch* b);
+int64_t ps_batch_num_boundary_items(ps_batch* b);
+/* per item: spot, ordinal, the spot's 4-card board, the boundary node's pot
+ * (starting_pot + 2 * amount) and the stack behind it (effective_stack - amount);
+ * any pointer may be null */
+int ps_batch_boundary_items(ps_batch* b, int32_t* spot, int32_t* ordinal, uint8_t* boards, float* pots,
+                            float* stacks);
+/* boundary values of every item, [items][2][1326]; each spot takes the entries
+ * of its own hands (replaces update_leaf_cfvs, batch.rs:557-585, with the
+ * semantics of set_boundary_cfvs, interpreter.rs:343).  on_device = 1: a
+ * device pointer whose values are ready; the call returns once they are
+ * consumed.  Values are zero until set. */
+int ps_batch_set_boundary_cfvs(ps_batch* b, const float* values, int32_t on_device);
+/* each player's reach at every boundary under the average strategy as of the
+ * last PS_EPI_ROOT epilogue (or ps_batch_solve), [items][2][1326], 0 outside
+ * the spot's hands (replaces download_reach + compute_reach_at_nodes,
+ * batch.rs:537-555, :765-790) */
+int ps_batch_boundary_reach(ps_batch* b, float* out, int32_t on_device);
+/* both players' root cfvalues of every spot under the average strategy as of
+ * the last PS_EPI_ROOT epilogue, ps_batch_solve or ps_batch_adjoint, [n][2][1326]
+ * (0 outside the spot's hands) */
+int ps_batch_root_cfvalues_all(ps_batch* b, float* out, int32_t on_device);
+/* batched fixed-strategy evaluation and its adjoint: ps_eval_fixed_strategy_adjoint
+ * (no reference counterpart; the adjoint of utility.rs:422-443) for every spot at
+ * once, with each spot's initial weights and its average strategy held fixed.
+ * cot [n][2][1326]: dL/d(root cfvalues of player p).  Refreshes the root
+ * cfvalues; dw [n][2][1326]: dL/d(initial weights of player p); dB
+ * [items][2][1326]: dL/d(boundary values).  dw or dB may be null.  Spots with
+ * isomorphic chance pruning: PS_ERR_UNSUPPORTED. */
+int ps_batch_adjoint(ps_batch* b, const float* cot, float* dw, float* dB, int32_t on_device);
+/* boundary-network input rows (cfvnet eval/boundary_evaluator.rs:27-60, rows
+ * ordered as gpu_boundary_eval.rs:164-185): for each of n items, player and
+ * river card not on the board, 2720 values: oop reach | ip reach (zeroed where
+ * a hand holds the river) | 52 board one-hot | 13 rank presence |
+ * pot/(pot+stack) | stack/(pot+stack) | player.  boards [n][4], pots, stacks:
+ * host; reach [n][2][1326] and out [n][2][48][2720]: device (f32, or bf16 when
+ * out_bf16).  stream: a cudaStream_t or null */
+int ps_boundary_encode(int32_t n, const uint8_t* boards, const float* pots, const float* stacks, const float* reach,
+                       void* out, int32_t out_bf16, void* stream);
+
 /* ---- misc ---- */
 /* BetSizeOptions::try_from one list (bet_size.rs:82-112): per entry the kind
  * (0 PotRelative, 1 PrevBetRelative, 2 Additive, 3 Geometric, 4 AllIn), its

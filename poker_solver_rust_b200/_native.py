@@ -130,6 +130,18 @@ _sig("ps_batch_config", i32, vp, P(i32), P(i32), P(i32))
 _sig("ps_batch_autotune_log", i32, vp, P(i32), P(i32), P(f32), i32)
 _sig("ps_batch_scan_buffers", i32, vp)
 _sig("ps_batch_io_bytes", i32, vp, P(u64), P(u64))
+_sig("ps_batch_run_iterations", i32, vp, u32, u32, i32)
+_sig("ps_batch_reset", i32, vp)
+_sig("ps_batch_num_boundary_items", i64, vp)
+_sig("ps_batch_boundary_items", i32, vp, P(i32), P(i32), P(C.c_uint8), P(f32), P(f32))
+_sig("ps_batch_set_boundary_cfvs", i32, vp, vp, i32)
+_sig("ps_batch_boundary_reach", i32, vp, vp, i32)
+_sig("ps_batch_root_cfvalues_all", i32, vp, vp, i32)
+_sig("ps_batch_adjoint", i32, vp, vp, vp, vp, i32)
+_sig("ps_boundary_encode", i32, i32, P(C.c_uint8), P(f32), P(f32), vp, vp, i32, vp)
+
+PS_EPI_ROOT = 1
+PS_EPI_EXPL = 2
 
 EXPORTED = sorted(_SIGS)
 

@@ -63,3 +63,35 @@ def fixed_strategy_values(game, w0, w1, b0, b1):
     """Root cfvalues (cfv0, cfv1) of `game` as a differentiable function of
     the initial weights and boundary values (see FixedStrategyValues)."""
     return FixedStrategyValues.apply(game, w0, w1, b0, b1)
+
+
+class BatchSolvedValues(torch.autograd.Function):
+    """Boundary values -> root cfvalues of a batch of depth-limited spots.
+
+    Forward: the boundary values B [items, 2, 1326] (combo layout, CUDA) go
+    into the batch, every spot runs `iterations` DCFR iterations from zero
+    state in one launch, and the root cfvalues of both players under the
+    resulting average strategy come back as [n, 2, 1326].  Backward: the
+    batched adjoint (ps_batch_adjoint) with that strategy held fixed, i.e. the
+    gradient of the fixed-strategy evaluation, as FixedStrategyValues gives it
+    for one game.  Everything stays on the device.
+    """
+
+    @staticmethod
+    def forward(ctx, batch, values, iterations):
+        batch.set_boundary_cfvs(values)
+        batch.reset()
+        batch.run_iterations(0, int(iterations), root=True)
+        ctx.batch = batch
+        return batch.root_cfvalues_all(device=True).to(values.dtype)
+
+    @staticmethod
+    def backward(ctx, g):
+        _, dB = ctx.batch.adjoint(g.float())
+        return None, dB.to(g.dtype), None
+
+
+def batch_solved_values(batch, values, iterations: int):
+    """Root cfvalues [n, 2, 1326] of a BatchSolver's depth-limited spots solved
+    with boundary values `values` [items, 2, 1326] (see BatchSolvedValues)."""
+    return BatchSolvedValues.apply(batch, values, iterations)

@@ -138,7 +138,8 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 struct Layout {  // byte offsets inside the pool
   size_t cards[2], w[2], same[2], ops[2], steps[2], groups[2], nodes, board_cards, iso_perm[2], iso_off, iso_ent;  // static
   size_t gidx[2], coff[2], thr[2], nvalid[2], heads[2];                                                       // setup
-  size_t R, S, ipcfv, chcfv, bcfv, rootv[2];                                                          // state
+  size_t R, S, ipcfv, chcfv, rootv[2];                                                                // state
+  size_t bcfv, breach;  // boundary values and boundary reach (kept across state resets)
 };
 
 // ---------------------------------------------------------------------------
@@ -150,13 +151,20 @@ struct Batch {
   DeviceConsts* dc = nullptr;
   cudaStream_t stream = nullptr;
   char* pool = nullptr;
-  size_t static_bytes = 0, setup_bytes = 0, state_bytes = 0;
+  size_t static_bytes = 0, setup_bytes = 0, state_bytes = 0, bnd_bytes = 0;
   char* h_static = nullptr;  // pinned staging of the static region (from g_pinned, during build only)
   size_t h_static_cap = 0;
   SpotDev* d_spots = nullptr;
   std::vector<SpotDev> h_spots;
   int2* d_work = nullptr;
   int nwork = 0;
+  // boundary items: (spot, boundary ordinal) for every depth boundary of every
+  // spot, spots in order, ordinals ascending
+  std::vector<int2> items;
+  int2* d_items = nullptr;
+  bool ready = false;  // state zeroed and board tables built since the last reset
+  char* adj_pool = nullptr;  // per-spot adjoint vectors (cotangents, weight and boundary gradients)
+  size_t adj_bgrad_off = 0, adj_bytes = 0;
   float* d_scratch = nullptr;
   size_t scratch_floats = 0;
   int scratch_ctas = 0;
@@ -197,6 +205,8 @@ struct Batch {
     if (h_static) g_pinned.release(h_static, h_static_cap);
     cudaFree(d_spots);
     cudaFree(d_work);
+    cudaFree(d_items);
+    cudaFree(adj_pool);
     cudaFree(d_scratch);
     cudaFree(d_disc);
     cudaFree(d_target);
@@ -221,7 +231,7 @@ struct Batch {
     const int n = (int)games.size();
     lay.resize(n);
     // ---- layout ----
-    size_t so = 0, su = 0, st = 0;
+    size_t so = 0, su = 0, st = 0, sb = 0;
     auto take = [](size_t& off, size_t bytes) {
       size_t r = off;
       off += align256(bytes);
@@ -253,14 +263,17 @@ struct Batch {
       L.S = take(st, g.num_storage * 4 + 16);
       L.ipcfv = take(st, g.num_storage_ip * 4 + 16);
       L.chcfv = take(st, g.num_storage_chance * 4 + 16);
-      L.bcfv = take(st, (size_t)g.num_boundary * 2 * g.vstride * 4 + 16);
       for (int p = 0; p < 2; ++p) L.rootv[p] = take(st, (size_t)g.hs[p] * 4);
+      L.bcfv = take(sb, (size_t)g.num_boundary * 2 * g.vstride * 4 + 16);
+      L.breach = take(sb, (size_t)g.num_boundary * 2 * g.vstride * 4 + 16);
       max_vstride = std::max(max_vstride, g.vstride);
     }
     static_bytes = so;
     setup_bytes = su;
     state_bytes = st;
-    CU(cudaMalloc(&pool, static_bytes + setup_bytes + state_bytes));
+    bnd_bytes = sb;
+    CU(cudaMalloc(&pool, static_bytes + setup_bytes + state_bytes + bnd_bytes));
+    CU(cudaMemsetAsync(pool + static_bytes + setup_bytes + state_bytes, 0, bnd_bytes, stream));
     h_static_cap = std::max<size_t>(static_bytes, 16);
     CU(g_pinned.acquire(h_static_cap, &h_static));
     // ---- fill static ----
@@ -269,6 +282,7 @@ struct Batch {
     char* dS = pool;
     char* dU = pool + static_bytes;
     char* dT = pool + static_bytes + setup_bytes;
+    char* dB = dT + state_bytes;
     // every spot fills its own regions: spread over the host cores
     auto fill = [&](int i) {
       Game& g = *games[i];
@@ -359,7 +373,8 @@ struct Batch {
       s.board_cards = (const uint8_t*)(dS + L.board_cards);
       s.iso_off = (const int32_t*)(dS + L.iso_off);
       s.iso_ent = (const int32_t*)(dS + L.iso_ent);
-      s.bcfv = (const float*)(dT + L.bcfv);
+      s.bcfv = (const float*)(dB + L.bcfv);
+      s.breach = g.num_boundary > 0 ? (float*)(dB + L.breach) : nullptr;
       for (int p = 0; p < 2; ++p) s.root_out[p] = (float*)(dT + L.rootv[p]);
       s.R = (float*)(dT + L.R);
       s.S = (float*)(dT + L.S);
@@ -378,6 +393,9 @@ struct Batch {
     for (int i = 0; i < n; ++i)
       for (size_t b = 0; b < games[i]->boards.size(); ++b) work.push_back(make_int2(i, (int)b));
     nwork = (int)work.size();
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < games[i]->num_boundary; ++k) items.push_back(make_int2(i, k));
+    if (!items.empty()) CU(cudaMalloc(&d_items, sizeof(int2) * items.size()));
     CU(cudaMalloc(&d_spots, sizeof(SpotDev) * n));
     CU(cudaMalloc(&d_work, sizeof(int2) * std::max(1, nwork)));
     CU(cudaMalloc(&d_target, sizeof(float) * n));
@@ -483,6 +501,8 @@ struct Batch {
     CU(cudaMemcpyAsync(d_work, work.data(), sizeof(int2) * nwork, cudaMemcpyHostToDevice, stream));
     CU(cudaMemcpyAsync(d_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
     CU(cudaMemcpyAsync(d_inst, inst.data(), sizeof(int) * inst.size(), cudaMemcpyHostToDevice, stream));
+    if (!items.empty())
+      CU(cudaMemcpyAsync(d_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, stream));
     CU(cudaStreamSynchronize(stream));
     g_pinned.release(h_static, h_static_cap);  // uploaded: the staging buffer goes back to the pool
     h_static = nullptr;
@@ -579,6 +599,7 @@ struct Batch {
       g_tune[key] = best;
     }
     CU(cudaMemsetAsync(pool + static_bytes + setup_bytes, 0, state_bytes, stream));
+    ready = true;  // the trials' state is cleared and the board tables stay built
     return adopt_block(best.first, best.second, cap_ctas);
   }
 
@@ -625,6 +646,7 @@ struct Batch {
     CU(cudaMemsetAsync(pool + static_bytes + setup_bytes, 0, state_bytes, stream));
     CU(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
     CU(launch_setup(d_spots, d_work, nwork, dc->table, d_err, std::max(1, std::min(nwork, dc->nsm * 4)), stream));
+    ready = true;
     return PS_OK;
   }
 
@@ -685,8 +707,8 @@ struct Batch {
     if (fresh && (rc = enqueue_setup())) return rc;
     if (!fresh) CU(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
     CU(cudaEventRecord(ev[2], stream));
-    CU(launch_solve(d_spots, ninst, inst_k, d_inst, d_counter, d_disc, (int)max_iter, d_target, d_scratch,
-                    scratch_floats,
+    const SolveJob job{0, (int)max_iter, 1, EPI_ROOT};
+    CU(launch_solve(d_spots, ninst, inst_k, d_inst, d_counter, d_disc, job, d_target, d_scratch, scratch_floats,
                     d_expl, d_iters, d_err, grid, block, plan, stream));
     CU(cudaEventRecord(ev[3], stream));
     h_expl.resize(n);
@@ -696,6 +718,108 @@ struct Batch {
     CU(cudaStreamSynchronize(stream));
     CU(cudaEventElapsedTime(&last_solve_ms, ev[2], ev[3]));
     CU(cudaEventElapsedTime(&last_setup_ms, ev[1], ev[2]));
+    return check_err();
+  }
+
+  // Allocates the per-spot adjoint vectors on first use: cotangents and
+  // weight gradients [hs] per player, then all boundary gradients.
+  int ensure_adjoint() {
+    if (adj_pool) return PS_OK;
+    const int n = (int)games.size();
+    size_t off = 0;
+    std::vector<size_t> o(n);
+    for (int i = 0; i < n; ++i) {
+      o[i] = off;
+      off += align256(16 * (size_t)(games[i]->hs[0] + games[i]->hs[1]));
+    }
+    adj_bgrad_off = off;
+    std::vector<size_t> ob(n);
+    for (int i = 0; i < n; ++i) {
+      ob[i] = off;
+      off += align256((size_t)games[i]->num_boundary * 2 * games[i]->vstride * 4);
+    }
+    adj_bytes = std::max<size_t>(off, 256);
+    CU(cudaMalloc(&adj_pool, adj_bytes));
+    for (int i = 0; i < n; ++i) {
+      SpotDev& s = h_spots[i];
+      float* v = (float*)(adj_pool + o[i]);
+      const int h0 = games[i]->hs[0], h1 = games[i]->hs[1];
+      s.adj_g[0] = v;
+      s.adj_g[1] = v + h0;
+      s.adj_dw[0] = v + h0 + h1;
+      s.adj_dw[1] = v + 2 * h0 + h1;
+      s.bgrad = games[i]->num_boundary > 0 ? (float*)(adj_pool + ob[i]) : nullptr;
+    }
+    CU(cudaMemcpyAsync(d_spots, h_spots.data(), sizeof(SpotDev) * n, cudaMemcpyHostToDevice, stream));
+    CU(cudaStreamSynchronize(stream));
+    return PS_OK;
+  }
+
+  // Fixed-strategy evaluation under the average strategy and its adjoint for
+  // every spot from the cotangents already in sp.adj_g: root values into
+  // sp.root_out, gradients into sp.adj_dw and sp.bgrad.
+  int adjoint() {
+    for (auto& gp : games)
+      if (!gp->iso_list.empty())
+        return fail(PS_ERR_UNSUPPORTED, "the adjoint needs spots without isomorphic chance pruning");
+    int rc = ensure_adjoint();
+    if (rc) return rc;
+    if (!ready && (rc = enqueue_setup())) return rc;
+    CU(cudaMemsetAsync(adj_pool + adj_bgrad_off, 0, adj_bytes - adj_bgrad_off, stream));
+    CU(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
+    if (grid_mode) {
+      const SpotDev& s = h_spots[0];
+      for (int pass = 0; pass < 4; ++pass) {
+        const int p = pass < 2 ? pass : 3 - pass;
+        CU(average(0, p, pass < 2 ? s.w[p ^ 1] : s.adj_g[p ^ 1], pass < 2 ? s.root_out[p] : s.adj_dw[p],
+                   pass < 2 ? -1 : (p ^ 1), s.bgrad));
+      }
+    } else {
+      CU(cudaMemsetAsync(d_counter, 0, sizeof(int), stream));
+      SolveJob job{0, 0, 0, 0};
+      job.adjoint = 1;
+      CU(launch_solve(d_spots, ninst, inst_k, d_inst, d_counter, d_disc, job, d_target, d_scratch, scratch_floats,
+                      d_expl, d_iters, d_err, grid, block, plan, stream));
+    }
+    CU(cudaStreamSynchronize(stream));
+    return check_err();
+  }
+
+  // DCFR iterations [t0, t1) of every spot from the current state, with no
+  // exploitability checks (batch.rs:414-535 run_iterations), then the
+  // requested epilogue (EPI_ROOT: root cfvalues and boundary reach under the
+  // average strategy; EPI_EXPL: exploitability, reported by ps_batch_results
+  // with iterations = t1).  The first call after construction or a reset
+  // zeroes the state and builds the board tables.
+  int run_iterations(uint32_t t0, uint32_t t1, int epilogue) {
+    const int n = (int)games.size();
+    int rc = ensure_disc(t1 + 1);
+    if (rc) return rc;
+    if (!ready && (rc = enqueue_setup())) return rc;
+    CU(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
+    CU(cudaEventRecord(ev[2], stream));
+    if (grid_mode) {
+      CU(grid_launch({GRID_ITERATE, (int)t0, (int)t1, 0.f, 0, -1, nullptr, nullptr, nullptr}));
+      if (epilogue & EPI_EXPL) CU(grid_launch({GRID_EXPL, 0, 0, 0.f, 0, -1, nullptr, nullptr, nullptr}));
+      if (epilogue & EPI_ROOT)
+        for (int p = 0; p < 2; ++p)
+          CU(grid_launch({GRID_AVERAGE, 0, 0, 0.f, p, -1, nullptr, nullptr, h_spots[0].root_out[p],
+                          h_spots[0].breach}));
+    } else {
+      CU(cudaMemsetAsync(d_counter, 0, sizeof(int), stream));
+      const SolveJob job{(int)t0, (int)t1, 0, epilogue};
+      CU(launch_solve(d_spots, ninst, inst_k, d_inst, d_counter, d_disc, job, d_target, d_scratch, scratch_floats,
+                      d_expl, d_iters, d_err, grid, block, plan, stream));
+    }
+    CU(cudaEventRecord(ev[3], stream));
+    if (epilogue & EPI_EXPL) {
+      h_expl.resize(n);
+      h_iters.assign(n, (int)t1);
+      CU(cudaMemcpyAsync(h_expl.data(), d_expl, sizeof(float) * n, cudaMemcpyDeviceToHost, stream));
+    }
+    CU(cudaStreamSynchronize(stream));
+    CU(cudaEventElapsedTime(&last_solve_ms, ev[2], ev[3]));
+    last_setup_ms = 0;
     return check_err();
   }
 };
@@ -1653,10 +1777,6 @@ int ps_batch_new(const ps_card_config* cards, const ps_tree_config* trees, int32
           continue;
         }
         if (!g->init(c.range[0], c.range[1], board, tc, errs[i])) continue;
-        if (g->num_boundary > 0) {
-          errs[i] = "depth-boundary trees are not supported in batches";
-          continue;
-        }
         B->games[i] = std::move(g);
         ok[i] = 1;
       }
@@ -1677,6 +1797,158 @@ void ps_batch_free(ps_batch* b) { delete b; }
 int ps_batch_solve(ps_batch* pb, uint32_t max_iter, const float* target) {
   if (!pb || !target) return fail(PS_ERR_INVALID, "bad argument");
   return pb->b->solve(max_iter, target, true);
+}
+
+int ps_batch_run_iterations(ps_batch* pb, uint32_t t0, uint32_t t1, int32_t epilogue) {
+  if (!pb || t1 < t0 || t1 > (1u << 24) || (epilogue & ~(EPI_ROOT | EPI_EXPL)))
+    return fail(PS_ERR_INVALID, "bad argument");
+  return pb->b->run_iterations(t0, t1, epilogue);
+}
+
+int ps_batch_reset(ps_batch* pb) {
+  if (!pb) return fail(PS_ERR_INVALID, "null batch");
+  pb->b->ready = false;
+  pb->b->h_expl.clear();
+  return PS_OK;
+}
+
+int64_t ps_batch_num_boundary_items(ps_batch* pb) { return pb ? (int64_t)pb->b->items.size() : -1; }
+
+int ps_batch_boundary_items(ps_batch* pb, int32_t* spot, int32_t* ordinal, uint8_t* boards, float* pots,
+                            float* stacks) {
+  if (!pb) return fail(PS_ERR_INVALID, "null batch");
+  Batch& B = *pb->b;
+  for (size_t i = 0; i < B.items.size(); ++i) {
+    const Game& g = *B.games[B.items[i].x];
+    if (spot) spot[i] = B.items[i].x;
+    if (ordinal) ordinal[i] = B.items[i].y;
+    if (boards) {
+      const uint8_t bd[4] = {g.flop[0], g.flop[1], g.flop[2], g.turn};
+      std::memcpy(boards + 4 * i, bd, 4);
+    }
+    // the boundary node's pot and the stack behind it (cfvnet neural_net_evaluator.rs:109-110)
+    int64_t node = -1;
+    for (size_t k = 0; k < g.bnd_ordinal.size(); ++k)
+      if (g.bnd_ordinal[k] == B.items[i].y) node = (int64_t)k;
+    const int amount = node >= 0 ? g.arena[node].amount : 0;
+    if (pots) pots[i] = (float)(g.cfg.starting_pot + 2 * amount);
+    if (stacks) stacks[i] = (float)(g.cfg.effective_stack - amount);
+  }
+  return PS_OK;
+}
+
+int ps_batch_set_boundary_cfvs(ps_batch* pb, const float* values, int32_t on_device) {
+  if (!pb || !values) return fail(PS_ERR_INVALID, "bad argument");
+  Batch& B = *pb->b;
+  const size_t ni = B.items.size();
+  if (ni == 0) return PS_OK;
+  const float* src = values;
+  float* tmp = nullptr;
+  if (!on_device) {
+    CU(cudaMalloc(&tmp, 4 * ni * 2 * 1326));
+    CU(cudaMemcpyAsync(tmp, values, 4 * ni * 2 * 1326, cudaMemcpyHostToDevice, B.stream));
+    src = tmp;
+  }
+  std::unique_ptr<float, decltype(&cudaFree)> keep(tmp, &cudaFree);
+  CU(launch_boundary_combo(B.d_spots, B.d_items, (int)ni, BC_SET_VALUES, src, nullptr, B.stream));
+  CU(cudaStreamSynchronize(B.stream));
+  return PS_OK;
+}
+
+int ps_batch_boundary_reach(ps_batch* pb, float* out, int32_t on_device) {
+  if (!pb || !out) return fail(PS_ERR_INVALID, "bad argument");
+  Batch& B = *pb->b;
+  const size_t ni = B.items.size();
+  if (ni == 0) return PS_OK;
+  float* dst = out;
+  float* tmp = nullptr;
+  if (!on_device) {
+    CU(cudaMalloc(&tmp, 4 * ni * 2 * 1326));
+    dst = tmp;
+  }
+  std::unique_ptr<float, decltype(&cudaFree)> keep(tmp, &cudaFree);
+  CU(launch_boundary_combo(B.d_spots, B.d_items, (int)ni, BC_REACH, nullptr, dst, B.stream));
+  if (!on_device) CU(cudaMemcpyAsync(out, tmp, 4 * ni * 2 * 1326, cudaMemcpyDeviceToHost, B.stream));
+  CU(cudaStreamSynchronize(B.stream));
+  return PS_OK;
+}
+
+int ps_batch_root_cfvalues_all(ps_batch* pb, float* out, int32_t on_device) {
+  if (!pb || !out) return fail(PS_ERR_INVALID, "bad argument");
+  Batch& B = *pb->b;
+  const size_t n = B.games.size(), bytes = 4 * n * 2 * 1326;
+  float* dst = out;
+  float* tmp = nullptr;
+  if (!on_device) {
+    CU(cudaMalloc(&tmp, bytes));
+    dst = tmp;
+  }
+  std::unique_ptr<float, decltype(&cudaFree)> keep(tmp, &cudaFree);
+  CU(launch_spot_combo(B.d_spots, (int)n, SC_ROOT, nullptr, dst, B.stream));
+  if (!on_device) CU(cudaMemcpyAsync(out, tmp, bytes, cudaMemcpyDeviceToHost, B.stream));
+  CU(cudaStreamSynchronize(B.stream));
+  return PS_OK;
+}
+
+int ps_batch_adjoint(ps_batch* pb, const float* cot, float* dw, float* dB, int32_t on_device) {
+  if (!pb || !cot) return fail(PS_ERR_INVALID, "bad argument");
+  Batch& B = *pb->b;
+  int rc = B.ensure_adjoint();
+  if (rc) return rc;
+  const size_t n = B.games.size(), ni = B.items.size();
+  const size_t vb = 4 * n * 2 * 1326, ib = 4 * ni * 2 * 1326;
+  const float* d_cot = cot;
+  float* d_dw = dw;
+  float* d_dB = dB;
+  char* tmp = nullptr;
+  if (!on_device) {
+    CU(cudaMalloc(&tmp, 2 * vb + ib + 16));
+    d_cot = (const float*)tmp;
+    d_dw = dw ? (float*)(tmp + vb) : nullptr;
+    d_dB = dB ? (float*)(tmp + 2 * vb) : nullptr;
+    CU(cudaMemcpyAsync((void*)d_cot, cot, vb, cudaMemcpyHostToDevice, B.stream));
+  }
+  std::unique_ptr<char, decltype(&cudaFree)> keep(tmp, &cudaFree);
+  CU(launch_spot_combo(B.d_spots, (int)n, SC_COT, d_cot, nullptr, B.stream));
+  if ((rc = B.adjoint())) return rc;
+  if (d_dw) CU(launch_spot_combo(B.d_spots, (int)n, SC_DW, nullptr, d_dw, B.stream));
+  if (d_dB && ni) CU(launch_boundary_combo(B.d_spots, B.d_items, (int)ni, BC_GRAD, nullptr, d_dB, B.stream));
+  if (!on_device) {
+    if (dw) CU(cudaMemcpyAsync(dw, d_dw, vb, cudaMemcpyDeviceToHost, B.stream));
+    if (dB && ni) CU(cudaMemcpyAsync(dB, d_dB, ib, cudaMemcpyDeviceToHost, B.stream));
+  }
+  CU(cudaStreamSynchronize(B.stream));
+  return PS_OK;
+}
+
+int ps_boundary_encode(int32_t n, const uint8_t* boards, const float* pots, const float* stacks, const float* reach,
+                       void* out, int32_t out_bf16, void* stream) {
+  if (n < 0 || (n > 0 && (!boards || !pots || !stacks || !reach || !out)))
+    return fail(PS_ERR_INVALID, "bad argument");
+  if (n == 0) return PS_OK;
+  std::vector<uint8_t> hb((size_t)n * 4);
+  for (int i = 0; i < n; ++i) {
+    uint64_t seen = 0;
+    for (int k = 0; k < 4; ++k) {
+      const uint8_t c = boards[4 * i + k];
+      if (c >= 52 || (seen >> c & 1)) return fail(PS_ERR_INVALID, "boards must hold 4 distinct cards below 52");
+      seen |= 1ull << c;
+      hb[4 * i + k] = c;
+    }
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t ob = ((hb.size() + 15) & ~(size_t)15);
+  char* d = nullptr;
+  CU(cudaMalloc(&d, ob + 8 * (size_t)n + 16));
+  std::unique_ptr<char, decltype(&cudaFree)> keep(d, &cudaFree);
+  float* d_pot = (float*)(d + ob);
+  float* d_stack = d_pot + n;
+  CU(cudaMemcpyAsync(d, hb.data(), hb.size(), cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(d_pot, pots, 4 * (size_t)n, cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(d_stack, stacks, 4 * (size_t)n, cudaMemcpyHostToDevice, s));
+  CU(launch_boundary_encode(n, (const uint8_t*)d, d_pot, d_stack, reach, out, out_bf16 ? 1 : 0, s));
+  CU(cudaStreamSynchronize(s));
+  return PS_OK;
 }
 
 int ps_batch_results(ps_batch* pb, float* expl, int32_t* iters) {

@@ -9,8 +9,11 @@
 //   cfv_p[h] = (pot + stack) * sum_{r not in hand h} w_o[r] * net[i][p][r][c(h)]
 //                              / sum_{r not in hand h} w_o[r]            (0 if the sum is 0)
 // Player 0 is weighted by IP reach, player 1 by OOP reach, as in the reference.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include "ps_launch.hpp"
 
 namespace ps {
 
@@ -85,6 +88,157 @@ __global__ void k_boundary_river_reduce(int n, const uint8_t* __restrict__ board
     }
     out[((size_t)item * 2 + p) * H + h] = den > 0.0 ? (float)(num / den * scale) : 0.0f;
   }
+}
+
+// combo index of two distinct cards (card.rs:50-55)
+__device__ __forceinline__ int combo_index(int a, int b) {
+  const int lo = a < b ? a : b, hi = a < b ? b : a;
+  return lo * (101 - lo) / 2 + hi - 1;
+}
+
+// One block per boundary item (spot, ordinal), both players: between the
+// spot's hand-order rows (stride vstride) and the item's 1326-combo rows.
+__global__ void k_boundary_combo(const SpotDev* __restrict__ spots, const int2* __restrict__ items, int which,
+                                 const float* __restrict__ in, float* __restrict__ out) {
+  const int2 it = items[blockIdx.x];
+  const SpotDev& sp = spots[it.x];
+  for (int p = 0; p < 2; ++p) {
+    const uint8_t* cards = sp.cards[p];
+    const size_t hrow = ((size_t)it.y * 2 + p) * sp.vstride;
+    const size_t crow = ((size_t)blockIdx.x * 2 + p) * kCombos;
+    if (which == BC_SET_VALUES) {
+      float* dst = const_cast<float*>(sp.bcfv) + hrow;
+      const float* src = in + crow;
+      for (int h = threadIdx.x; h < sp.vstride; h += blockDim.x)
+        dst[h] = h < sp.H[p] ? src[combo_index(cards[2 * h], cards[2 * h + 1])] : 0.f;
+    } else {
+      const float* from = which == BC_REACH ? sp.breach : sp.bgrad;
+      float* dst = out + crow;
+      for (int c = threadIdx.x; c < kCombos; c += blockDim.x) dst[c] = 0.f;
+      __syncthreads();
+      if (from)
+        for (int h = threadIdx.x; h < sp.H[p]; h += blockDim.x)
+          dst[combo_index(cards[2 * h], cards[2 * h + 1])] = from[hrow + h];
+      __syncthreads();
+    }
+  }
+}
+
+cudaError_t launch_boundary_combo(const SpotDev* spots, const int2* items, int nitems, int which,
+                                  const float* in, float* out, cudaStream_t s) {
+  if (nitems <= 0) return cudaSuccess;
+  k_boundary_combo<<<nitems, 256, 0, s>>>(spots, items, which, in, out);
+  return cudaGetLastError();
+}
+
+// One block per spot, both players: between the spot's hand-order vectors and
+// its 1326-combo rows.
+__global__ void k_spot_combo(const SpotDev* __restrict__ spots, int which, const float* __restrict__ in,
+                             float* __restrict__ out) {
+  const SpotDev& sp = spots[blockIdx.x];
+  for (int p = 0; p < 2; ++p) {
+    const uint8_t* cards = sp.cards[p];
+    const size_t crow = ((size_t)blockIdx.x * 2 + p) * kCombos;
+    if (which == SC_COT) {
+      float* dst = sp.adj_g[p];
+      for (int h = threadIdx.x; h < sp.hs[p]; h += blockDim.x)
+        dst[h] = h < sp.H[p] ? in[crow + combo_index(cards[2 * h], cards[2 * h + 1])] : 0.f;
+    } else {
+      const float* from = which == SC_ROOT ? sp.root_out[p] : sp.adj_dw[p];
+      float* dst = out + crow;
+      for (int c = threadIdx.x; c < kCombos; c += blockDim.x) dst[c] = 0.f;
+      __syncthreads();
+      if (from)
+        for (int h = threadIdx.x; h < sp.H[p]; h += blockDim.x)
+          dst[combo_index(cards[2 * h], cards[2 * h + 1])] = from[h];
+      __syncthreads();
+    }
+  }
+}
+
+cudaError_t launch_spot_combo(const SpotDev* spots, int n, int which, const float* in, float* out,
+                              cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_spot_combo<<<n, 256, 0, s>>>(spots, which, in, out);
+  return cudaGetLastError();
+}
+
+// Input rows of the boundary network, one block per (item, player): the
+// item's two reach rows are staged in shared memory and written out once per
+// river card with the hands holding that card zeroed.  Pure store bandwidth:
+// 2720 values per row, written as 16-byte (f32) or 8-byte (bf16) vectors.
+template <bool BF16>
+__global__ void k_boundary_encode(const uint8_t* __restrict__ boards, const float* __restrict__ pots,
+                                  const float* __restrict__ stacks, const float* __restrict__ reach,
+                                  void* __restrict__ out) {
+  const int item = blockIdx.x >> 1, player = blockIdx.x & 1;
+  __shared__ float s_r[2 * kCombos];
+  __shared__ uint16_t s_pair[kCombos];  // c1 | c2 << 8
+  __shared__ uint8_t s_river[kRivers];
+  const uint8_t* bd = boards + 4 * item;
+  const uint64_t bmask = (1ull << bd[0]) | (1ull << bd[1]) | (1ull << bd[2]) | (1ull << bd[3]);
+  if (threadIdx.x == 0) {
+    int k = 0;
+    for (int c = 0; c < 52; ++c)
+      if (!(bmask >> c & 1)) s_river[k++] = (uint8_t)c;
+  }
+  for (int c1 = threadIdx.x; c1 < 51; c1 += blockDim.x)
+    for (int c2 = c1 + 1; c2 < 52; ++c2) s_pair[combo_index(c1, c2)] = (uint16_t)(c1 | c2 << 8);
+  const float* r = reach + (size_t)item * 2 * kCombos;
+  for (int c = threadIdx.x; c < 2 * kCombos; c += blockDim.x) s_r[c] = r[c];
+  // boundary_evaluator.rs:35-36, :54-56 in f32
+  const float pot = pots[item], stack = stacks[item];
+  const float total = __fadd_rn(pot, stack);
+  const float norm = total > 0.f ? total : 1.f;
+  const float fpot = __fdiv_rn(pot, norm), fstack = __fdiv_rn(stack, norm), fpl = (float)player;
+  const unsigned ranks4 = (1u << (bd[0] >> 2)) | (1u << (bd[1] >> 2)) | (1u << (bd[2] >> 2)) | (1u << (bd[3] >> 2));
+  __syncthreads();
+  constexpr int kVec = kBoundaryInput / 4;
+  for (int ri = 0; ri < kRivers; ++ri) {
+    const int river = s_river[ri];
+    const uint64_t b5 = bmask | (1ull << river);
+    const unsigned ranks = ranks4 | (1u << (river >> 2));
+    const size_t row = ((size_t)blockIdx.x * kRivers + ri) * kBoundaryInput;
+    for (int q = threadIdx.x; q < kVec; q += blockDim.x) {
+      float v[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int f = 4 * q + e;
+        float x;
+        if (f < 2 * kCombos) {
+          const int c = f < kCombos ? f : f - kCombos;
+          const unsigned pr = s_pair[c];
+          x = ((pr & 0xFF) == (unsigned)river || (pr >> 8) == (unsigned)river) ? 0.f : s_r[f];
+        } else if (f < 2 * kCombos + 52) {
+          x = (b5 >> (f - 2 * kCombos) & 1) ? 1.f : 0.f;
+        } else if (f < 2 * kCombos + 65) {
+          x = (ranks >> (f - 2 * kCombos - 52) & 1) ? 1.f : 0.f;
+        } else {
+          x = f == kBoundaryInput - 3 ? fpot : f == kBoundaryInput - 2 ? fstack : fpl;
+        }
+        v[e] = x;
+      }
+      if (BF16) {
+        __nv_bfloat162 a = __floats2bfloat162_rn(v[0], v[1]), b = __floats2bfloat162_rn(v[2], v[3]);
+        uint2 w;
+        w.x = *reinterpret_cast<unsigned*>(&a);
+        w.y = *reinterpret_cast<unsigned*>(&b);
+        reinterpret_cast<uint2*>(static_cast<__nv_bfloat16*>(out) + row)[q] = w;
+      } else {
+        reinterpret_cast<float4*>(static_cast<float*>(out) + row)[q] = make_float4(v[0], v[1], v[2], v[3]);
+      }
+    }
+  }
+}
+
+cudaError_t launch_boundary_encode(int n, const uint8_t* boards, const float* pots, const float* stacks,
+                                   const float* reach, void* out, int bf16, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  if (bf16)
+    k_boundary_encode<true><<<2 * n, 256, 0, s>>>(boards, pots, stacks, reach, out);
+  else
+    k_boundary_encode<false><<<2 * n, 256, 0, s>>>(boards, pots, stacks, reach, out);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_boundary_river_reduce(int n, const uint8_t* boards, const float* denorm, const float* net,

@@ -99,6 +99,12 @@ struct SpotDev {
   float* chcfv;        // chance-node cfvalues (finalize)
   float* slots;        // [num_slots][vstride] scratch vectors
   float* root_out[2];  // [hs] root cfv per player (exploitability / root_cfvalues)
+  float* breach;       // [num_boundary][2][vstride] each player's reach at each boundary under the
+                       // average strategy (written by the batched solve's epilogue), or null
+  // batched adjoint of the fixed-strategy evaluation (null until first used):
+  float* adj_g[2];     // [hs] cotangent of player p's root cfvalues
+  float* adj_dw[2];    // [hs] gradient with respect to player p's initial weights
+  float* bgrad;        // [num_boundary][2][vstride] gradient with respect to the boundary values, or null
 };
 
 // One DCFR iteration's discount factors (computed on the host in f64, solver.rs:26-44).

@@ -796,13 +796,13 @@ __device__ bool bind_ctx(Ctx& c, const SpotDev* sp, float* scratch, size_t scrat
 #endif
 #define PS_SOLVE_BOUNDS __launch_bounds__(kMaxSolveBlock, PS_LB_MIN)
 
-// Batched persistent solve: CTAs pull spots from `counter` (in `order`), and
-// run the full reference solve loop (solver.rs:108-176) per spot:
-//   expl = exploitability; for t < max_iter { if expl <= target break;
-//   iterate(t); if (t+1) % 5 == 0 || t+1 == max_iter: expl = exploitability }.
+// Batched persistent solve: CTAs pull instances (up to K spots of one tree
+// shape) from `counter` and run job's work on them (SolveJob): the full
+// reference solve loop (solver.rs:108-176) per spot, or a fixed iteration
+// range, then the optional average-strategy epilogue.
 __global__ void PS_SOLVE_BOUNDS k_solve(const SpotDev* __restrict__ spots, int ninst, int K,
                                         const int* __restrict__ inst, int* counter, const Discount* __restrict__ disc,
-                                        int max_iter, const float* __restrict__ target, float* scratch,
+                                        SolveJob job, const float* __restrict__ target, float* scratch,
                                         size_t scratch_floats, float* out_expl, int* out_iters, SmemPlan plan,
                                         int* err) {
   extern __shared__ float4 smem4[];
@@ -833,38 +833,78 @@ __global__ void PS_SOLVE_BOUNDS k_solve(const SpotDev* __restrict__ spots, int n
       iters[k] = 0;
     }
     if (!active) continue;
-    // the reference loop per spot (solver.rs:108-176): expl = exploitability;
-    // for t < max_iter { if expl <= target break; iterate(t); if (t+1) % 5 == 0
-    // || t+1 == max_iter: expl = exploitability }; a spot leaves the lockstep
-    // set at the first check that meets its target
-    exploitability_multi(cs, K, active, expl);
-    unsigned live = 0;
-    for (int k = 0; k < K; ++k)
-      if ((active >> k & 1u) && !(expl[k] <= tgt[k])) live |= 1u << k;
-    int t = 0;
-    for (; t < max_iter && live; ++t) {
-      dcfr_iteration_multi(cs, K, live, disc[t]);
-      if ((t + 1) % 5 == 0 || t + 1 == max_iter) {
-        exploitability_multi(cs, K, live, expl);
-        for (int k = 0; k < K; ++k)
-          if ((live >> k & 1u) && expl[k] <= tgt[k]) {
-            iters[k] = t + 1;
-            live &= ~(1u << k);
-          }
+    if (job.adjoint) {
+      // the fixed-strategy evaluation and its adjoint for every spot, as
+      // ps_eval_fixed_strategy_adjoint runs them for one game: forward passes
+      // from the spots' weights (values, boundary-gradient factors), then the
+      // transposed passes from the cotangents with the payoffs of the other
+      // player (owner)
+      const Discount dz{0.f, 0.f, 0.f, 0.f};
+      for (int k = 0; k < K; ++k) {
+        cs[k].signed_reach = 1;
+        cs[k].bgrad = cs[k].sp->bgrad;
       }
+      for (int pass = 0; pass < 4; ++pass) {
+        const int p = pass < 2 ? pass : 3 - pass;  // traversers 0, 1, then 1, 0
+        for (int k = 0; k < K; ++k) {
+          cs[k].root_reach = pass < 2 ? cs[k].sp->w[p ^ 1] : cs[k].sp->adj_g[p ^ 1];
+          cs[k].owner = pass < 2 ? -1 : (p ^ 1);
+        }
+        run_pass_multi(cs, K, active, p, dz, M_AVG);
+        for (int k = 0; k < K; ++k) {
+          if (!(active >> k & 1u)) continue;
+          const SpotDev& sp = *cs[k].sp;
+          float* dst = pass < 2 ? sp.root_out[p] : sp.adj_dw[p];
+          const float* r = slot_at(cs[k], sp.root_slot[p]);
+          for (int h = threadIdx.x; h < sp.H[p]; h += blockDim.x) dst[h] = r[h];
+        }
+        __syncthreads();
+      }
+      continue;
     }
-    for (int k = 0; k < K; ++k)
-      if (live >> k & 1u) iters[k] = t;
-    if (threadIdx.x == 0)
+    int t = job.t0;
+    if (job.checks) {
+      // the reference loop per spot (solver.rs:108-176): expl = exploitability;
+      // for t < max_iter { if expl <= target break; iterate(t); if (t+1) % 5 == 0
+      // || t+1 == max_iter: expl = exploitability }; a spot leaves the lockstep
+      // set at the first check that meets its target
+      const int max_iter = job.t1;
+      exploitability_multi(cs, K, active, expl);
+      unsigned live = 0;
+      for (int k = 0; k < K; ++k)
+        if ((active >> k & 1u) && !(expl[k] <= tgt[k])) live |= 1u << k;
+      for (t = 0; t < max_iter && live; ++t) {
+        dcfr_iteration_multi(cs, K, live, disc[t]);
+        if ((t + 1) % 5 == 0 || t + 1 == max_iter) {
+          exploitability_multi(cs, K, live, expl);
+          for (int k = 0; k < K; ++k)
+            if ((live >> k & 1u) && expl[k] <= tgt[k]) {
+              iters[k] = t + 1;
+              live &= ~(1u << k);
+            }
+        }
+      }
+      for (int k = 0; k < K; ++k)
+        if (live >> k & 1u) iters[k] = t;
+    } else {
+      // a fixed iteration range (batch.rs:414-535 run_iterations)
+      for (; t < job.t1; ++t) dcfr_iteration_multi(cs, K, active, disc[t]);
+      for (int k = 0; k < K; ++k) iters[k] = t;
+      if (job.epilogue & EPI_EXPL) exploitability_multi(cs, K, active, expl);
+    }
+    if (threadIdx.x == 0 && (job.checks || (job.epilogue & EPI_EXPL)))
       for (int k = 0; k < K; ++k)
         if (active >> k & 1u) {
           out_expl[ids[k]] = expl[k];
           out_iters[ids[k]] = iters[k];
         }
+    if (!(job.epilogue & EPI_ROOT)) continue;
     // root cfvalues of both players under the average strategy: the
     // per-hand values a datagen record needs (the reference computes them on
-    // the host from the strategy sums)
+    // the host from the strategy sums); the same passes record the reach at
+    // the depth boundaries (batch.rs:765-790 compute_reach_at_nodes)
     const Discount dz{0.f, 0.f, 0.f, 0.f};
+    for (int k = 0; k < K; ++k) cs[k].breach = cs[k].sp->breach;
     for (int p = 0; p < 2; ++p) {
       for (int k = 0; k < K; ++k) cs[k].root_reach = cs[k].sp->w[p ^ 1];
       run_pass_multi(cs, K, active, p, dz, M_AVG);
@@ -1238,14 +1278,16 @@ cudaError_t launch_setup(const SpotDev* spots, const int2* work, int nwork, cons
 }
 
 cudaError_t launch_solve(const SpotDev* spots, int ninst, int K, const int* inst, int* counter,
-                         const Discount* disc, int max_iter, const float* target, float* scratch,
+                         const Discount* disc, const SolveJob& job, const float* target, float* scratch,
                          size_t scratch_floats, float* out_expl, int* out_iters, int* err, int grid, int block,
                          const SmemPlan& plan, cudaStream_t s) {
-  if (K < 1 || K > kMaxInst) return cudaErrorInvalidValue;
+  if (K < 1 || K > kMaxInst || job.t0 < 0 || job.t1 < job.t0 || (job.checks && job.t0 != 0) ||
+      (job.adjoint && (job.checks || job.t1 != job.t0)))
+    return cudaErrorInvalidValue;
   size_t smem = plan.total();
   cudaError_t e = set_smem((const void*)k_solve, smem);
   if (e != cudaSuccess) return e;
-  k_solve<<<grid, block, smem, s>>>(spots, ninst, K, inst, counter, disc, max_iter, target, scratch, scratch_floats,
+  k_solve<<<grid, block, smem, s>>>(spots, ninst, K, inst, counter, disc, job, target, scratch, scratch_floats,
                                      out_expl, out_iters, plan, err);
   return cudaGetLastError();
 }

@@ -57,15 +57,57 @@ int grid_ctas(int block, const SmemPlan& plan);
 cudaError_t launch_boundary_river_reduce(int n, const uint8_t* boards, const float* denorm, const float* net,
                                          const float* reach, const int32_t* hands, int H, float* out,
                                          cudaStream_t s);
+// Boundary items of a batch (item = (spot, boundary ordinal)) in the 1326-combo
+// layout (card.rs:50-55 index), [items][2][1326], against each spot's hand-order
+// buffers.  which: BC_SET_VALUES gathers `in` into sp.bcfv; BC_REACH / BC_GRAD
+// scatter sp.breach / sp.bgrad into `out` (combos outside the spot's hand list
+// read 0).
+enum { BC_SET_VALUES = 0, BC_REACH = 1, BC_GRAD = 2 };
+cudaError_t launch_boundary_combo(const SpotDev* spots, const int2* items, int nitems, int which,
+                                  const float* in, float* out, cudaStream_t s);
+// Per-spot vectors of a batch in the combo layout, [n][2][1326]: SC_ROOT and
+// SC_DW scatter sp.root_out / sp.adj_dw into `out`; SC_COT gathers `in` into
+// sp.adj_g.
+enum { SC_ROOT = 0, SC_COT = 1, SC_DW = 2 };
+cudaError_t launch_spot_combo(const SpotDev* spots, int n, int which, const float* in, float* out,
+                              cudaStream_t s);
+// Boundary-network input rows (cfvnet eval/boundary_evaluator.rs:27-60) for
+// every item, player and river card not on the item's board: [n][2][48][2720],
+// oop reach | ip reach (1326 each, zeroed where a hand holds the river card) |
+// 52 board one-hot | 13 rank presence | pot/(pot+stack) | stack/(pot+stack) | player.
+// boards [n][4], pots [n], stacks [n], reach [n][2][1326]; device pointers;
+// out is f32, or bf16 (round to nearest even) when bf16 != 0.
+constexpr int kBoundaryInput = 2720;
+cudaError_t launch_boundary_encode(int n, const uint8_t* boards, const float* pots, const float* stacks,
+                                   const float* reach, void* out, int bf16, cudaStream_t s);
 cudaError_t launch_grid(const SpotDev* spot, const GridJob& job, const Discount* disc, float* scratch,
                         size_t scratch_floats, float* out_expl, int* out_iters, unsigned* bar, double* gred,
                         int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s);
 cudaError_t launch_setup(const SpotDev* spots, const int2* work, int nwork, const int32_t* table, int* err,
                          int grid, cudaStream_t s);
+// Work of one persistent batched-solve launch.
+//   checks = 1: the reference's solve loop over iterations [0, t1): exploitability
+//     before the first iteration, after every fifth and after the last one; a
+//     spot stops at the first check that meets its target (t0 must be 0).
+//   checks = 0: iterations [t0, t1) for every spot, no checks (the reference
+//     GPU batch's run_iterations); EPI_EXPL adds one exploitability at the end.
+//   EPI_ROOT: afterwards, both players' root cfvalues under the average
+//     strategy into sp.root_out; spots with a boundary-reach buffer (sp.breach)
+//     also record each player's reach at every depth boundary in the same passes.
+//   adjoint = 1 (no iterations): the fixed-strategy evaluation under the
+//     average strategy from the spots' weights (sp.root_out) and its adjoint
+//     from the cotangents sp.adj_g (sp.adj_dw, sp.bgrad zeroed beforehand).
+enum { EPI_ROOT = 1, EPI_EXPL = 2 };
+struct SolveJob {
+  int t0, t1;
+  int checks;
+  int epilogue;
+  int adjoint = 0;
+};
 // Persistent batched solve over `ninst` instances of K spots (inst: [ninst][K]
 // spot ids, -1 = empty); scratch holds K * scratch_floats floats per CTA.
 cudaError_t launch_solve(const SpotDev* spots, int ninst, int K, const int* inst, int* counter,
-                         const Discount* disc, int max_iter, const float* target, float* scratch,
+                         const Discount* disc, const SolveJob& job, const float* target, float* scratch,
                          size_t scratch_floats, float* out_expl, int* out_iters, int* err, int grid, int block,
                          const SmemPlan& plan, cudaStream_t s);
 cudaError_t launch_iterate(const SpotDev* spots, int nspots, const Discount* disc, int t0, int t1,

@@ -49,3 +49,90 @@ def boundary_river_reduce(boards, pots, stacks, net, reach, hands):
         s.ctypes.data_as(C.POINTER(C.c_float)), C.c_void_p(net.data_ptr()), C.c_void_p(reach.data_ptr()),
         C.c_void_p(hands.data_ptr()), hands.numel(), C.c_void_p(out.data_ptr()), C.c_void_p(stream)))
     return out
+
+
+def boundary_encode(boards, pots, stacks, reach, bf16: bool = False):
+    """Boundary-network input rows on the device (ps_boundary_encode):
+    [n, 2, 48, 2720] for n items, their two players and the 48 river cards
+    not on each 4-card board (cfvnet eval/boundary_evaluator.rs:27-60).
+
+    boards [n, 4], pots / stacks [n] are host arrays; reach [n, 2, 1326]
+    (OOP, IP) is a CUDA tensor.  Returns a CUDA tensor, f32 or bf16."""
+    import torch
+
+    b = np.ascontiguousarray(boards, np.uint8).reshape(-1, 4)
+    p = np.ascontiguousarray(pots, np.float32)
+    s = np.ascontiguousarray(stacks, np.float32)
+    n = b.shape[0]
+    assert reach.is_cuda and tuple(reach.shape) == (n, 2, 1326)
+    reach = reach.contiguous().float()
+    out = torch.empty((n, 2, 48, 2720), dtype=torch.bfloat16 if bf16 else torch.float32, device=reach.device)
+    if n == 0:
+        return out
+    stream = torch.cuda.current_stream(reach.device).cuda_stream
+    N.check(N.lib().ps_boundary_encode(
+        n, b.ctypes.data_as(C.POINTER(C.c_uint8)), p.ctypes.data_as(C.POINTER(C.c_float)),
+        s.ctypes.data_as(C.POINTER(C.c_float)), C.c_void_p(reach.data_ptr()), C.c_void_p(out.data_ptr()),
+        int(bf16), C.c_void_p(stream)))
+    return out
+
+
+def evaluate_boundaries(items: dict, reach, net, pot_source: str = "boundary", denormalize: bool = False,
+                        bf16: bool = False, chunk_items: int = 1024):
+    """Boundary values of every item from a boundary-value network, all on
+    the device: input rows (boundary_encode) -> net -> reach-weighted 48-river
+    average (boundary_river_reduce); the host steps of the reference's
+    datagen/gpu_boundary_eval.rs:107-269.
+
+    items: BatchSolver.boundary_items(); reach: [items, 2, 1326] CUDA tensor
+    (BatchSolver.boundary_reach(device=True)); net: a callable mapping
+    [rows, 2720] to [rows, 1326].  pot_source: "boundary" encodes each
+    boundary's own pot and stack (as cfvnet datagen/domain/
+    neural_net_evaluator.rs:109-110 does), "root" the spot's starting pot and
+    stack (as datagen/domain/pipeline.rs:818-819 does).  denormalize: scale
+    the averages by pot + stack (chips), as gpu_boundary_eval.rs:238-256 does.
+    Returns [items, 2, 1326] (combo layout) for BatchSolver.set_boundary_cfvs."""
+    import torch
+
+    n = len(items["spot"])
+    if pot_source == "root":
+        pots, stacks = items["root_pots"], items["root_stacks"]
+    else:
+        pots, stacks = items["pots"], items["stacks"]
+    out = torch.empty((n, 2, 1326), dtype=torch.float32, device=reach.device)
+    combos = torch.arange(1326, dtype=torch.int32, device=reach.device)
+    for a in range(0, n, chunk_items):
+        z = slice(a, min(n, a + chunk_items))
+        m = z.stop - z.start
+        rows = boundary_encode(items["boards"][z], pots[z], stacks[z], reach[z], bf16=bf16)
+        with torch.no_grad():
+            y = net(rows.view(m * 96, 2720)).float().view(m, 2, 48, 1326)
+        if denormalize:
+            dp, ds = pots[z], stacks[z]
+        else:
+            dp, ds = np.ones(m, np.float32), np.zeros(m, np.float32)
+        out[z] = boundary_river_reduce(items["boards"][z], dp, ds, y, reach[z], combos)
+    return out
+
+
+def solve_with_boundary_net(batch, net, iterations: int, eval_interval: int, **eval_kwargs):
+    """The turn-datagen loop of cfvnet datagen/domain/pipeline.rs:648-700 on a
+    batch of depth-limited spots, with every step on the device: boundary
+    values from the network under the uniform strategy, then every
+    `eval_interval` iterations again from the reach under the current average
+    strategy, until `iterations`.  One launch per interval runs its
+    iterations plus the average-strategy epilogue that yields the next
+    boundary reach; the last one also the exploitability and the root
+    cfvalues (BatchSolver.results / root_cfvalues).  Returns the items."""
+    items = batch.boundary_items()
+    batch.reset()
+    batch.run_iterations(0, 0, root=True)  # average strategy of zero sums: uniform
+    t = 0
+    while True:
+        reach = batch.boundary_reach(device=True)
+        batch.set_boundary_cfvs(evaluate_boundaries(items, reach, net, **eval_kwargs))
+        end = min(iterations, t + eval_interval)
+        batch.run_iterations(t, end, root=True, exploitability=end >= iterations)
+        t = end
+        if t >= iterations:
+            return items

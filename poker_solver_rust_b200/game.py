@@ -494,6 +494,10 @@ def _pack_configs(card_configs, tree_configs):
     return cc, tc, (ranges, strings, menus, T)
 
 
+def _is_cuda_tensor(x) -> bool:
+    return type(x).__module__.startswith("torch") and getattr(x, "is_cuda", False)
+
+
 class BatchSolver:
     """Thousands of independent subgames solved by one persistent launch
     (replaces the per-spot GpuBatchSolver launches of the reference's GPU
@@ -511,6 +515,7 @@ class BatchSolver:
         self._h = h
         self.n = n
         self.starting_pots = np.array([t.starting_pot for t in tree_configs], np.float32)
+        self.effective_stacks = np.array([t.effective_stack for t in tree_configs], np.float32)
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -567,3 +572,114 @@ class BatchSolver:
         N.check(N.lib().ps_batch_config(self._h, C.byref(a), C.byref(b), C.byref(c)))
         return {"block_threads": a.value, "grid": b.value, "ctas_per_sm": c.value,
                 "scan_buffers": N.check(N.lib().ps_batch_scan_buffers(self._h))}
+
+    # ---- depth-limited spots: iteration ranges and boundary values
+    #      (gpu-range-solver batch.rs:279-585) ----
+
+    def run_iterations(self, start: int, end: int, root: bool = True, exploitability: bool = False) -> None:
+        """DCFR iterations [start, end) of every spot from the current state in
+        one launch, with no exploitability checks (batch.rs:414
+        run_iterations).  root: afterwards compute the root cfvalues and the
+        boundary reach under the average strategy; exploitability: also the
+        exploitability of every spot (results())."""
+        epi = (N.PS_EPI_ROOT if root else 0) | (N.PS_EPI_EXPL if exploitability else 0)
+        N.check(N.lib().ps_batch_run_iterations(self._h, start, end, epi))
+
+    def reset(self) -> None:
+        """The next run_iterations starts from zero regrets and strategy sums."""
+        N.check(N.lib().ps_batch_reset(self._h))
+
+    def num_boundary_items(self) -> int:
+        return int(N.lib().ps_batch_num_boundary_items(self._h))
+
+    def boundary_items(self) -> dict:
+        """Per boundary item (one depth boundary of one spot, spot by spot):
+        spot, ordinal, 4-card board, the boundary's pot and the stack behind it,
+        and the spot's starting pot and effective stack."""
+        n = self.num_boundary_items()
+        spot = np.zeros(n, np.int32)
+        ordinal = np.zeros(n, np.int32)
+        boards = np.zeros((n, 4), np.uint8)
+        pots = np.zeros(n, np.float32)
+        stacks = np.zeros(n, np.float32)
+        if n:
+            N.check(N.lib().ps_batch_boundary_items(
+                self._h, spot.ctypes.data_as(C.POINTER(C.c_int32)), ordinal.ctypes.data_as(C.POINTER(C.c_int32)),
+                boards.ctypes.data_as(C.POINTER(C.c_uint8)), _fp(pots), _fp(stacks)))
+        return {"spot": spot, "ordinal": ordinal, "boards": boards, "pots": pots, "stacks": stacks,
+                "root_pots": self.starting_pots[spot], "root_stacks": self.effective_stacks[spot]}
+
+    def set_boundary_cfvs(self, values) -> None:
+        """Boundary values of every item, [items, 2, 1326] in the 1326-combo
+        layout (numpy array or CUDA tensor); each spot takes its own hands'
+        entries, with the semantics of PostFlopGame.set_boundary_cfvs."""
+        n = self.num_boundary_items()
+        if _is_cuda_tensor(values):
+            import torch
+
+            v = values.detach().to(torch.float32).contiguous()
+            assert tuple(v.shape) == (n, 2, 1326), v.shape
+            torch.cuda.current_stream(v.device).synchronize()
+            N.check(N.lib().ps_batch_set_boundary_cfvs(self._h, C.c_void_p(v.data_ptr()), 1))
+        else:
+            v = np.ascontiguousarray(values, np.float32)
+            assert v.shape == (n, 2, 1326), v.shape
+            N.check(N.lib().ps_batch_set_boundary_cfvs(self._h, C.c_void_p(v.ctypes.data), 0))
+
+    def root_cfvalues_all(self, device: bool = False):
+        """Both players' root cfvalues of every spot under the average strategy
+        (last root epilogue, solve or adjoint), [n, 2, 1326] in the combo
+        layout (numpy, or a CUDA tensor when device=True)."""
+        if device:
+            import torch
+
+            out = torch.empty((self.n, 2, 1326), dtype=torch.float32, device="cuda")
+            torch.cuda.current_stream().synchronize()
+            N.check(N.lib().ps_batch_root_cfvalues_all(self._h, C.c_void_p(out.data_ptr()), 1))
+            return out
+        out = np.zeros((self.n, 2, 1326), np.float32)
+        N.check(N.lib().ps_batch_root_cfvalues_all(self._h, C.c_void_p(out.ctypes.data), 0))
+        return out
+
+    def adjoint(self, cotangent):
+        """Batched adjoint of the fixed-strategy evaluation (ps_batch_adjoint):
+        cotangent [n, 2, 1326] = dL/d(root cfvalues) -> (dL/d(initial weights)
+        [n, 2, 1326], dL/d(boundary values) [items, 2, 1326]), as CUDA tensors
+        for a CUDA cotangent, numpy arrays otherwise."""
+        ni = self.num_boundary_items()
+        if _is_cuda_tensor(cotangent):
+            import torch
+
+            g = cotangent.detach().to(torch.float32).contiguous()
+            assert tuple(g.shape) == (self.n, 2, 1326), g.shape
+            dw = torch.empty_like(g)
+            dB = torch.empty((ni, 2, 1326), dtype=torch.float32, device=g.device)
+            torch.cuda.current_stream(g.device).synchronize()
+            N.check(N.lib().ps_batch_adjoint(self._h, C.c_void_p(g.data_ptr()), C.c_void_p(dw.data_ptr()),
+                                             C.c_void_p(dB.data_ptr()), 1))
+            return dw, dB
+        g = np.ascontiguousarray(cotangent, np.float32)
+        assert g.shape == (self.n, 2, 1326), g.shape
+        dw = np.zeros_like(g)
+        dB = np.zeros((ni, 2, 1326), np.float32)
+        N.check(N.lib().ps_batch_adjoint(self._h, C.c_void_p(g.ctypes.data), C.c_void_p(dw.ctypes.data),
+                                         C.c_void_p(dB.ctypes.data), 0))
+        return dw, dB
+
+    def boundary_reach(self, device: bool = False):
+        """Each player's reach at every boundary under the average strategy as
+        of the last root epilogue, [items, 2, 1326] (numpy, or a CUDA tensor
+        when device=True)."""
+        n = self.num_boundary_items()
+        if device:
+            import torch
+
+            out = torch.empty((n, 2, 1326), dtype=torch.float32, device="cuda")
+            torch.cuda.current_stream().synchronize()
+            if n:
+                N.check(N.lib().ps_batch_boundary_reach(self._h, C.c_void_p(out.data_ptr()), 1))
+            return out
+        out = np.zeros((n, 2, 1326), np.float32)
+        if n:
+            N.check(N.lib().ps_batch_boundary_reach(self._h, C.c_void_p(out.ctypes.data), 0))
+        return out

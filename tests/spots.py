@@ -77,6 +77,54 @@ def datagen_spots(n: int, seed: int = 7):
     return [datagen_spot(rng) for _ in range(n)]
 
 
+_PAIRS = None
+
+
+def _board_blocked(board):
+    global _PAIRS
+    if _PAIRS is None:
+        _PAIRS = np.array([ps.index_to_card_pair(i) for i in range(1326)])
+    b = np.asarray(board)
+    return np.isin(_PAIRS[:, 0], b) | np.isin(_PAIRS[:, 1], b)
+
+
+def turn_boundary_spot(rng):
+    """Depth-limited turn spot: the turn settings of turn_spot (bets 33% / 75%
+    / all-in, raise 60%) with a depth boundary at every non-fold turn
+    terminal, and the range / pot / stack distributions of datagen_spot."""
+    board = [int(x) for x in rng.choice(52, 4, replace=False)]
+    blocked = _board_blocked(board)
+    r = []
+    for _ in range(2):
+        w = rng.beta(0.5, 0.5, 1326).astype(np.float32)
+        w[rng.random(1326) < 0.3] = 0.0
+        w[blocked] = 0.0
+        r.append(w)
+    pot = int(rng.integers(20, 201))
+    stack = max(1, int(round(float(rng.uniform(0.5, 10.0)) * pot)))
+    sizes = B("33%, 75%, a", "60%")
+    tc = TreeConfig(initial_state=BoardState.Turn, starting_pot=pot, effective_stack=stack,
+                    turn_bet_sizes=[sizes, sizes], river_bet_sizes=[sizes, sizes], depth_limit=0)
+    return r, board, tc
+
+
+def turn_boundary_spots(n: int, seed: int = 11):
+    rng = np.random.default_rng(seed)
+    return [turn_boundary_spot(rng) for _ in range(n)]
+
+
+def boundary_values(rng, batch, scale=0.25):
+    """Seeded boundary values [items, 2, 1326] ~ N(0, (scale * pot)^2) of a
+    batch's boundary items, zero on board-blocked combos."""
+    items = batch.boundary_items()
+    n = len(items["spot"])
+    v = rng.normal(0.0, 1.0, (n, 2, 1326)).astype(np.float32)
+    v *= (scale * batch.starting_pots[items["spot"]])[:, None, None]
+    for k in range(n):
+        v[k, :, _board_blocked(items["boards"][k])] = 0.0
+    return v
+
+
 def card_config(ranges, board):
     turn = board[3] if len(board) > 3 else ps.NOT_DEALT
     river = board[4] if len(board) > 4 else ps.NOT_DEALT

@@ -2,8 +2,8 @@
 
 Boundary reach: the oracle records the opponent's reach at every boundary it
 evaluates; after its average-strategy passes (root_cfvalues) from the same
-strategy sums it must match ps_boundary_reach.  River reduction: an f64 numpy
-restatement of cfvnet/src/datagen/gpu_boundary_eval.rs:207-269 on random
+strategy sums it must match ps_boundary_reach.  River reduction: the oracle's f64
+numpy restatement of cfvnet/src/datagen/gpu_boundary_eval.rs:207-269 on random
 inputs; the device sums the per-river weights in another order, so values
 agree to f32 rounding (tolerance 1e-6 relative).
 """
@@ -14,6 +14,7 @@ import torch
 
 import poker_solver_rust_b200 as ps
 from poker_solver_rust_b200.datagen import boundary_reach, boundary_river_reduce
+from oracle import boundary_io as bio
 from tests import spots
 from tests.test_gpu_adjoint import _copy_strategy, _sparse
 
@@ -44,37 +45,6 @@ def test_boundary_reach_matches_oracle():
             assert np.abs(got[k][p] - ref).max() <= 1e-6 * max(1.0, np.abs(ref).max())
 
 
-def _cards(idx):
-    return ps.index_to_card_pair(int(idx))
-
-
-def _reference_reduce(boards, pots, stacks, net, reach, hands):
-    n = boards.shape[0]
-    out = np.zeros((n, 2, len(hands)))
-    for i in range(n):
-        rivers = [c for c in range(52) if c not in set(boards[i])]
-        denorm = float(np.float32(pots[i]) + np.float32(stacks[i]))
-        for p in range(2):
-            opp = reach[i, 1 - p].astype(np.float64)
-            w = []
-            for rv in rivers:
-                z = opp.copy()
-                for c in range(1326):
-                    if rv in _cards(c):
-                        z[c] = 0.0
-                w.append(z.sum())
-            for hi, combo in enumerate(hands):
-                c0, c1 = _cards(combo)
-                num = den = 0.0
-                for ri, rv in enumerate(rivers):
-                    if rv in (c0, c1):
-                        continue
-                    num += w[ri] * float(net[i, p, ri, combo])
-                    den += w[ri]
-                out[i, p, hi] = num / den * denorm if den > 0 else 0.0
-    return out.astype(np.float32)
-
-
 def test_boundary_river_reduce_matches_reference():
     rng = np.random.default_rng(11)
     n = 3
@@ -82,13 +52,14 @@ def test_boundary_river_reduce_matches_reference():
     pots = rng.uniform(20, 200, n).astype(np.float32).round()
     stacks = rng.uniform(20, 400, n).astype(np.float32).round()
     reach = rng.random((n, 2, 1326)).astype(np.float32)
+    pairs = bio.combo_pairs()
     for i in range(n):  # no reach on combos blocked by the board
         for c in range(1326):
-            if set(_cards(c)) & set(boards[i].tolist()):
+            if set(pairs[c].tolist()) & set(boards[i].tolist()):
                 reach[i, :, c] = 0.0
     net = rng.normal(0, 0.1, (n, 2, 48, 1326)).astype(np.float32)
     hands = rng.choice(1326, 200, replace=False).astype(np.int32)
-    ref = _reference_reduce(boards, pots, stacks, net, reach, hands)
+    ref = bio.river_reduce(boards, pots, stacks, net, reach, hands)
     got = boundary_river_reduce(boards, pots, stacks, torch.from_numpy(net).cuda(), torch.from_numpy(reach).cuda(),
                                 torch.from_numpy(hands).cuda()).cpu().numpy()
     assert np.abs(got - ref).max() <= 1e-6 * max(1.0, np.abs(ref).max())

@@ -262,3 +262,32 @@ def test_oracle_early_termination():
     g = spots.oracle_game(r, board, tc)
     e = g.solve(1000, 1e10)
     assert e >= 0.0 and g.iterations_run == 0
+
+
+def test_boundary_io_known_answers():
+    """The boundary-network I/O restatement against the reference's own unit
+    tests: gpu_boundary_eval.rs:296-337 (zero_conflicting_hands) and
+    boundary_evaluator.rs:664-678 (encode_boundary_input_from_ranges), plus the
+    reduction's defining property: a network that outputs the same value for
+    every row averages to that value times pot + stack."""
+    from oracle import boundary_io as bio
+
+    r = bio.zero_conflicting_hands(np.ones(1326, np.float32), 10)
+    assert int((r == 0).sum()) == 51
+    for c1 in range(52):
+        for c2 in range(c1 + 1, 52):
+            assert r[bio.card_pair_to_index(c1, c2)] == (0.0 if 10 in (c1, c2) else 1.0)
+    r = bio.zero_conflicting_hands(np.full(1326, 0.5, np.float32), 0)
+    assert r[bio.card_pair_to_index(1, 2)] == 0.5 and r[bio.card_pair_to_index(0, 1)] == 0.0
+    row = bio.encode_row(np.full(1326, 0.5, np.float32), np.full(1326, 0.5, np.float32), [0, 4, 8, 12, 16],
+                         100.0, 150.0, 0)
+    assert row.shape == (2720,) and bio.POT_INDEX == 2717
+    assert abs(row[bio.POT_INDEX] - 0.4) < 1e-6 and abs(row[bio.POT_INDEX + 1] - 0.6) < 1e-6
+    assert row[2652:2704].sum() == 5 and row[2704:2717].sum() == 5  # five cards of five ranks
+    rng = np.random.default_rng(4)
+    boards = np.array([[48, 42, 33, 24]], np.uint8)
+    reach = rng.random((1, 2, 1326)).astype(np.float32)
+    net = np.full((1, 2, 48, 1326), 0.25, np.float32)
+    hands = np.arange(0, 1326, 97)
+    out = bio.river_reduce(boards, [100.0], [200.0], net, reach, hands)
+    assert np.allclose(out, 0.25 * 300.0, rtol=1e-6)
