@@ -166,6 +166,108 @@ def turn_game_measure(ps, spots, iters: int, cpu_iters: int):
     return out
 
 
+def turn_adjoint_measure(ps, spots, n: int, iters: int, cpu_sample: int):
+    """Depth-limited turn spots solved with seeded boundary values, then the
+    gradient of loss = MSE(root cfvalues, seeded target) with respect to the
+    boundary values through the batched adjoint (BatchSolvedValues): spots/s
+    forward + backward on the device, beside the oracle's forward (the same
+    iterations per spot, spot-parallel on the host cores) on a sample."""
+    import torch
+    from poker_solver_rust_b200.autograd import batch_solved_values
+
+    sp = spots.turn_boundary_spots(n, seed=11)
+    free0 = torch.cuda.mem_get_info()[0]
+    torch.cuda.reset_peak_memory_stats()
+    bs = ps.BatchSolver([spots.card_config(r, b) for r, b, _ in sp], [t for _, _, t in sp])
+    rng = np.random.default_rng(12)
+    V = spots.boundary_values(rng, bs)
+    B = torch.tensor(V, device="cuda", requires_grad=True)
+    target = torch.tensor(rng.normal(0, 1, (n, 2, 1326)).astype(np.float32), device="cuda") * \
+        torch.tensor(0.25 * bs.starting_pots, device="cuda")[:, None, None]
+    times = []
+    for rep in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        cfv = batch_solved_values(bs, B, iters)
+        loss = ((cfv - target) ** 2).mean()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        B.grad = None
+        loss.backward()
+        torch.cuda.synchronize()
+        times.append((t1 - t0, time.perf_counter() - t1))
+    fwd, bwd = min(times, key=lambda x: x[0] + x[1])
+    used = (free0 - torch.cuda.mem_get_info()[0]) / 1e9
+    out = {"workload": f"{n} depth-limited turn spots (bets 33%/75%/a, raise 60%, boundary at each non-fold turn "
+                       "terminal; Beta(0.5,0.5) ranges 30% zeroed, pot U[20,200], SPR U[0.5,10]), boundary values "
+                       f"~N(0,(pot/4)^2), {iters} DCFR iterations, loss = MSE(root cfvalues, seeded target), "
+                       "gradient w.r.t. the boundary values",
+           "boundary_items": bs.num_boundary_items(), "iterations": iters,
+           "spots_per_s_fwd_bwd": n / (fwd + bwd), "fwd_ms": fwd * 1e3, "bwd_ms": bwd * 1e3,
+           "device_gb": used, "note": "host-timed with device synchronisation; device_gb = device memory held "
+                                      "by the batch and the tensors at the end"}
+    if cpu_sample > 0:
+        threads = os.cpu_count() or 1
+        sample = sp[:max(cpu_sample, threads)]
+        items = bs.boundary_items()
+
+        def one(i):
+            r, b, t = sample[i]
+            o = spots.oracle_game(r, b, t)
+            ks = np.nonzero(items["spot"] == i)[0]
+            for j, k in enumerate(ks):
+                for p in range(2):
+                    cards = o.private_cards(p)
+                    o.set_boundary_cfvs(j, p, np.ascontiguousarray(
+                        V[k, p, [ps.card_pair_to_index(int(x), int(y)) for x, y in cards]]))
+            for it in range(iters):
+                o.solve_step(it)
+            o.root_cfvalues(0)
+            o.root_cfvalues(1)
+
+        from concurrent.futures import ThreadPoolExecutor
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(threads) as ex:
+            list(ex.map(one, range(len(sample))))
+        dt = time.perf_counter() - t0
+        out["cpu_forward"] = {"spots_per_s": len(sample) / dt, "cores": threads, "kind": "port",
+                              "sample": f"first {len(sample)} spots: boundary values, {iters} iterations, root "
+                                        "cfvalues (no gradient)"}
+    return out
+
+
+def turn_datagen_measure(ps, spots, n: int, iters: int, interval: int):
+    """The on-device turn-datagen loop (solve_with_boundary_net) on n
+    depth-limited turn spots with a stand-in boundary network (7 x 500 bf16
+    MLP, seeded random weights): spots/s for `iters` iterations with the
+    boundaries re-evaluated every `interval`."""
+    import torch
+    from poker_solver_rust_b200.datagen import solve_with_boundary_net
+
+    sp = spots.turn_boundary_spots(n, seed=21)
+    bs = ps.BatchSolver([spots.card_config(r, b) for r, b, _ in sp], [t for _, _, t in sp])
+    torch.manual_seed(0)
+    layers = [torch.nn.Linear(2720, 500), torch.nn.ReLU()]
+    for _ in range(6):
+        layers += [torch.nn.Linear(500, 500), torch.nn.ReLU()]
+    net = torch.nn.Sequential(*layers, torch.nn.Linear(500, 1326)).cuda().to(torch.bfloat16)
+    best = None
+    for rep in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        solve_with_boundary_net(bs, net, iters, interval, bf16=True)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    e, _ = bs.results()
+    return {"workload": f"{n} depth-limited turn spots, {iters} iterations, boundary network re-evaluated every "
+                        f"{interval} (7x500 bf16 MLP stand-in, 2720 -> 1326)",
+            "boundary_items": bs.num_boundary_items(), "spots_per_s": n / best, "seconds": best,
+            "mean_expl_pct_pot": float(np.mean(e / bs.starting_pots) * 100),
+            "note": "host-timed end to end on the device: input rows, network, 48-river average, boundary "
+                    "values, iterations"}
+
+
 def make_workload(n_spots: int, seed: int):
     from tests import spots
 
@@ -235,6 +337,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--turn-iters", type=int, default=500, help="single turn game iterations (0 = skip)")
     ap.add_argument("--turn-cpu-iters", type=int, default=1)
+    ap.add_argument("--adjoint-spots", type=int, default=1024, help="depth-limited turn spots + adjoint (0 = skip)")
+    ap.add_argument("--adjoint-iters", type=int, default=300)
+    ap.add_argument("--datagen-spots", type=int, default=512, help="turn-datagen loop spots (0 = skip)")
     ap.add_argument("--stage", type=int, default=-1)
     ap.add_argument("--bufs", type=int, default=0, help="terminal scan buffers per CTA (0 = half the warps)")
     ap.add_argument("--inst", type=int, default=0, help="spots per CTA in lockstep (0 = library default)")
@@ -340,6 +445,13 @@ def main():
     if rank == 0 and args.turn_iters > 0:
         turn = turn_game_measure(ps, spots, args.turn_iters, args.turn_cpu_iters)
 
+    # ---- depth-limited turn spots: solve + adjoint, and the datagen loop ----
+    adjoint = datagen = None
+    if rank == 0 and args.adjoint_spots > 0:
+        adjoint = turn_adjoint_measure(ps, spots, args.adjoint_spots, args.adjoint_iters, args.cpu_sample)
+    if rank == 0 and args.datagen_spots > 0:
+        datagen = turn_datagen_measure(ps, spots, args.datagen_spots, 100, 10)
+
     # ---- CPU baseline (oracle) on a bounded sample ----
     cpu = None
     if rank == 0 and args.cpu_sample > 0:
@@ -373,6 +485,8 @@ def main():
             "cpu_baseline": cpu,
             "plain_gpu": plain,
             "turn_game": turn,
+            "turn_adjoint": adjoint,
+            "turn_datagen": datagen,
             "clocks": clocks,
             "detail": {"setup_ms": statistics.median(setup_ms), "solve_ms": statistics.median(solve_ms),
                        "mean_iterations": float(iters.mean()), "max_iterations": int(iters.max()),
