@@ -269,6 +269,16 @@ int ps_batch_root_cfvalues_all(ps_batch* b, float* out, int32_t on_device);
  * [items][2][1326]: dL/d(boundary values).  dw or dB may be null.  Spots with
  * isomorphic chance pruning: PS_ERR_UNSUPPORTED. */
 int ps_batch_adjoint(ps_batch* b, const float* cot, float* dw, float* dB, int32_t on_device);
+/* training records of every spot (cfvnet datagen/storage.rs:5-57 format, two
+ * per spot: player 0 then 1) from the root cfvalues of the last ps_batch_solve
+ * or PS_EPI_ROOT epilogue, with the values of the GPU river datagen
+ * (datagen/domain/pipeline.rs:353-411): cfvs = (root cfvalue * num_combinations
+ * - pot/2) / (pot/2) on the player's hands, valid_mask = either player's hands,
+ * game_value = sum(range * cfvs) in f32; replaces compute_evs_from_strategy_sum
+ * + the record assembly.  All spots need the same board size.
+ * ps_batch_record_bytes: the size of the packed records. */
+int64_t ps_batch_record_bytes(ps_batch* b);
+int ps_batch_records(ps_batch* b, uint8_t* out, int32_t on_device);
 /* boundary-network input rows (cfvnet eval/boundary_evaluator.rs:27-60, rows
  * ordered as gpu_boundary_eval.rs:164-185): for each of n items, player and
  * river card not on the board, 2720 values: oop reach | ip reach (zeroed where

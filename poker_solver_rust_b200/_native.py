@@ -138,6 +138,8 @@ _sig("ps_batch_set_boundary_cfvs", i32, vp, vp, i32)
 _sig("ps_batch_boundary_reach", i32, vp, vp, i32)
 _sig("ps_batch_root_cfvalues_all", i32, vp, vp, i32)
 _sig("ps_batch_adjoint", i32, vp, vp, vp, vp, i32)
+_sig("ps_batch_record_bytes", i64, vp)
+_sig("ps_batch_records", i32, vp, vp, i32)
 _sig("ps_boundary_encode", i32, i32, P(C.c_uint8), P(f32), P(f32), vp, vp, i32, vp)
 
 PS_EPI_ROOT = 1

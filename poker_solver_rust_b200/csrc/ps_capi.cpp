@@ -164,6 +164,7 @@ struct Batch {
   int2* d_items = nullptr;
   bool ready = false;  // state zeroed and board tables built since the last reset
   char* adj_pool = nullptr;  // per-spot adjoint vectors (cotangents, weight and boundary gradients)
+  char* rec_pool = nullptr;  // input ranges [n][2][1326] and RecordMeta [n] for the record writer
   size_t adj_bgrad_off = 0, adj_bytes = 0;
   float* d_scratch = nullptr;
   size_t scratch_floats = 0;
@@ -207,6 +208,7 @@ struct Batch {
     cudaFree(d_work);
     cudaFree(d_items);
     cudaFree(adj_pool);
+    cudaFree(rec_pool);
     cudaFree(d_scratch);
     cudaFree(d_disc);
     cudaFree(d_target);
@@ -719,6 +721,51 @@ struct Batch {
     CU(cudaEventElapsedTime(&last_solve_ms, ev[2], ev[3]));
     CU(cudaEventElapsedTime(&last_setup_ms, ev[1], ev[2]));
     return check_err();
+  }
+
+  // Board size shared by every spot (records of one file share it), or -1.
+  int board_size() const {
+    int bs = -1;
+    for (auto& gp : games) {
+      const int k = gp->turn == NOT_DEALT ? 3 : gp->river == NOT_DEALT ? 4 : 5;
+      if (bs >= 0 && k != bs) return -1;
+      bs = k;
+    }
+    return bs;
+  }
+
+  size_t record_bytes() const {
+    const int bs = board_size();
+    return bs < 0 ? 0 : games.size() * 2 * (size_t)(1 + bs + 13 + 13 * 1326);
+  }
+
+  // Packs the training records of every spot into `out` (device memory).
+  int records(uint8_t* out) {
+    const int n = (int)games.size();
+    if (board_size() < 0) return fail(PS_ERR_INVALID, "records of one batch need one board size");
+    const size_t rb = align256((size_t)n * 2 * 1326 * 4);
+    if (!rec_pool) {
+      std::vector<float> r((size_t)n * 2 * 1326);
+      std::vector<RecordMeta> m(n);
+      for (int i = 0; i < n; ++i) {
+        const Game& g = *games[i];
+        std::memcpy(&r[(size_t)i * 2 * 1326], g.range[0], 4 * 1326);
+        std::memcpy(&r[(size_t)i * 2 * 1326 + 1326], g.range[1], 4 * 1326);
+        RecordMeta& x = m[i];
+        std::memset(&x, 0, sizeof(x));
+        x.pot = (float)g.cfg.starting_pot;
+        x.stack = (float)g.cfg.effective_stack;
+        const uint8_t bd[5] = {g.flop[0], g.flop[1], g.flop[2], g.turn, g.river};
+        x.board_size = (uint8_t)(g.turn == NOT_DEALT ? 3 : g.river == NOT_DEALT ? 4 : 5);
+        std::memcpy(x.board, bd, x.board_size);
+      }
+      CU(cudaMalloc(&rec_pool, rb + sizeof(RecordMeta) * n));
+      CU(cudaMemcpyAsync(rec_pool, r.data(), 4 * r.size(), cudaMemcpyHostToDevice, stream));
+      CU(cudaMemcpyAsync(rec_pool + rb, m.data(), sizeof(RecordMeta) * n, cudaMemcpyHostToDevice, stream));
+    }
+    CU(launch_pack_records(d_spots, n, (const float*)rec_pool, (const RecordMeta*)(rec_pool + rb), out, stream));
+    CU(cudaStreamSynchronize(stream));
+    return PS_OK;
   }
 
   // Allocates the per-spot adjoint vectors on first use: cotangents and
@@ -1918,6 +1965,30 @@ int ps_batch_adjoint(ps_batch* pb, const float* cot, float* dw, float* dB, int32
     if (dB && ni) CU(cudaMemcpyAsync(dB, d_dB, ib, cudaMemcpyDeviceToHost, B.stream));
   }
   CU(cudaStreamSynchronize(B.stream));
+  return PS_OK;
+}
+
+int64_t ps_batch_record_bytes(ps_batch* pb) {
+  if (!pb) return fail(PS_ERR_INVALID, "null batch");
+  if (pb->b->board_size() < 0) return fail(PS_ERR_INVALID, "records of one batch need one board size");
+  return (int64_t)pb->b->record_bytes();
+}
+
+int ps_batch_records(ps_batch* pb, uint8_t* out, int32_t on_device) {
+  if (!pb || !out) return fail(PS_ERR_INVALID, "bad argument");
+  Batch& B = *pb->b;
+  const size_t bytes = B.record_bytes();
+  if (bytes == 0) return fail(PS_ERR_INVALID, "records of one batch need one board size");
+  uint8_t* dst = out;
+  uint8_t* tmp = nullptr;
+  if (!on_device) {
+    CU(cudaMalloc(&tmp, bytes));
+    dst = tmp;
+  }
+  std::unique_ptr<uint8_t, decltype(&cudaFree)> keep(tmp, &cudaFree);
+  int rc = B.records(dst);
+  if (rc) return rc;
+  if (!on_device) CU(cudaMemcpy(out, tmp, bytes, cudaMemcpyDeviceToHost));
   return PS_OK;
 }
 

@@ -241,6 +241,76 @@ cudaError_t launch_boundary_encode(int n, const uint8_t* boards, const float* po
   return cudaGetLastError();
 }
 
+// Training records (cfvnet datagen/storage.rs:5-57), one block per (spot,
+// player), packed byte by byte (the format is unaligned):
+//   [board_size u8][board][pot f32][stack f32][player u8][game_value f32]
+//   [oop_range f32 x1326][ip_range f32 x1326][cfvs f32 x1326][valid_mask u8 x1326]
+// with the values of the GPU river datagen (datagen/domain/pipeline.rs:353-411):
+// cfvs[c] = (f64(f32(rootcfv[h] * num_combinations)) - pot/2) / (pot/2) for the
+// hands of the player's list, 0 elsewhere; valid_mask marks the hands of
+// either player's list (one mask for both records);
+// game_value = sum over combos of range * cfv, in f32, in combo order.
+__device__ __forceinline__ void put_bytes(uint8_t* dst, const void* src, int n) {
+  const uint8_t* s = static_cast<const uint8_t*>(src);
+  for (int i = 0; i < n; ++i) dst[i] = s[i];
+}
+
+__global__ void k_pack_records(const SpotDev* __restrict__ spots, const float* __restrict__ ranges,
+                               const RecordMeta* __restrict__ meta, uint8_t* __restrict__ out) {
+  const int spot = blockIdx.x >> 1, player = blockIdx.x & 1;
+  const SpotDev& sp = spots[spot];
+  const RecordMeta m = meta[spot];
+  const int bs = m.board_size;
+  const size_t rsize = 1 + bs + 4 + 4 + 1 + 4 + 3 * 4 * kCombos + kCombos;
+  uint8_t* rec = out + (size_t)blockIdx.x * rsize;
+  __shared__ float s_cfv[kCombos];
+  __shared__ uint8_t s_valid[kCombos];
+  for (int c = threadIdx.x; c < kCombos; c += blockDim.x) {
+    s_cfv[c] = 0.f;
+    s_valid[c] = 0;
+  }
+  __syncthreads();
+  const double half = 0.5 * (double)m.pot;
+  const double norm = half > 0.0 ? half : 1.0;
+  const float comb = (float)sp.num_combinations;
+  const uint8_t* cards = sp.cards[player];
+  for (int h = threadIdx.x; h < sp.H[player]; h += blockDim.x) {
+    const int c = combo_index(cards[2 * h], cards[2 * h + 1]);
+    const float ev = __fmul_rn(sp.root_out[player][h], comb);
+    s_cfv[c] = (float)(((double)ev - half) / norm);
+  }
+  // one mask for both records: the hands of either player (pipeline.rs:366-377)
+  for (int q = 0; q < 2; ++q)
+    for (int h = threadIdx.x; h < sp.H[q]; h += blockDim.x)
+      s_valid[combo_index(sp.cards[q][2 * h], sp.cards[q][2 * h + 1])] = 1;
+  __syncthreads();
+  const float* rg = ranges + (size_t)spot * 2 * kCombos;
+  uint8_t* body = rec + 1 + bs + 13;
+  for (int i = threadIdx.x; i < 3 * kCombos; i += blockDim.x) {
+    const float v = i < 2 * kCombos ? rg[i] : s_cfv[i - 2 * kCombos];
+    put_bytes(body + 4 * i, &v, 4);
+  }
+  for (int c = threadIdx.x; c < kCombos; c += blockDim.x) body[12 * kCombos + c] = s_valid[c];
+  if (threadIdx.x == 0) {
+    const float* own = rg + (size_t)player * kCombos;
+    float gv = 0.f;
+    for (int c = 0; c < kCombos; ++c) gv = __fadd_rn(gv, __fmul_rn(own[c], s_cfv[c]));
+    rec[0] = (uint8_t)bs;
+    for (int k = 0; k < bs; ++k) rec[1 + k] = m.board[k];
+    put_bytes(rec + 1 + bs, &m.pot, 4);
+    put_bytes(rec + 5 + bs, &m.stack, 4);
+    rec[9 + bs] = (uint8_t)player;
+    put_bytes(rec + 10 + bs, &gv, 4);
+  }
+}
+
+cudaError_t launch_pack_records(const SpotDev* spots, int n, const float* ranges, const RecordMeta* meta,
+                                uint8_t* out, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_pack_records<<<2 * n, 256, 0, s>>>(spots, ranges, meta, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_boundary_river_reduce(int n, const uint8_t* boards, const float* denorm, const float* net,
                                          const float* reach, const int32_t* hands, int H, float* out,
                                          cudaStream_t s) {

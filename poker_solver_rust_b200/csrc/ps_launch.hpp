@@ -80,6 +80,18 @@ cudaError_t launch_spot_combo(const SpotDev* spots, int n, int which, const floa
 constexpr int kBoundaryInput = 2720;
 cudaError_t launch_boundary_encode(int n, const uint8_t* boards, const float* pots, const float* stacks,
                                    const float* reach, void* out, int bf16, cudaStream_t s);
+// Per-spot fields of a training record that the device descriptor lacks.
+struct RecordMeta {
+  float pot, stack;   // starting pot and effective stack
+  uint8_t board[5];
+  uint8_t board_size; // 3, 4 or 5
+  uint8_t pad[2];
+};
+// Packed training records (cfvnet datagen/storage.rs) of every spot from its
+// root cfvalues (sp.root_out): 2n records, spot by spot, player 0 then 1.
+// ranges [n][2][1326] are the spots' input ranges; all device pointers.
+cudaError_t launch_pack_records(const SpotDev* spots, int n, const float* ranges, const RecordMeta* meta,
+                                uint8_t* out, cudaStream_t s);
 cudaError_t launch_grid(const SpotDev* spot, const GridJob& job, const Discount* disc, float* scratch,
                         size_t scratch_floats, float* out_expl, int* out_iters, unsigned* bar, double* gred,
                         int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s);

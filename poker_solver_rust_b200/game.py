@@ -666,6 +666,17 @@ class BatchSolver:
                                          C.c_void_p(dB.ctypes.data), 0))
         return dw, dB
 
+    def records(self) -> np.ndarray:
+        """Training records of every spot, packed on the device in the
+        reference's binary format (poker_solver_rust_b200.records): two per
+        spot, player 0 then 1, from the root cfvalues of the last solve."""
+        from . import records as R
+
+        nbytes = N.check(N.lib().ps_batch_record_bytes(self._h))
+        out = np.zeros(nbytes, np.uint8)
+        N.check(N.lib().ps_batch_records(self._h, C.c_void_p(out.ctypes.data), 0))
+        return out.view(R.record_dtype(int(out[0])))
+
     def boundary_reach(self, device: bool = False):
         """Each player's reach at every boundary under the average strategy as
         of the last root epilogue, [items, 2, 1326] (numpy, or a CUDA tensor

@@ -291,3 +291,36 @@ def test_boundary_io_known_answers():
     hands = np.arange(0, 1326, 97)
     out = bio.river_reduce(boards, [100.0], [200.0], net, reach, hands)
     assert np.allclose(out, 0.25 * 300.0, rtol=1e-6)
+
+
+def test_record_format_pins(tmp_path):
+    """The record layout against the reference's storage tests
+    (storage.rs:151-230: sizes, round trips, 4-card boards) and the writer's
+    per-file rotation (writer.rs:30-83)."""
+    from poker_solver_rust_b200 import records as R
+
+    assert R.record_size(5) == 1 + 5 + 4 + 4 + 1 + 4 + 1326 * 4 * 3 + 1326 == 17257
+    for bs in (3, 4, 5):
+        assert R.record_dtype(bs).itemsize == R.record_size(bs)
+    rng = np.random.default_rng(0)
+    recs = np.zeros(5, R.record_dtype(4))
+    recs["board_size"] = 4
+    recs["board"] = [0, 4, 8, 12]
+    recs["pot"] = rng.uniform(10, 200, 5).astype(np.float32)
+    recs["player"] = [0, 1, 0, 1, 0]
+    recs["game_value"] = -0.1
+    recs["cfvs"] = rng.normal(0, 1, (5, 1326)).astype(np.float32)
+    recs["valid_mask"] = rng.random((5, 1326)) < 0.5
+    path = str(tmp_path / "data.bin")
+    with R.RecordWriter(path, per_file=2) as w:
+        w.write(recs[:3])
+        w.write(recs[3:])
+        assert w.count() == 5
+    names = sorted(p.name for p in tmp_path.iterdir())
+    assert names == ["data.bin", "data_00001.bin", "data_00002.bin"]
+    back = np.concatenate([R.read_records(str(tmp_path / n), 4) for n in names])
+    assert back.tobytes() == recs.tobytes()
+    raw = open(path, "rb").read()
+    assert raw[0] == 4 and list(raw[1:5]) == [0, 4, 8, 12]
+    assert np.frombuffer(raw[5:9], "<f4")[0] == recs["pot"][0]
+    assert len(raw) == 2 * R.record_size(4)
