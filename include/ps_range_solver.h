@@ -279,6 +279,27 @@ int ps_batch_adjoint(ps_batch* b, const float* cot, float* dw, float* dB, int32_
  * ps_batch_record_bytes: the size of the packed records. */
 int64_t ps_batch_record_bytes(ps_batch* b);
 int ps_batch_records(ps_batch* b, uint8_t* out, int32_t on_device);
+/* ---- situation sampling (cfvnet datagen/sampler.rs:30-60, :142-205 and
+ *      range_gen.rs:18-167) ---- */
+typedef struct ps_sampler_config {
+  int32_t board_size;          /* 4 (turn) or 5 (river) */
+  int32_t initial_stack;       /* chips (config.rs:72, default 200) */
+  int32_t num_pot_intervals;   /* 1..16 */
+  const int32_t* pot_intervals; /* [k][2], [lo, hi) (config.rs:151, default [[4,20],[20,80],[80,200],[200,400]]) */
+  int32_t num_spr_intervals;   /* 0..16; 0 = pot, then stack uniform in [5, initial_stack - pot/2] */
+  const double* spr_intervals; /* [k][2], [lo, hi): SPR bucket first, then a feasible pot bucket */
+  uint64_t seed;
+} ps_sampler_config;
+/* situations first .. first + n - 1 of the seed's stream, on the device: a
+ * board of board_size distinct cards (boards [n][5], unused slots 0), pot and
+ * effective stack (pots, stacks [n]), and the OOP and IP ranges [n][2][1326]
+ * drawn by the R(S,p) procedure over the combos ordered by hand strength (each
+ * sums to 1, board-blocked combos 0).  The draws come from a counter-based
+ * SplitMix64 stream instead of the reference's ChaCha8: same distributions,
+ * different numbers.  Output pointers are device memory; stream: a
+ * cudaStream_t or null. */
+int ps_sample_situations(const ps_sampler_config* cfg, int64_t first, int32_t n, uint8_t* boards, int32_t* pots,
+                         int32_t* stacks, float* ranges, void* stream);
 /* boundary-network input rows (cfvnet eval/boundary_evaluator.rs:27-60, rows
  * ordered as gpu_boundary_eval.rs:164-185): for each of n items, player and
  * river card not on the board, 2720 values: oop reach | ip reach (zeroed where

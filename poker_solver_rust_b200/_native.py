@@ -37,6 +37,12 @@ class PsTreeConfig(C.Structure):
     ]
 
 
+class PsSamplerConfig(C.Structure):
+    _fields_ = [("board_size", C.c_int32), ("initial_stack", C.c_int32), ("num_pot_intervals", C.c_int32),
+                ("pot_intervals", C.POINTER(C.c_int32)), ("num_spr_intervals", C.c_int32),
+                ("spr_intervals", C.POINTER(C.c_double)), ("seed", C.c_uint64)]
+
+
 class PsCardConfig(C.Structure):
     _fields_ = [
         ("range", C.POINTER(C.c_float) * 2),
@@ -138,6 +144,7 @@ _sig("ps_batch_set_boundary_cfvs", i32, vp, vp, i32)
 _sig("ps_batch_boundary_reach", i32, vp, vp, i32)
 _sig("ps_batch_root_cfvalues_all", i32, vp, vp, i32)
 _sig("ps_batch_adjoint", i32, vp, vp, vp, vp, i32)
+_sig("ps_sample_situations", i32, P(PsSamplerConfig), i64, i32, vp, vp, vp, vp, vp)
 _sig("ps_batch_record_bytes", i64, vp)
 _sig("ps_batch_records", i32, vp, vp, i32)
 _sig("ps_boundary_encode", i32, i32, P(C.c_uint8), P(f32), P(f32), vp, vp, i32, vp)

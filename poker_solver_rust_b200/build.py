@@ -17,7 +17,7 @@ OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libps_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["ps_kernels.cu", "ps_datagen.cu", "ps_host.cpp", "ps_capi.cpp"]
+SOURCES = ["ps_kernels.cu", "ps_datagen.cu", "ps_sampler.cu", "ps_host.cpp", "ps_capi.cpp"]
 HEADERS = ["ps_device.hpp", "ps_handeval.hpp", "ps_host.hpp", "ps_launch.hpp"]
 
 

@@ -1992,6 +1992,50 @@ int ps_batch_records(ps_batch* pb, uint8_t* out, int32_t on_device) {
   return PS_OK;
 }
 
+int ps_sample_situations(const ps_sampler_config* cfg, int64_t first, int32_t n, uint8_t* boards, int32_t* pots,
+                         int32_t* stacks, float* ranges, void* stream) {
+  if (!cfg || n < 0 || first < 0 || (n > 0 && (!boards || !pots || !stacks || !ranges)))
+    return fail(PS_ERR_INVALID, "bad argument");
+  if (cfg->board_size != 4 && cfg->board_size != 5) return fail(PS_ERR_INVALID, "board_size must be 4 or 5");
+  if (cfg->num_pot_intervals < 1 || cfg->num_pot_intervals > kMaxSamplerIntervals || !cfg->pot_intervals ||
+      cfg->num_spr_intervals < 0 || cfg->num_spr_intervals > kMaxSamplerIntervals ||
+      (cfg->num_spr_intervals > 0 && !cfg->spr_intervals))
+    return fail(PS_ERR_INVALID, "1 to 16 pot intervals and 0 to 16 SPR intervals");
+  if (cfg->initial_stack <= 0) return fail(PS_ERR_INVALID, "initial_stack must be > 0");
+  SamplerParams P{};
+  P.board_size = cfg->board_size;
+  P.initial_stack = cfg->initial_stack;
+  P.npot = cfg->num_pot_intervals;
+  P.nspr = cfg->num_spr_intervals;
+  for (int k = 0; k < P.npot; ++k) {
+    P.pot[k][0] = cfg->pot_intervals[2 * k];
+    P.pot[k][1] = cfg->pot_intervals[2 * k + 1];
+    if (P.pot[k][0] < 1 || P.pot[k][1] <= P.pot[k][0]) return fail(PS_ERR_INVALID, "pot intervals need 1 <= lo < hi");
+  }
+  for (int k = 0; k < P.nspr; ++k) {
+    P.spr[k][0] = cfg->spr_intervals[2 * k];
+    P.spr[k][1] = cfg->spr_intervals[2 * k + 1];
+    if (!(P.spr[k][0] >= 0.0) || !(P.spr[k][1] > P.spr[k][0]) || P.spr[k][1] > 1e6)
+      return fail(PS_ERR_INVALID, "SPR intervals need 0 <= lo < hi");
+  }
+  P.seed = cfg->seed;
+  P.first = first;
+  if (n == 0) return PS_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  int* d_err = nullptr;
+  CU(cudaMalloc(&d_err, sizeof(int)));
+  std::unique_ptr<int, decltype(&cudaFree)> keep(d_err, &cudaFree);
+  CU(cudaMemsetAsync(d_err, 0, sizeof(int), s));
+  CU(launch_sample_situations(P, n, boards, pots, stacks, ranges, d_err, s));
+  int e = 0;
+  CU(cudaMemcpyAsync(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  if (e)
+    return fail(PS_ERR_INVALID, "a situation could not be drawn: pot and SPR intervals infeasible for the initial "
+                                "stack (10000 attempts, as the reference)");
+  return PS_OK;
+}
+
 int ps_boundary_encode(int32_t n, const uint8_t* boards, const float* pots, const float* stacks, const float* reach,
                        void* out, int32_t out_bf16, void* stream) {
   if (n < 0 || (n > 0 && (!boards || !pots || !stacks || !reach || !out)))

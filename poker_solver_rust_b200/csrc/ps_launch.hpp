@@ -92,6 +92,22 @@ struct RecordMeta {
 // ranges [n][2][1326] are the spots' input ranges; all device pointers.
 cudaError_t launch_pack_records(const SpotDev* spots, int n, const float* ranges, const RecordMeta* meta,
                                 uint8_t* out, cudaStream_t s);
+// Situation sampler (ps_sampler.cu): the datagen configuration of
+// cfvnet config.rs:150-160 (pot intervals [lo, hi), optional SPR intervals,
+// initial stack) for situations first .. first + n - 1 of the seed's stream.
+constexpr int kMaxSamplerIntervals = 16;
+struct SamplerParams {
+  int board_size, initial_stack, npot, nspr;
+  int pot[kMaxSamplerIntervals][2];
+  double spr[kMaxSamplerIntervals][2];
+  uint64_t seed;
+  int64_t first;
+};
+// boards [n][5] (unused slots 0), pots [n], stacks [n], ranges [n][2][1326]
+// (OOP, IP); err is set to 1 when a situation cannot be drawn (the SPR
+// rejection exhausted); all device pointers.
+cudaError_t launch_sample_situations(const SamplerParams& P, int n, uint8_t* boards, int32_t* pots, int32_t* stacks,
+                                     float* ranges, int* err, cudaStream_t s);
 cudaError_t launch_grid(const SpotDev* spot, const GridJob& job, const Discount* disc, float* scratch,
                         size_t scratch_floats, float* out_expl, int* out_iters, unsigned* bar, double* gred,
                         int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s);

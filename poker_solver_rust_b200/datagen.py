@@ -105,8 +105,12 @@ def evaluate_boundaries(items: dict, reach, net, pot_source: str = "boundary", d
         z = slice(a, min(n, a + chunk_items))
         m = z.stop - z.start
         rows = boundary_encode(items["boards"][z], pots[z], stacks[z], reach[z], bf16=bf16)
+        x = rows.view(m * 96, 2720)
+        p = next(net.parameters(), None) if hasattr(net, "parameters") else None
+        if p is not None and p.dtype != x.dtype:
+            x = x.to(p.dtype)
         with torch.no_grad():
-            y = net(rows.view(m * 96, 2720)).float().view(m, 2, 48, 1326)
+            y = net(x).float().view(m, 2, 48, 1326)
         if denormalize:
             dp, ds = pots[z], stacks[z]
         else:

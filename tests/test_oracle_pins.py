@@ -324,3 +324,61 @@ def test_record_format_pins(tmp_path):
     assert raw[0] == 4 and list(raw[1:5]) == [0, 4, 8, 12]
     assert np.frombuffer(raw[5:9], "<f4")[0] == recs["pot"][0]
     assert len(raw) == 2 * R.record_size(4)
+
+
+def test_sampler_restatement_pins():
+    """The situation sampler's restatement against the reference's own tests:
+    the 7-card value encoding orders hands as range-solver's evaluator does
+    and gives the codes range_gen.rs:184-268 defines; R(S,p) ranges sum to 1,
+    are non-negative, zero on the board and heavier on strong hands
+    (range_gen.rs:330-438); boards, pots, stacks and SPR buckets keep their
+    bounds (sampler.rs:240-420)."""
+    from oracle import sampler as S
+
+    def c(r, s):
+        return 4 * r + s
+
+    assert S.eval7([c(12, 0), c(0, 1), c(1, 2), c(2, 3), c(3, 0), c(8, 1), c(9, 2)]) == (4 << 26) | (1 << 3)
+    assert S.eval7([c(12, 0), c(11, 0), c(10, 0), c(9, 0), c(8, 0), c(0, 1), c(1, 2)]) == (8 << 26) | (1 << 12)
+    rng = np.random.default_rng(5)
+    for _ in range(1500):
+        cards = rng.choice(52, 9, replace=False)
+        a = [int(x) for x in cards[:7]]
+        b = [int(x) for x in cards[2:9]]
+        ea, eb = S.eval7(a), S.eval7(b)
+        oa, ob = O.hand_evaluate(a), O.hand_evaluate(b)
+        assert np.sign(ea - eb) == np.sign(oa - ob), (a, b)
+    board = [c(10, 3), c(9, 2), c(0, 0), c(6, 1), c(1, 3)]  # Qs Jh 2c 8d 3s
+    vals = S.hand_values(board)
+    blocked = np.array([bool(set(p) & set(board)) for p in S.PAIRS])
+    assert (vals[blocked] == 0).all() and (vals[~blocked] > 0).all()
+    order = sorted(np.nonzero(~blocked)[0], key=lambda i: (vals[i], i))
+    top, bottom = order[len(order) * 3 // 4:], order[:len(order) // 4]
+    ts = bs = 0.0
+    for seed in range(60):
+        r = S.rsp_range(vals, S.mix64(seed), 0)
+        assert abs(float(r.sum()) - 1.0) < 1e-5 and (r >= 0).all() and not r[blocked].any()
+        ts += float(r[top].sum())
+        bs += float(r[bottom].sum())
+    assert ts > bs
+    assert np.array_equal(S.rsp_range(vals, 77, 1), S.rsp_range(vals, 77, 1))
+    v4 = S.hand_values(board[:4])
+    r4 = S.rsp_range(v4, 123, 0)
+    assert abs(float(r4.sum()) - 1.0) < 1e-5
+    pots = [[4, 20], [20, 80], [80, 200], [200, 400]]
+    for i in range(800):
+        b, pot, stack, _ = S.sample_board_pot(5, 200, pots, None, 42, i)
+        assert len(set(b)) == 5 and max(b) < 52
+        assert any(lo <= pot < hi for lo, hi in pots)
+        max_stack = 200 - pot // 2
+        assert stack == 5 if max_stack < 5 else 5 <= stack <= max_stack
+    sprs = [[0.0, 1.0], [1.0, 3.0], [3.0, 8.0]]
+    seen = set()
+    for i in range(600):
+        got = S.sample_board_pot(4, 400, [[4, 40], [40, 120], [120, 400]], sprs, 7, i)
+        assert got is not None
+        _, pot, stack, _ = got
+        k = [j for j, (lo, hi) in enumerate(sprs) if lo <= stack / pot < hi]
+        assert len(k) == 1 and stack >= 5
+        seen.add(k[0])
+    assert seen == {0, 1, 2}
