@@ -205,6 +205,14 @@ void ps_batch_free(ps_batch* b);
 int ps_batch_solve(ps_batch* b, uint32_t max_iter, const float* target_chips);
 int ps_batch_results(ps_batch* b, float* exploitability, int32_t* iterations);
 int ps_batch_root_strategy(ps_batch* b, int32_t spot, float* out); /* returns count */
+/* per-spot state after a solve (replaces extract_results, batch.rs:587-609,
+ * which downloads the strategy sums): nodes in the arena order of
+ * ps_num_nodes / ps_node_info for the same spot; ps_batch_node_storage gives a
+ * decision node's [A][H_actor] rows, which = 1 strategy sums, 2 regrets, as
+ * ps_node_storage does for a single game; returns the count (0 for terminal
+ * and chance nodes) */
+int64_t ps_batch_num_nodes(ps_batch* b, int32_t spot);
+int64_t ps_batch_node_storage(ps_batch* b, int32_t spot, int64_t node, int which, float* out);
 /* root cfvalues of `player` under the average strategy after the last
  * ps_batch_solve, computed on the device at the end of each spot's solve
  * (replaces compute_evs_from_strategy_sum, gpu-range-solver batch.rs:799-933);

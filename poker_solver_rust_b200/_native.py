@@ -130,6 +130,8 @@ _sig("ps_batch_solve", i32, vp, u32, P(f32))
 _sig("ps_batch_results", i32, vp, P(f32), P(i32))
 _sig("ps_batch_root_strategy", i32, vp, i32, P(f32))
 _sig("ps_batch_root_cfvalues", i32, vp, i32, i32, P(f32))
+_sig("ps_batch_num_nodes", i64, vp, i32)
+_sig("ps_batch_node_storage", i64, vp, i32, i64, i32, P(f32))
 _sig("ps_batch_last_timing", i32, vp, P(f32), P(f32))
 _sig("ps_batch_iteration_bytes", f64, vp, i32)
 _sig("ps_batch_config", i32, vp, P(i32), P(i32), P(i32))

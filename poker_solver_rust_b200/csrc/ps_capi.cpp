@@ -2094,6 +2094,28 @@ int ps_batch_root_strategy(ps_batch* pb, int32_t spot, float* out) {
   return na * H;
 }
 
+int64_t ps_batch_num_nodes(ps_batch* pb, int32_t spot) {
+  if (!pb || spot < 0 || spot >= (int)pb->b->games.size()) return fail(PS_ERR_INVALID, "bad spot");
+  return (int64_t)pb->b->games[spot]->arena.size();
+}
+
+int64_t ps_batch_node_storage(ps_batch* pb, int32_t spot, int64_t node, int which, float* out) {
+  if (!pb || !out || spot < 0 || spot >= (int)pb->b->games.size() || (which != 1 && which != 2))
+    return fail(PS_ERR_INVALID, "bad argument");
+  Batch& B = *pb->b;
+  const Game& g = *B.games[spot];
+  if (node < 0 || node >= (int64_t)g.arena.size()) return fail(PS_ERR_INVALID, "bad node index");
+  const ArenaNode& n = g.arena[node];
+  if (n.terminal() || n.chance()) return 0;
+  const int p = n.player, H = g.H[p], hs = g.hs[p];
+  const float* src = (which == 1 ? B.h_spots[spot].S : B.h_spots[spot].R) + n.rs_off;
+  std::vector<float> rows((size_t)n.nch * hs);
+  CU(cudaMemcpy(rows.data(), src, 4 * rows.size(), cudaMemcpyDeviceToHost));
+  for (int a = 0; a < n.nch; ++a)
+    std::copy(rows.begin() + (size_t)a * hs, rows.begin() + (size_t)a * hs + H, out + (size_t)a * H);
+  return (int64_t)n.nch * H;
+}
+
 int ps_batch_root_cfvalues(ps_batch* pb, int32_t spot, int player, float* out) {
   if (!pb || !out || spot < 0 || spot >= (int)pb->b->games.size() || (player != 0 && player != 1))
     return fail(PS_ERR_INVALID, "bad argument");

@@ -538,6 +538,16 @@ class BatchSolver:
         n = N.check(N.lib().ps_batch_root_strategy(self._h, spot, _fp(out)))
         return out[:n].copy()
 
+    def num_nodes(self, spot: int) -> int:
+        return int(N.check(N.lib().ps_batch_num_nodes(self._h, spot)))
+
+    def node_storage(self, spot: int, node: int, which: int) -> np.ndarray:
+        """[A * H_actor] rows of a decision node of one spot: which = 1
+        strategy sums, 2 regrets (PostFlopGame.node_storage for a batch)."""
+        out = _f32(16 * 1326)
+        n = N.check(N.lib().ps_batch_node_storage(self._h, spot, node, which, _fp(out)))
+        return out[:n].copy()
+
     def root_cfvalues(self, spot: int, player: int) -> np.ndarray:
         """Root cfvalues of `player` under the average strategy after the last
         solve (computed on the device at the end of the spot's solve)."""

@@ -373,6 +373,25 @@ def test_batch_matches_single_and_oracle():
     _report("batch", rows)
 
 
+def test_batch_node_storage_matches_single_game():
+    """ps_batch_node_storage (the batch's extract_results) returns every
+    decision node's strategy sums and regrets as the single game does after
+    the same solve."""
+    sp = spots.datagen_spots(3, seed=52)
+    cc = [spots.card_config(r, b) for r, b, _ in sp]
+    tcs = [t for _, _, t in sp]
+    bs = ps.BatchSolver(cc, tcs)
+    bs.solve(25, np.full(3, -1e30, np.float32))
+    for i, (r, b, t) in enumerate(sp):
+        g = spots.product_game(r, b, t)
+        for k in range(25):
+            ps.solve_step(g, k)
+        assert bs.num_nodes(i) == g.num_nodes()
+        for n in range(g.num_nodes()):
+            for which in (1, 2):
+                assert np.array_equal(bs.node_storage(i, n, which), g.node_storage(n, which))
+
+
 def test_batch_root_cfvalues_match_single_game():
     """The batch's device-side root cfvalues equal the single game's
     root_cfvalues after the same solve (same kernels, same arithmetic)."""
