@@ -154,14 +154,29 @@ int ps_boundary_reach(ps_game* g, float* out);
  * items (a request's boundaries, flattened), each with its 4-card board
  * (host [n][4]), pot and effective stack (host [n]).  Device arrays:
  *   net   [n][2][48][1326]  network outputs per player, river (the 48 cards not on
- *                           the board, ascending) and combo (card_pair_to_index order)
+ *                           the board, ascending) and combo (card_pair_to_index order);
+ *                           f32, or bf16 when net_bf16
  *   reach [n][2][1326]      OOP and IP reach at the boundary, combo order
  *   hands [H]               combo index of each output hand
  *   out   [n][2][H]         player 0 averaged with IP-reach weights, player 1 with OOP
  * stream: a cudaStream_t (NULL = the default stream); returns after the work is done. */
 int ps_boundary_river_reduce(int32_t n, const uint8_t* boards, const float* pots, const float* stacks,
-                             const float* net, const float* reach, const int32_t* hands, int32_t H, float* out,
-                             void* stream);
+                             const void* net, int32_t net_bf16, const float* reach, const int32_t* hands, int32_t H,
+                             float* out, void* stream);
+/* The first Linear layer (h outputs over the 2720 inputs) of a boundary
+ * network for every input row that ps_boundary_encode would write, without
+ * writing those rows (no reference counterpart; the reference runs the layer
+ * on the materialised rows, gpu_boundary_eval.rs:164-197).  A river card's row
+ * differs from the unmasked reach only in the 51 combos holding that card, so
+ *   row(i, p, r) = base[i] - percard[i][r] + the board, rank, pot, stack and
+ *                  player columns + bias,
+ * with base [n][h] = W[:, :2652] [oop | ip] and percard [n][52][h] = the same
+ * product over the combos holding each card (both from the caller's GEMMs),
+ * wcols [68][h] = W[:, 2652:] transposed, bias [h] or null.  boards, pots,
+ * stacks: host; the rest device; out [n][2][48][h], f32 or bf16. */
+int ps_boundary_first_layer(int32_t n, const uint8_t* boards, const float* pots, const float* stacks,
+                            const float* base, const float* percard, const float* wcols, const float* bias, int32_t h,
+                            void* out, int32_t out_bf16, void* stream);
 
 /* ---- navigation and queries (game/query.rs) ---- */
 int ps_back_to_root(ps_game* g);

@@ -91,7 +91,8 @@ _sig("ps_finalize", i32, vp)
 _sig("ps_root_cfvalues_with_reach", i32, vp, i32, P(f32), P(f32))
 _sig("ps_eval_fixed_strategy", i32, vp, P(f32), P(f32), P(f32), P(f32))
 _sig("ps_boundary_reach", i32, vp, P(f32))
-_sig("ps_boundary_river_reduce", i32, i32, P(C.c_uint8), P(f32), P(f32), vp, vp, vp, i32, vp, vp)
+_sig("ps_boundary_river_reduce", i32, i32, P(C.c_uint8), P(f32), P(f32), vp, i32, vp, vp, i32, vp, vp)
+_sig("ps_boundary_first_layer", i32, i32, P(C.c_uint8), P(f32), P(f32), vp, vp, vp, vp, i32, vp, i32, vp)
 _sig("ps_eval_fixed_strategy_adjoint", i32, vp, P(f32), P(f32), P(f32), P(f32), P(f32), P(f32), P(f32))
 _sig("ps_num_private_hands", i32, vp, i32)
 _sig("ps_private_cards", i32, vp, i32, P(C.c_uint8))

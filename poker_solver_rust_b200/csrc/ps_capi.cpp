@@ -1264,8 +1264,8 @@ int ps_boundary_reach(ps_game* G, float* out) {
 }
 
 int ps_boundary_river_reduce(int32_t n, const uint8_t* boards, const float* pots, const float* stacks,
-                             const float* net, const float* reach, const int32_t* hands, int32_t H, float* out,
-                             void* stream) {
+                             const void* net, int32_t net_bf16, const float* reach, const int32_t* hands, int32_t H,
+                             float* out, void* stream) {
   if (n < 0 || H < 0 || H > 1326 || (n > 0 && (!boards || !pots || !stacks || !net || !reach || !hands || !out)))
     return fail(PS_ERR_INVALID, "bad argument");
   if (n == 0 || H == 0) return PS_OK;
@@ -1288,7 +1288,39 @@ int ps_boundary_river_reduce(int32_t n, const uint8_t* boards, const float* pots
   float* d_dn = (float*)(d + ((hb.size() + 15) & ~(size_t)15));
   CU(cudaMemcpyAsync(d, hb.data(), hb.size(), cudaMemcpyHostToDevice, s));
   CU(cudaMemcpyAsync(d_dn, dn.data(), 4 * dn.size(), cudaMemcpyHostToDevice, s));
-  CU(launch_boundary_river_reduce(n, (const uint8_t*)d, d_dn, net, reach, hands, H, out, s));
+  CU(launch_boundary_river_reduce(n, (const uint8_t*)d, d_dn, net, net_bf16 ? 1 : 0, reach, hands, H, out, s));
+  CU(cudaStreamSynchronize(s));
+  return PS_OK;
+}
+
+int ps_boundary_first_layer(int32_t n, const uint8_t* boards, const float* pots, const float* stacks,
+                            const float* base, const float* percard, const float* wcols, const float* bias, int32_t h,
+                            void* out, int32_t out_bf16, void* stream) {
+  if (n < 0 || h < 0 || (n > 0 && h > 0 && (!boards || !pots || !stacks || !base || !percard || !wcols || !out)))
+    return fail(PS_ERR_INVALID, "bad argument");
+  if (n == 0 || h == 0) return PS_OK;
+  std::vector<uint8_t> hb((size_t)n * 4);
+  for (int i = 0; i < n; ++i) {
+    uint64_t seen = 0;
+    for (int k = 0; k < 4; ++k) {
+      const uint8_t c = boards[4 * i + k];
+      if (c >= 52 || (seen >> c & 1)) return fail(PS_ERR_INVALID, "boards must hold 4 distinct cards below 52");
+      seen |= 1ull << c;
+      hb[4 * i + k] = c;
+    }
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t ob = (hb.size() + 15) & ~(size_t)15;
+  char* d = nullptr;
+  CU(cudaMalloc(&d, ob + 8 * (size_t)n + 16));
+  std::unique_ptr<char, decltype(&cudaFree)> keep(d, &cudaFree);
+  float* d_pot = (float*)(d + ob);
+  float* d_stack = d_pot + n;
+  CU(cudaMemcpyAsync(d, hb.data(), hb.size(), cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(d_pot, pots, 4 * (size_t)n, cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(d_stack, stacks, 4 * (size_t)n, cudaMemcpyHostToDevice, s));
+  CU(launch_boundary_first_layer(n, (const uint8_t*)d, d_pot, d_stack, base, percard, wcols, bias, h, out,
+                                 out_bf16 ? 1 : 0, s));
   CU(cudaStreamSynchronize(s));
   return PS_OK;
 }

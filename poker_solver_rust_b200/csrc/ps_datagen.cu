@@ -29,8 +29,12 @@ __device__ __forceinline__ void combo_cards(int idx, int& c1, int& c2) {
   c2 = idx - a * (101 - a) / 2 + 1;
 }
 
+__device__ __forceinline__ double net_value(const float* p, size_t i) { return (double)p[i]; }
+__device__ __forceinline__ double net_value(const __nv_bfloat16* p, size_t i) { return (double)__bfloat162float(p[i]); }
+
+template <typename T>
 __global__ void k_boundary_river_reduce(int n, const uint8_t* __restrict__ boards, const float* __restrict__ denorm,
-                                        const float* __restrict__ net, const float* __restrict__ reach,
+                                        const T* __restrict__ net, const float* __restrict__ reach,
                                         const int32_t* __restrict__ hands, int H, float* __restrict__ out) {
   const int item = blockIdx.x >> 1, p = blockIdx.x & 1, o = p ^ 1;
   if (item >= n) return;
@@ -69,7 +73,7 @@ __global__ void k_boundary_river_reduce(int n, const uint8_t* __restrict__ board
     s_w[ri] = total - blocked;
   }
   __syncthreads();
-  const float* np_ = net + ((size_t)item * 2 + p) * kRivers * kCombos;
+  const T* np_ = net + ((size_t)item * 2 + p) * kRivers * kCombos;
   const double scale = (double)denorm[item];
   for (int h = threadIdx.x; h < H; h += blockDim.x) {
     const int combo = hands[h];
@@ -83,7 +87,7 @@ __global__ void k_boundary_river_reduce(int n, const uint8_t* __restrict__ board
     for (int ri = 0; ri < kRivers; ++ri) {
       const int r = s_river[ri];
       if (r == c1 || r == c2) continue;
-      num += s_w[ri] * (double)np_[(size_t)ri * kCombos + combo];
+      num += s_w[ri] * net_value(np_, (size_t)ri * kCombos + combo);
       den += s_w[ri];
     }
     out[((size_t)item * 2 + p) * H + h] = den > 0.0 ? (float)(num / den * scale) : 0.0f;
@@ -311,11 +315,73 @@ cudaError_t launch_pack_records(const SpotDev* spots, int n, const float* ranges
   return cudaGetLastError();
 }
 
-cudaError_t launch_boundary_river_reduce(int n, const uint8_t* boards, const float* denorm, const float* net,
-                                         const float* reach, const int32_t* hands, int H, float* out,
+cudaError_t launch_boundary_river_reduce(int n, const uint8_t* boards, const float* denorm, const void* net,
+                                         int net_bf16, const float* reach, const int32_t* hands, int H, float* out,
                                          cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  k_boundary_river_reduce<<<2 * n, 256, 0, s>>>(n, boards, denorm, net, reach, hands, H, out);
+  if (net_bf16)
+    k_boundary_river_reduce<__nv_bfloat16><<<2 * n, 256, 0, s>>>(
+        n, boards, denorm, static_cast<const __nv_bfloat16*>(net), reach, hands, H, out);
+  else
+    k_boundary_river_reduce<float><<<2 * n, 256, 0, s>>>(n, boards, denorm, static_cast<const float*>(net), reach,
+                                                         hands, H, out);
+  return cudaGetLastError();
+}
+
+// First layer of a boundary network (a Linear over the 2720 input values)
+// for every input row of boundary_encode, without writing the rows: for item
+// i, player p and river card r,
+//   W x = W_reach [oop|ip] - sum over combos holding r of W_reach[., c] reach[c]
+//         + board / rank one-hot columns + pot, stack, player columns (+ bias)
+// base[i] = W_reach [oop|ip] and percard[i][k] (the sum over the combos
+// holding card k) come from the caller's GEMMs; this kernel adds the column
+// terms and writes [n][2][48][h], one block per (item, player).
+template <bool BF16>
+__global__ void k_boundary_first_layer(const uint8_t* __restrict__ boards, const float* __restrict__ pots,
+                                       const float* __restrict__ stacks, const float* __restrict__ base,
+                                       const float* __restrict__ percard, const float* __restrict__ wcols,
+                                       const float* __restrict__ bias, int h, void* __restrict__ out) {
+  const int item = blockIdx.x >> 1, player = blockIdx.x & 1;
+  const uint8_t* bd = boards + 4 * item;
+  const uint64_t bmask = (1ull << bd[0]) | (1ull << bd[1]) | (1ull << bd[2]) | (1ull << bd[3]);
+  const unsigned ranks4 = (1u << (bd[0] >> 2)) | (1u << (bd[1] >> 2)) | (1u << (bd[2] >> 2)) | (1u << (bd[3] >> 2));
+  const float pot = pots[item], stack = stacks[item];
+  const float total = __fadd_rn(pot, stack);
+  const float norm = total > 0.f ? total : 1.f;
+  const float fpot = __fdiv_rn(pot, norm), fstack = __fdiv_rn(stack, norm);
+  const float* wpot = wcols + (size_t)(52 + 13) * h;
+  const float* wstack = wpot + h;
+  const float* wplayer = wstack + h;
+  for (int j = threadIdx.x; j < h; j += blockDim.x) {
+    float c = base[(size_t)item * h + j];
+    for (int k = 0; k < 4; ++k) c += wcols[(size_t)bd[k] * h + j];
+    for (int q = 0; q < 13; ++q)
+      if (ranks4 >> q & 1) c += wcols[(size_t)(52 + q) * h + j];
+    c += fpot * wpot[j] + fstack * wstack[j] + (player ? wplayer[j] : 0.f) + (bias ? bias[j] : 0.f);
+    int ri = 0;
+    for (int r = 0; r < 52; ++r) {
+      if (bmask >> r & 1) continue;
+      float v = c - percard[((size_t)item * 52 + r) * h + j] + wcols[(size_t)r * h + j];
+      if (!(ranks4 >> (r >> 2) & 1)) v += wcols[(size_t)(52 + (r >> 2)) * h + j];
+      const size_t o = (((size_t)item * 2 + player) * kRivers + ri) * h + j;
+      if (BF16)
+        static_cast<__nv_bfloat16*>(out)[o] = __float2bfloat16_rn(v);
+      else
+        static_cast<float*>(out)[o] = v;
+      ++ri;
+    }
+  }
+}
+
+cudaError_t launch_boundary_first_layer(int n, const uint8_t* boards, const float* pots, const float* stacks,
+                                        const float* base, const float* percard, const float* wcols,
+                                        const float* bias, int h, void* out, int bf16, cudaStream_t s) {
+  if (n <= 0 || h <= 0) return cudaSuccess;
+  const int threads = h >= 256 ? 256 : ((h + 31) / 32) * 32;
+  if (bf16)
+    k_boundary_first_layer<true><<<2 * n, threads, 0, s>>>(boards, pots, stacks, base, percard, wcols, bias, h, out);
+  else
+    k_boundary_first_layer<false><<<2 * n, threads, 0, s>>>(boards, pots, stacks, base, percard, wcols, bias, h, out);
   return cudaGetLastError();
 }
 

@@ -52,11 +52,20 @@ struct GridJob {
 };
 int grid_ctas(int block, const SmemPlan& plan);
 // Reach-weighted 48-river average of boundary-network outputs (ps_datagen.cu):
-// boards [n][4], denorm [n] (pot + stack), net [n][2][48][1326], reach
-// [n][2][1326], hands [H] combo indices, out [n][2][H]; all device pointers.
-cudaError_t launch_boundary_river_reduce(int n, const uint8_t* boards, const float* denorm, const float* net,
-                                         const float* reach, const int32_t* hands, int H, float* out,
+// boards [n][4], denorm [n] (pot + stack), net [n][2][48][1326] (f32, or bf16
+// when net_bf16), reach [n][2][1326], hands [H] combo indices, out [n][2][H];
+// all device pointers.
+cudaError_t launch_boundary_river_reduce(int n, const uint8_t* boards, const float* denorm, const void* net,
+                                         int net_bf16, const float* reach, const int32_t* hands, int H, float* out,
                                          cudaStream_t s);
+// First layer of a boundary network over every input row of
+// launch_boundary_encode without the rows: base [n][h] (weights times the
+// reach rows), percard [n][52][h] (weights times the reach of the combos
+// holding each card), wcols [68][h] (the board, rank, pot, stack and player
+// columns), bias [h] or null; out [n][2][48][h], f32 or bf16.
+cudaError_t launch_boundary_first_layer(int n, const uint8_t* boards, const float* pots, const float* stacks,
+                                        const float* base, const float* percard, const float* wcols,
+                                        const float* bias, int h, void* out, int bf16, cudaStream_t s);
 // Boundary items of a batch (item = (spot, boundary ordinal)) in the 1326-combo
 // layout (card.rs:50-55 index), [items][2][1326], against each spot's hand-order
 // buffers.  which: BC_SET_VALUES gathers `in` into sp.bcfv; BC_REACH / BC_GRAD

@@ -11,6 +11,9 @@
   kernels, so the comparison is bit for bit.
 - The datagen loop (solve_with_boundary_net) against the same loop composed by
   hand from single games and the separately checked device pieces.
+- The factored first layer (boundary_first_layer) against the network's first
+  Linear on the encoded rows, within 1e-5 of the largest output (f32; the sums
+  run in another order); bf16 output as the rounding of the f32 one.
 """
 
 import numpy as np
@@ -19,8 +22,8 @@ import torch
 
 import poker_solver_rust_b200 as ps
 from oracle import boundary_io as bio
-from poker_solver_rust_b200.datagen import (boundary_encode, boundary_reach, boundary_river_reduce,
-                                            solve_with_boundary_net)
+from poker_solver_rust_b200.datagen import (boundary_encode, boundary_first_layer, boundary_reach,
+                                            boundary_river_reduce, evaluate_boundaries, solve_with_boundary_net)
 from tests import spots
 from tests.test_gpu_adjoint import _sparse
 
@@ -141,7 +144,7 @@ def test_solve_with_boundary_net_composes_the_pieces():
     sp = _dl_spots(3, 90)
     net = _net()
     bs = _batch(sp)
-    items = solve_with_boundary_net(bs, net, iterations=12, eval_interval=5)
+    items = solve_with_boundary_net(bs, net, iterations=12, eval_interval=5, factored=False)
     e, it = bs.results()
     assert (it == 12).all()
     # the same loop by hand: single games, their own boundary reach, the
@@ -235,3 +238,45 @@ def test_batch_solved_values_autograd():
     _, dB = bs.adjoint(cot)
     assert torch.equal(B.grad, dB)
     assert B.grad.abs().sum() > 0
+
+
+def _random_items(rng, n):
+    boards = np.stack([rng.choice(52, 4, replace=False) for _ in range(n)]).astype(np.uint8)
+    pots = rng.uniform(10, 300, n).astype(np.float32).round()
+    stacks = rng.uniform(0, 400, n).astype(np.float32).round()
+    reach = rng.random((n, 2, 1326)).astype(np.float32)
+    pairs = bio.combo_pairs()
+    for i in range(n):
+        blocked = np.isin(pairs[:, 0], boards[i]) | np.isin(pairs[:, 1], boards[i])
+        reach[i, :, blocked] = 0.0
+    return boards, pots, stacks, torch.from_numpy(reach).cuda()
+
+
+def test_factored_first_layer_matches_dense():
+    rng = np.random.default_rng(23)
+    boards, pots, stacks, reach = _random_items(rng, 3)
+    torch.manual_seed(1)
+    lin = torch.nn.Linear(2720, 40).cuda()
+    with torch.no_grad():
+        dense = lin(boundary_encode(boards, pots, stacks, reach).view(-1, 2720)).view(3, 2, 48, 40)
+        fact = boundary_first_layer(boards, pots, stacks, reach, lin.weight, lin.bias)
+        f16 = boundary_first_layer(boards, pots, stacks, reach, lin.weight, lin.bias, bf16=True)
+    scale = dense.abs().max().item()
+    assert (fact - dense).abs().max().item() <= 1e-5 * scale
+    assert torch.equal(f16, fact.to(torch.bfloat16))
+
+
+def test_bf16_river_average_and_factored_evaluation():
+    rng = np.random.default_rng(29)
+    boards, pots, stacks, reach = _random_items(rng, 2)
+    combos = torch.arange(1326, dtype=torch.int32, device="cuda")
+    y = torch.tensor(rng.normal(0, 0.1, (2, 2, 48, 1326)).astype(np.float32), device="cuda").to(torch.bfloat16)
+    a = boundary_river_reduce(boards, pots, stacks, y, reach, combos)
+    b = boundary_river_reduce(boards, pots, stacks, y.float(), reach, combos)
+    assert torch.equal(a, b)
+    torch.manual_seed(2)
+    net = torch.nn.Sequential(torch.nn.Linear(2720, 32), torch.nn.ReLU(), torch.nn.Linear(32, 1326)).cuda()
+    items = {"boards": boards, "pots": pots, "stacks": stacks, "spot": np.zeros(2, np.int32)}
+    fast = evaluate_boundaries(items, reach, net)
+    slow = evaluate_boundaries(items, reach, net, factored=False)
+    assert (fast - slow).abs().max().item() <= 1e-4 * slow.abs().max().item()
