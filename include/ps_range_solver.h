@@ -172,8 +172,8 @@ int ps_boundary_river_reduce(int32_t n, const uint8_t* boards, const float* pots
  *                  player columns + bias,
  * with base [n][h] = W[:, :2652] [oop | ip] and percard [n][52][h] = the same
  * product over the combos holding each card (both from the caller's GEMMs),
- * wcols [68][h] = W[:, 2652:] transposed, bias [h] or null.  boards, pots,
- * stacks: host; the rest device; out [n][2][48][h], f32 or bf16. */
+ * wcols [68][h] = W[:, 2652:] transposed, bias [h] or null; h <= 8192.
+ * boards, pots, stacks: host; the rest device; out [n][2][48][h], f32 or bf16. */
 int ps_boundary_first_layer(int32_t n, const uint8_t* boards, const float* pots, const float* stacks,
                             const float* base, const float* percard, const float* wcols, const float* bias, int32_t h,
                             void* out, int32_t out_bf16, void* stream);

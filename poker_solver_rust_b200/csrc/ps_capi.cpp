@@ -1299,6 +1299,7 @@ int ps_boundary_first_layer(int32_t n, const uint8_t* boards, const float* pots,
   if (n < 0 || h < 0 || (n > 0 && h > 0 && (!boards || !pots || !stacks || !base || !percard || !wcols || !out)))
     return fail(PS_ERR_INVALID, "bad argument");
   if (n == 0 || h == 0) return PS_OK;
+  if (h > kMaxFirstLayerWidth) return fail(PS_ERR_INVALID, "first layer wider than 8192");
   std::vector<uint8_t> hb((size_t)n * 4);
   for (int i = 0; i < n; ++i) {
     uint64_t seen = 0;

@@ -334,17 +334,27 @@ cudaError_t launch_boundary_river_reduce(int n, const uint8_t* boards, const flo
 //   W x = W_reach [oop|ip] - sum over combos holding r of W_reach[., c] reach[c]
 //         + board / rank one-hot columns + pot, stack, player columns (+ bias)
 // base[i] = W_reach [oop|ip] and percard[i][k] (the sum over the combos
-// holding card k) come from the caller's GEMMs; this kernel adds the column
-// terms and writes [n][2][48][h], one block per (item, player).
+// holding card k) come from the caller's GEMMs.  One block per item: the
+// river-independent part of the row goes to shared memory, then every
+// (river, column) element is independent and coalesced along the columns;
+// both players' rows come from one read of percard (they differ by the player
+// column).  out [n][2][48][h].
 template <bool BF16>
 __global__ void k_boundary_first_layer(const uint8_t* __restrict__ boards, const float* __restrict__ pots,
                                        const float* __restrict__ stacks, const float* __restrict__ base,
                                        const float* __restrict__ percard, const float* __restrict__ wcols,
                                        const float* __restrict__ bias, int h, void* __restrict__ out) {
-  const int item = blockIdx.x >> 1, player = blockIdx.x & 1;
+  extern __shared__ float s_c[];  // [h]
+  __shared__ uint8_t s_river[kRivers];
+  const int item = blockIdx.x;
   const uint8_t* bd = boards + 4 * item;
   const uint64_t bmask = (1ull << bd[0]) | (1ull << bd[1]) | (1ull << bd[2]) | (1ull << bd[3]);
   const unsigned ranks4 = (1u << (bd[0] >> 2)) | (1u << (bd[1] >> 2)) | (1u << (bd[2] >> 2)) | (1u << (bd[3] >> 2));
+  if (threadIdx.x == 0) {
+    int k = 0;
+    for (int c = 0; c < 52; ++c)
+      if (!(bmask >> c & 1)) s_river[k++] = (uint8_t)c;
+  }
   const float pot = pots[item], stack = stacks[item];
   const float total = __fadd_rn(pot, stack);
   const float norm = total > 0.f ? total : 1.f;
@@ -357,18 +367,23 @@ __global__ void k_boundary_first_layer(const uint8_t* __restrict__ boards, const
     for (int k = 0; k < 4; ++k) c += wcols[(size_t)bd[k] * h + j];
     for (int q = 0; q < 13; ++q)
       if (ranks4 >> q & 1) c += wcols[(size_t)(52 + q) * h + j];
-    c += fpot * wpot[j] + fstack * wstack[j] + (player ? wplayer[j] : 0.f) + (bias ? bias[j] : 0.f);
-    int ri = 0;
-    for (int r = 0; r < 52; ++r) {
-      if (bmask >> r & 1) continue;
-      float v = c - percard[((size_t)item * 52 + r) * h + j] + wcols[(size_t)r * h + j];
-      if (!(ranks4 >> (r >> 2) & 1)) v += wcols[(size_t)(52 + (r >> 2)) * h + j];
-      const size_t o = (((size_t)item * 2 + player) * kRivers + ri) * h + j;
-      if (BF16)
-        static_cast<__nv_bfloat16*>(out)[o] = __float2bfloat16_rn(v);
-      else
-        static_cast<float*>(out)[o] = v;
-      ++ri;
+    s_c[j] = c + fpot * wpot[j] + fstack * wstack[j] + (bias ? bias[j] : 0.f);
+  }
+  __syncthreads();
+  const float* pc = percard + (size_t)item * 52 * h;
+  const size_t o0 = (size_t)item * 2 * kRivers * h, o1 = o0 + (size_t)kRivers * h;
+  for (int e = threadIdx.x; e < kRivers * h; e += blockDim.x) {
+    const int ri = e / h, j = e - ri * h;
+    const int r = s_river[ri];
+    float v = s_c[j] - pc[(size_t)r * h + j] + wcols[(size_t)r * h + j];
+    if (!(ranks4 >> (r >> 2) & 1)) v += wcols[(size_t)(52 + (r >> 2)) * h + j];
+    const float v1 = v + wplayer[j];
+    if (BF16) {
+      static_cast<__nv_bfloat16*>(out)[o0 + e] = __float2bfloat16_rn(v);
+      static_cast<__nv_bfloat16*>(out)[o1 + e] = __float2bfloat16_rn(v1);
+    } else {
+      static_cast<float*>(out)[o0 + e] = v;
+      static_cast<float*>(out)[o1 + e] = v1;
     }
   }
 }
@@ -377,11 +392,12 @@ cudaError_t launch_boundary_first_layer(int n, const uint8_t* boards, const floa
                                         const float* base, const float* percard, const float* wcols,
                                         const float* bias, int h, void* out, int bf16, cudaStream_t s) {
   if (n <= 0 || h <= 0) return cudaSuccess;
-  const int threads = h >= 256 ? 256 : ((h + 31) / 32) * 32;
+  if (h > kMaxFirstLayerWidth) return cudaErrorInvalidValue;
+  const size_t smem = sizeof(float) * (size_t)h;
   if (bf16)
-    k_boundary_first_layer<true><<<2 * n, threads, 0, s>>>(boards, pots, stacks, base, percard, wcols, bias, h, out);
+    k_boundary_first_layer<true><<<n, 256, smem, s>>>(boards, pots, stacks, base, percard, wcols, bias, h, out);
   else
-    k_boundary_first_layer<false><<<2 * n, threads, 0, s>>>(boards, pots, stacks, base, percard, wcols, bias, h, out);
+    k_boundary_first_layer<false><<<n, 256, smem, s>>>(boards, pots, stacks, base, percard, wcols, bias, h, out);
   return cudaGetLastError();
 }
 

@@ -62,7 +62,9 @@ cudaError_t launch_boundary_river_reduce(int n, const uint8_t* boards, const flo
 // launch_boundary_encode without the rows: base [n][h] (weights times the
 // reach rows), percard [n][52][h] (weights times the reach of the combos
 // holding each card), wcols [68][h] (the board, rank, pot, stack and player
-// columns), bias [h] or null; out [n][2][48][h], f32 or bf16.
+// columns), bias [h] or null; out [n][2][48][h], f32 or bf16; h at most
+// kMaxFirstLayerWidth (its row part stays in shared memory).
+constexpr int kMaxFirstLayerWidth = 8192;
 cudaError_t launch_boundary_first_layer(int n, const uint8_t* boards, const float* pots, const float* stacks,
                                         const float* base, const float* percard, const float* wcols,
                                         const float* bias, int h, void* out, int bf16, cudaStream_t s);
