@@ -77,6 +77,41 @@ struct PinnedPool {
   }
 };
 PinnedPool g_pinned;
+
+// Device staging for the per-call metadata of the datagen entry points
+// (boards, pots, stacks, an error word): one buffer per device that only
+// grows.  A call holds it, under the lock, until its stream work is done, so
+// the common case allocates and frees nothing (cudaFree would synchronise the
+// whole device).
+struct DeviceStaging {
+  std::mutex mu;
+  char* buf[16] = {};
+  size_t cap[16] = {};
+};
+DeviceStaging g_staging;
+
+struct StagingLease {
+  std::unique_lock<std::mutex> lk;
+  char* ptr = nullptr;
+  cudaError_t acquire(size_t bytes) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 16) return cudaErrorInvalidDevice;
+    lk = std::unique_lock<std::mutex>(g_staging.mu);
+    if (g_staging.cap[dev] < bytes) {
+      if (g_staging.buf[dev]) cudaFree(g_staging.buf[dev]);
+      g_staging.buf[dev] = nullptr;
+      g_staging.cap[dev] = 0;
+      const size_t c = std::max<size_t>(bytes, (size_t)1 << 16);
+      e = cudaMalloc(&g_staging.buf[dev], c);
+      if (e != cudaSuccess) return e;
+      g_staging.cap[dev] = c;
+    }
+    ptr = g_staging.buf[dev];
+    return cudaSuccess;
+  }
+};
 std::map<long, std::pair<int, int>> g_tune;  // autotuned (CTA size, scan-buffer warps) per
                                              // (device, hand-count class, tree-size class)
 DeviceConsts g_dev[16];
@@ -1282,9 +1317,9 @@ int ps_boundary_river_reduce(int32_t n, const uint8_t* boards, const float* pots
     dn[i] = (float)((double)pots[i] + (double)stacks[i]);
   }
   cudaStream_t s = (cudaStream_t)stream;
-  char* d = nullptr;
-  CU(cudaMalloc(&d, hb.size() + 4 * dn.size() + 16));
-  std::unique_ptr<char, decltype(&cudaFree)> keep(d, &cudaFree);
+  StagingLease lease;
+  CU(lease.acquire(hb.size() + 4 * dn.size() + 16));
+  char* d = lease.ptr;
   float* d_dn = (float*)(d + ((hb.size() + 15) & ~(size_t)15));
   CU(cudaMemcpyAsync(d, hb.data(), hb.size(), cudaMemcpyHostToDevice, s));
   CU(cudaMemcpyAsync(d_dn, dn.data(), 4 * dn.size(), cudaMemcpyHostToDevice, s));
@@ -1312,9 +1347,9 @@ int ps_boundary_first_layer(int32_t n, const uint8_t* boards, const float* pots,
   }
   cudaStream_t s = (cudaStream_t)stream;
   const size_t ob = (hb.size() + 15) & ~(size_t)15;
-  char* d = nullptr;
-  CU(cudaMalloc(&d, ob + 8 * (size_t)n + 16));
-  std::unique_ptr<char, decltype(&cudaFree)> keep(d, &cudaFree);
+  StagingLease lease;
+  CU(lease.acquire(ob + 8 * (size_t)n + 16));
+  char* d = lease.ptr;
   float* d_pot = (float*)(d + ob);
   float* d_stack = d_pot + n;
   CU(cudaMemcpyAsync(d, hb.data(), hb.size(), cudaMemcpyHostToDevice, s));
@@ -2055,9 +2090,9 @@ int ps_sample_situations(const ps_sampler_config* cfg, int64_t first, int32_t n,
   P.first = first;
   if (n == 0) return PS_OK;
   cudaStream_t s = (cudaStream_t)stream;
-  int* d_err = nullptr;
-  CU(cudaMalloc(&d_err, sizeof(int)));
-  std::unique_ptr<int, decltype(&cudaFree)> keep(d_err, &cudaFree);
+  StagingLease lease;
+  CU(lease.acquire(sizeof(int)));
+  int* d_err = (int*)lease.ptr;
   CU(cudaMemsetAsync(d_err, 0, sizeof(int), s));
   CU(launch_sample_situations(P, n, boards, pots, stacks, ranges, d_err, s));
   int e = 0;
@@ -2086,9 +2121,9 @@ int ps_boundary_encode(int32_t n, const uint8_t* boards, const float* pots, cons
   }
   cudaStream_t s = (cudaStream_t)stream;
   const size_t ob = ((hb.size() + 15) & ~(size_t)15);
-  char* d = nullptr;
-  CU(cudaMalloc(&d, ob + 8 * (size_t)n + 16));
-  std::unique_ptr<char, decltype(&cudaFree)> keep(d, &cudaFree);
+  StagingLease lease;
+  CU(lease.acquire(ob + 8 * (size_t)n + 16));
+  char* d = lease.ptr;
   float* d_pot = (float*)(d + ob);
   float* d_stack = d_pot + n;
   CU(cudaMemcpyAsync(d, hb.data(), hb.size(), cudaMemcpyHostToDevice, s));
