@@ -140,7 +140,8 @@ def turn_game_measure(ps, spots, iters: int, cpu_iters: int):
     stack 300, bets 33% / 75% / all-in, raise 60%) solved for a fixed number of
     iterations on the whole GPU (grid mode), timed through ps.solve from host
     to host (exploitability every 5 iterations and finalize included), beside
-    the oracle's time for `cpu_iters` iterations on one host thread."""
+    the oracle's time for `cpu_iters` iterations with the chance children
+    spread over all host threads."""
     import torch
 
     r, b, t = spots.turn_spot(2)
@@ -157,12 +158,20 @@ def turn_game_measure(ps, spots, iters: int, cpu_iters: int):
            "gpu_note": "ps.solve from host: iterations, exploitability every 5, finalize",
            "exploitability_pct_pot": 100.0 * e / t.starting_pot}
     if cpu_iters > 0:
-        o = spots.oracle_game(r, b, t)
-        t0 = time.perf_counter()
-        for it in range(cpu_iters):
-            o.solve_step(it)
-        out["cpu_ms_per_iteration"] = (time.perf_counter() - t0) / cpu_iters * 1e3
-        out["cpu"] = {"threads": 1, "kind": "port", "iterations_timed": cpu_iters}
+        from oracle import oracle as O
+
+        threads = os.cpu_count() or 1
+        O.set_chance_threads(threads)  # river chance children in parallel, as the reference's rayon
+        try:
+            o = spots.oracle_game(r, b, t)
+            t0 = time.perf_counter()
+            for it in range(cpu_iters):
+                o.solve_step(it)
+            out["cpu_ms_per_iteration"] = (time.perf_counter() - t0) / cpu_iters * 1e3
+        finally:
+            O.set_chance_threads(1)
+        out["cpu"] = {"threads": threads, "kind": "port", "iterations_timed": cpu_iters,
+                      "parallel": "the 48 river chance children of each chance node, as solver.rs:264-326 with rayon"}
     return out
 
 
@@ -344,7 +353,7 @@ def main():
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--turn-iters", type=int, default=500, help="single turn game iterations (0 = skip)")
-    ap.add_argument("--turn-cpu-iters", type=int, default=1)
+    ap.add_argument("--turn-cpu-iters", type=int, default=3)
     ap.add_argument("--adjoint-spots", type=int, default=1024, help="depth-limited turn spots + adjoint (0 = skip)")
     ap.add_argument("--adjoint-iters", type=int, default=300)
     ap.add_argument("--datagen-spots", type=int, default=512, help="turn-datagen loop spots (0 = skip)")

@@ -64,6 +64,7 @@ def lib():
             sig = {
                 "orc_last_error": (C.c_char_p, []),
                 "orc_set_hand_table_path": (None, [C.c_char_p]),
+                "orc_set_chance_threads": (None, [i32]),
                 "orc_hand_table_exhaustive": (i32, [P(i32), i32, P(C.c_uint64)]),
                 "orc_hand_table": (i32, [P(i32), i32]),
                 "orc_hand_evaluate_internal": (i32, [P(i32)]),
@@ -142,6 +143,12 @@ def hand_table() -> np.ndarray:
     out = np.zeros(8192, np.int32)
     n = lib().orc_hand_table(_p(out, C.c_int32), 8192)
     return out[:n].copy()
+
+
+def set_chance_threads(n: int) -> None:
+    """Threads for the chance children of solve passes, as the reference's
+    rayon parallelism (solver.rs:264-326); results do not depend on it."""
+    lib().orc_set_chance_threads(int(n))
 
 
 def hand_evaluate_internal(cards) -> int:

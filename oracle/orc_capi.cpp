@@ -51,6 +51,7 @@ struct OrcTreeConfig {
 const char* orc_last_error() { return g_err.c_str(); }
 
 void orc_set_hand_table_path(const char* p) { set_hand_table_path(p); }
+void orc_set_chance_threads(int n) { set_chance_threads(n); }
 
 int orc_hand_table_exhaustive(int32_t* table_out, int cap, uint64_t* counts9) {
   std::vector<int32_t> t;

@@ -7,7 +7,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <condition_variable>
 #include <cstring>
+#include <atomic>
 #include <functional>
 #include <mutex>
 #include <stdexcept>
@@ -1395,6 +1397,91 @@ static void apply_swap_list(F* v, const std::vector<std::pair<uint16_t, uint16_t
   for (auto [i, j] : sl) std::swap(v[i], v[j]);
 }
 
+// Chance children evaluated in parallel on a persistent pool, as the
+// reference's solve_recursive does with rayon (solver.rs:264-326 over
+// for_each_child): children write disjoint slices and are summed in child
+// order afterwards, so the results do not depend on the thread count.
+// Nested calls from a worker run inline.
+namespace {
+struct ChancePool {
+  std::mutex m, run_mu;
+  std::condition_variable cv, done;
+  std::vector<std::thread> workers;
+  const std::function<void(size_t)>* job = nullptr;
+  size_t count = 0;
+  std::atomic<size_t> next{0};
+  size_t finished = 0;  // workers that have checked in for the current job
+  uint64_t gen = 0;
+  bool stop = false;
+  static thread_local bool in_worker;
+
+  void resize(int n) {
+    shutdown();
+    stop = false;
+    for (int i = 0; i + 1 < n; ++i) workers.emplace_back([this] { loop(); });
+  }
+  void shutdown() {
+    {
+      std::lock_guard<std::mutex> lk(m);
+      stop = true;
+    }
+    cv.notify_all();
+    for (auto& t : workers) t.join();
+    workers.clear();
+  }
+  // every worker takes part in every job and checks in when done, so no
+  // worker can still hold a job when the next one starts
+  void loop() {
+    in_worker = true;
+    uint64_t seen = 0;
+    for (;;) {
+      const std::function<void(size_t)>* f;
+      size_t n;
+      {
+        std::unique_lock<std::mutex> lk(m);
+        cv.wait(lk, [&] { return stop || gen != seen; });
+        if (stop) return;
+        seen = gen;
+        f = job;
+        n = count;
+      }
+      for (size_t i; (i = next.fetch_add(1)) < n;) (*f)(i);
+      {
+        std::lock_guard<std::mutex> lk(m);
+        ++finished;
+      }
+      done.notify_all();
+    }
+  }
+  void parallel_for(size_t n, const std::function<void(size_t)>& f) {
+    if (workers.empty() || in_worker || n < 2) {
+      for (size_t i = 0; i < n; ++i) f(i);
+      return;
+    }
+    std::lock_guard<std::mutex> outer(run_mu);
+    {
+      std::lock_guard<std::mutex> lk(m);
+      job = &f;
+      count = n;
+      next = 0;
+      finished = 0;
+      ++gen;
+    }
+    cv.notify_all();
+    in_worker = true;
+    for (size_t i; (i = next.fetch_add(1)) < n;) f(i);
+    in_worker = false;
+    std::unique_lock<std::mutex> lk(m);
+    done.wait(lk, [&] { return finished == workers.size(); });
+  }
+  ~ChancePool() { shutdown(); }
+};
+thread_local bool ChancePool::in_worker = false;
+ChancePool g_chance_pool;
+}  // namespace
+
+void set_chance_threads(int n) { g_chance_pool.resize(n < 1 ? 1 : n); }
+
 // solver.rs:221-479
 template <class F>
 void Game<F>::solve_recursive(F* result, Node* node, int player, const F* cfreach,
@@ -1415,7 +1502,10 @@ void Game<F>::solve_recursive(F* result, Node* node, int player, const F* cfreac
     std::vector<F> upd(no);
     F scalar = (F)1 / (F)chance_factor(*node);
     for (size_t i = 0; i < no; ++i) upd[i] = cfreach[i] * scalar;
-    for (size_t a = 0; a < na; ++a) solve_recursive(&cfv[a * nh], child(node, a), player, upd.data(), params);
+    const std::function<void(size_t)> one = [&](size_t a) {
+      solve_recursive(&cfv[a * nh], child(node, a), player, upd.data(), params);
+    };
+    g_chance_pool.parallel_for(na, one);
     std::vector<double> acc(nh);
     for (size_t h = 0; h < nh; ++h) acc[h] = (double)cfv[h];
     for (size_t a = 1; a < na; ++a)

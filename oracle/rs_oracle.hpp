@@ -39,6 +39,8 @@ std::pair<int, int> index_to_card_pair(int index);
 int32_t hand_evaluate_internal(const int cards[7]);
 const std::vector<int32_t>& hand_table();
 void set_hand_table_path(const char* path);
+// threads for the chance children of solve passes (1 = sequential)
+void set_chance_threads(int n);
 uint16_t hand_evaluate(const int cards[7]);
 // Exhaustive enumeration over all C(52,7) hands (hand.rs:407-449): fills
 // the sorted distinct value table and the 9 category counts.

@@ -382,3 +382,20 @@ def test_sampler_restatement_pins():
         assert len(k) == 1 and stack >= 5
         seen.add(k[0])
     assert seen == {0, 1, 2}
+
+
+def test_oracle_chance_threads_keep_results():
+    """The oracle's parallel chance children (the reference's rayon split,
+    solver.rs:264-326) give the same state as the sequential walk."""
+    r, b, t = spots.turn_spot(4)
+    out = []
+    for threads in (1, 4):
+        O.set_chance_threads(threads)
+        try:
+            o = spots.oracle_game(r, b, t)
+            for it in range(2):
+                o.solve_step(it)
+            out.append((o.compute_exploitability(), o.root_cfvalues(0)))
+        finally:
+            O.set_chance_threads(1)
+    assert out[0][0] == out[1][0] and np.array_equal(out[0][1], out[1][1])
