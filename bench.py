@@ -175,6 +175,41 @@ def turn_game_measure(ps, spots, iters: int, cpu_iters: int):
     return out
 
 
+def river_game_measure(ps, spots, iters: int, cpu_iters: int):
+    """One plain river subgame (5-card board, U[0,1] ranges masked by the
+    board, pot 100, stack 200, bets 50% / 100% / all-in, raise 100%) solved
+    for `iters` iterations through ps.solve on one CTA (a river game is
+    latency-bound: iterations/s and the exploitability reached), beside the
+    oracle on one host thread (river nodes never parallelise in the
+    reference, node.rs:347-349).  The tree has no bet cap: the reference's
+    tree builder has none, so both sides solve the same tree."""
+    import torch
+
+    r, b, t = spots.river_spot(1)
+    ps.solve(spots.product_game(r, b, t), 5, 0.0)  # warm
+    g = spots.product_game(r, b, t)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e = ps.solve(g, iters, 0.0)
+    dt = time.perf_counter() - t0
+    H0 = g.num_private_hands(0)
+    root = g.strategy_at_index(0).reshape(-1, H0)
+    out = {"workload": "river subgame: pot 100, stack 200, bets 50%/100%/a, raise 100%",
+           "nodes": g.num_nodes(), "hands": [H0, g.num_private_hands(1)],
+           "iterations": iters, "gpu_iterations_per_s": iters / dt, "gpu_ms_per_iteration": dt / iters * 1e3,
+           "gpu_note": "ps.solve from host: iterations, exploitability every 5, finalize",
+           "exploitability_pct_pot": 100.0 * e / t.starting_pot,
+           "root_action_frequencies": [float(x) for x in root.mean(axis=1)]}
+    if cpu_iters > 0:
+        o = spots.oracle_game(r, b, t)
+        t0 = time.perf_counter()
+        for it in range(cpu_iters):
+            o.solve_step(it)
+        out["cpu_iterations_per_s"] = cpu_iters / (time.perf_counter() - t0)
+        out["cpu"] = {"threads": 1, "kind": "port", "iterations_timed": cpu_iters}
+    return out
+
+
 def turn_adjoint_measure(ps, spots, n: int, iters: int, cpu_sample: int):
     """Depth-limited turn spots solved with seeded boundary values, then the
     gradient of loss = MSE(root cfvalues, seeded target) with respect to the
@@ -354,6 +389,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--turn-iters", type=int, default=500, help="single turn game iterations (0 = skip)")
     ap.add_argument("--turn-cpu-iters", type=int, default=3)
+    ap.add_argument("--river-iters", type=int, default=1000, help="single river game iterations (0 = skip)")
+    ap.add_argument("--river-cpu-iters", type=int, default=200)
     ap.add_argument("--adjoint-spots", type=int, default=1024, help="depth-limited turn spots + adjoint (0 = skip)")
     ap.add_argument("--adjoint-iters", type=int, default=300)
     ap.add_argument("--datagen-spots", type=int, default=512, help="turn-datagen loop spots (0 = skip)")
@@ -462,6 +499,11 @@ def main():
     if rank == 0 and args.turn_iters > 0:
         turn = turn_game_measure(ps, spots, args.turn_iters, args.turn_cpu_iters)
 
+    # ---- single river game (config 1 of the spec) ----
+    river = None
+    if rank == 0 and args.river_iters > 0:
+        river = river_game_measure(ps, spots, args.river_iters, args.river_cpu_iters)
+
     # ---- depth-limited turn spots: solve + adjoint, and the datagen loop ----
     adjoint = datagen = None
     if rank == 0 and args.adjoint_spots > 0:
@@ -501,6 +543,7 @@ def main():
                                          "spot-iterations (profiles/k_solve_river_datagen_1024.md)"},
             "cpu_baseline": cpu,
             "plain_gpu": plain,
+            "river_game": river,
             "turn_game": turn,
             "turn_adjoint": adjoint,
             "turn_datagen": datagen,
