@@ -170,6 +170,13 @@ bool parse_tree_config(const ps_tree_config* c, TreeCfg& t, std::string& err) {
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+#ifndef PS_SINGLE_STAGE
+#define PS_SINGLE_STAGE 1  // single games stage single-board tables in shared memory
+#endif
+#ifndef PS_SINGLE_BUFS
+#define PS_SINGLE_BUFS 8  // single games: terminal scan buffers on all 8 warps
+#endif
+
 struct Layout {  // byte offsets inside the pool
   size_t cards[2], w[2], same[2], ops[2], steps[2], groups[2], nodes, board_cards, iso_perm[2], iso_off, iso_ent;  // static
   size_t gidx[2], coff[2], thr[2], nvalid[2], heads[2];                                                       // setup
@@ -461,6 +468,7 @@ struct Batch {
     plan.bufs = opts && opts->scan_buffers > 0 ? std::min(opts->scan_buffers, plan.warps)
                                                : std::max(1, plan.warps / 2);
     plan.tables = (single_board && stage == 1) ? table_bytes_for(hs_max, hs_max) : 0;
+    plan.split = n <= dc->nsm ? 1 : 0;  // a CTA per spot with an SM to itself: latency-bound
     int occ = solve_occupancy(block, plan);
     ctas_per_sm = opts && opts->ctas_per_sm > 0 ? std::min(opts->ctas_per_sm, occ) : occ;
     grid = std::max(1, std::min(n, dc->nsm * ctas_per_sm));
@@ -1102,7 +1110,15 @@ int ps_game_allocate_memory(ps_game* G, int enable_compression) {
   if (!G) return fail(PS_ERR_INVALID, "null game");
   if (enable_compression) return fail(PS_ERR_UNSUPPORTED, "compressed (16-bit) storage is not supported: state is FP32");
   if (G->state != GState::TreeBuilt) return PS_OK;
-  int rc = G->b->build(nullptr);
+  // one game on one CTA is latency-bound: its board tables go to shared
+  // memory when it has a single board, and every warp holds a terminal scan
+  // buffer (occupancy does not matter for a lone CTA)
+  ps_batch_opts o{};
+  o.block_threads = 0;
+  o.sort_by_cost = 1;
+  o.stage_tables = PS_SINGLE_STAGE;
+  o.scan_buffers = PS_SINGLE_BUFS;
+  int rc = G->b->build(&o);
   if (!rc) rc = G->b->run_setup();
   if (rc) return rc;
   G->state = GState::MemoryAllocated;

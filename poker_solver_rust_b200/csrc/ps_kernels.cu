@@ -86,6 +86,8 @@ struct Ctx {
   float* breach; // boundary reach buffer [num_boundary][2][vstride] (reach of each player), or null
   double* red;   // smem: reduction scratch       [32]
   Tables t0;     // board-0 tables (shared memory when staged, else global)
+  int split;     // 1: node ops may be split over idle warps (few items per step)
+  int part, parts;  // split node op: this item's column block and the number of blocks
 };
 
 __device__ __forceinline__ const float* slot_in(const Ctx& c, uint16_t id) {
@@ -155,15 +157,18 @@ __device__ __forceinline__ void prefetch_l2(const float* p, int n) { prefetch_l2
 // sigma from regret matching (DCFR) or from the normalised cumulative strategy,
 // then children's reach = sigma_a * reach.  Two sweeps over the actions: the
 // first forms the denominator, the second (L1 hits) the children.
-__device__ __noinline__ void op_fwd_opp(const Ctx& c, const Op& op, int o, int mode) {
+template <bool SPLIT>
+__device__ __noinline__ void op_fwd_opp_t(const Ctx& c, const Op& op, int o, int mode) {
+  // SPLIT: this item is column block c.part of c.parts (interleaved 32-column blocks)
+  const int part = SPLIT ? c.part : 0, parts = SPLIT ? c.parts : 1;
   const SpotDev& sp = *c.sp;
   const int hso = sp.hs[o], na = op.na, q4 = hso >> 2;
   const float* base = (mode == M_DCFR ? sp.R : sp.S) + sp.nodes[op.node].rs_off;
   const float* src = slot_in(c, op.src);
   float* dst = slot_at(c, op.blk);
   const float def = 1.0f / (float)na;
-  prefetch_l2(base, na * hso);
-  for (int q = (threadIdx.x & 31); q < q4; q += 32) {
+  if (part == 0) prefetch_l2(base, na * hso);
+  for (int q = part * 32 + (threadIdx.x & 31); q < q4; q += 32 * parts) {
     const int h = q << 2;
     float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int a = 0; a < na; ++a) {
@@ -179,17 +184,25 @@ __device__ __noinline__ void op_fwd_opp(const Ctx& c, const Op& op, int o, int m
     }
   }
 }
+__device__ __forceinline__ void op_fwd_opp(const Ctx& c, const Op& op, int o, int mode) {
+  op_fwd_opp_t<false>(c, op, o, mode);
+}
 
 // Chance node (solver.rs:264-276): one scaled reach shared by all children.
-__device__ __noinline__ void op_fwd_chance(const Ctx& c, const Op& op, int o) {
+template <bool SPLIT>
+__device__ __noinline__ void op_fwd_chance_t(const Ctx& c, const Op& op, int o) {
+  // SPLIT: this item is column block c.part of c.parts (interleaved 32-column blocks)
+  const int part = SPLIT ? c.part : 0, parts = SPLIT ? c.parts : 1;
   const SpotDev& sp = *c.sp;
   const int q4 = sp.hs[o] >> 2;
   const float f = __fdiv_rn(1.0f, (float)sp.nodes[op.node].chance_factor);
   const float4 f4 = make_float4(f, f, f, f);
   const float* src = slot_in(c, op.src);
   float* dst = slot_at(c, op.blk);
-  for (int q = (threadIdx.x & 31); q < q4; q += 32) st4(dst + (q << 2), mul4(ld4(src + (q << 2)), f4));
+  for (int q = part * 32 + (threadIdx.x & 31); q < q4; q += 32 * parts)
+    st4(dst + (q << 2), mul4(ld4(src + (q << 2)), f4));
 }
+__device__ __forceinline__ void op_fwd_chance(const Ctx& c, const Op& op, int o) { op_fwd_chance_t<false>(c, op, o); }
 
 // ---------------------------------------------------------------------------
 // Backward ops
@@ -202,7 +215,10 @@ __device__ __noinline__ void op_fwd_chance(const Ctx& c, const Op& op, int o) {
 //   AVG  (utility.rs:689-727): sigma = S / sum S; cfv = sum sigma_a cfv_a; SAVE stores cfv_a.
 // Three sweeps over the actions (denominator, result + S, regrets) keep the
 // per-thread state to a few float4 registers; repeated loads hit L1.
-__device__ __noinline__ void op_bwd_trav(const Ctx& c, const Op& op, int p, const Discount dc, int mode) {
+template <bool SPLIT>
+__device__ __noinline__ void op_bwd_trav_t(const Ctx& c, const Op& op, int p, const Discount dc, int mode) {
+  // SPLIT: this item is column block c.part of c.parts (interleaved 32-column blocks)
+  const int part = SPLIT ? c.part : 0, parts = SPLIT ? c.parts : 1;
   const SpotDev& sp = *c.sp;
   const int hsp = sp.hs[p], na = op.na, q4 = hsp >> 2;
   const NodeDev& nd = sp.nodes[op.node];
@@ -211,12 +227,14 @@ __device__ __noinline__ void op_bwd_trav(const Ctx& c, const Op& op, int p, cons
   const float* cb = slot_at(c, op.blk);
   float* dst = slot_at(c, op.dst);
   const float def = 1.0f / (float)na;
-  if (mode != M_BR) {
-    prefetch_l2(mode == M_DCFR ? R : S, na * hsp);
-    if (mode == M_DCFR) prefetch_l2(S, na * hsp);
+  if (part == 0) {
+    if (mode != M_BR) {
+      prefetch_l2(mode == M_DCFR ? R : S, na * hsp);
+      if (mode == M_DCFR) prefetch_l2(S, na * hsp);
+    }
+    for (int a = 0; a < na; ++a) prefetch_l2(cb + (size_t)a * c.vstride, hsp);
   }
-  for (int a = 0; a < na; ++a) prefetch_l2(cb + (size_t)a * c.vstride, hsp);
-  for (int q = (threadIdx.x & 31); q < q4; q += 32) {
+  for (int q = part * 32 + (threadIdx.x & 31); q < q4; q += 32 * parts) {
     const int h = q << 2;
     float4 res = make_float4(0.f, 0.f, 0.f, 0.f);
     if (mode == M_BR) {
@@ -263,16 +281,23 @@ __device__ __noinline__ void op_bwd_trav(const Ctx& c, const Op& op, int p, cons
     }
   }
 }
+__device__ __forceinline__ void op_bwd_trav(const Ctx& c, const Op& op, int p, const Discount dc, int mode) {
+  op_bwd_trav_t<false>(c, op, p, dc, mode);
+}
 
 // Opponent decision node: cfv = sum_a cfv_a (solver.rs:471).
-__device__ __noinline__ void op_bwd_opp(const Ctx& c, const Op& op, int p, int mode) {
+template <bool SPLIT>
+__device__ __noinline__ void op_bwd_opp_t(const Ctx& c, const Op& op, int p, int mode) {
+  // SPLIT: this item is column block c.part of c.parts (interleaved 32-column blocks)
+  const int part = SPLIT ? c.part : 0, parts = SPLIT ? c.parts : 1;
   const SpotDev& sp = *c.sp;
   const int q4 = sp.hs[p] >> 2, na = op.na;
   const NodeDev& nd = sp.nodes[op.node];
   const float* cb = slot_at(c, op.blk);
   float* dst = slot_at(c, op.dst);
-  for (int a = 0; a < na; ++a) prefetch_l2(cb + (size_t)a * c.vstride, sp.hs[p]);
-  for (int q = (threadIdx.x & 31); q < q4; q += 32) {
+  if (part == 0)
+    for (int a = 0; a < na; ++a) prefetch_l2(cb + (size_t)a * c.vstride, sp.hs[p]);
+  for (int q = part * 32 + (threadIdx.x & 31); q < q4; q += 32 * parts) {
     const int h = q << 2;
     float4 res = ld4(cb + h);
     for (int a = 1; a < na; ++a) res = add4(res, ld4(cb + (size_t)a * c.vstride + h));
@@ -284,10 +309,16 @@ __device__ __noinline__ void op_bwd_opp(const Ctx& c, const Op& op, int p, int m
     }
   }
 }
+__device__ __forceinline__ void op_bwd_opp(const Ctx& c, const Op& op, int p, int mode) {
+  op_bwd_opp_t<false>(c, op, p, mode);
+}
 
 // Chance node: cfv = sum over dealt cards, plus the suit-swapped rows of the
 // isomorphic cards that were not dealt (solver.rs:291-325).
-__device__ __noinline__ void op_bwd_chance(const Ctx& c, const Op& op, int p, int mode) {
+template <bool SPLIT>
+__device__ __noinline__ void op_bwd_chance_t(const Ctx& c, const Op& op, int p, int mode) {
+  // SPLIT: this item is column block c.part of c.parts (interleaved 32-column blocks)
+  const int part = SPLIT ? c.part : 0, parts = SPLIT ? c.parts : 1;
   const SpotDev& sp = *c.sp;
   const int hsp = sp.hs[p], na = op.na;
   const NodeDev& nd = sp.nodes[op.node];
@@ -298,7 +329,7 @@ __device__ __noinline__ void op_bwd_chance(const Ctx& c, const Op& op, int p, in
     i0 = sp.iso_off[op.board];
     i1 = sp.iso_off[op.board + 1];
   }
-  for (int h = (threadIdx.x & 31); h < hsp; h += 32) {
+  for (int h = part * 32 + (threadIdx.x & 31); h < hsp; h += 32 * parts) {
     float res = cb[h];
     for (int a = 1; a < na; ++a) res = __fadd_rn(res, cb[(size_t)a * c.vstride + h]);
     for (int i = i0; i < i1; ++i) {
@@ -309,6 +340,9 @@ __device__ __noinline__ void op_bwd_chance(const Ctx& c, const Op& op, int p, in
     dst[h] = res;
     if (mode == M_AVG_SAVE && nd.ch_player == p && h < sp.H[p]) sp.chcfv[nd.ch_off + h] = res;
   }
+}
+__device__ __forceinline__ void op_bwd_chance(const Ctx& c, const Op& op, int p, int mode) {
+  op_bwd_chance_t<false>(c, op, p, mode);
 }
 
 // ---------------------------------------------------------------------------
@@ -632,8 +666,69 @@ __device__ __noinline__ void run_pass_multi(Ctx* cs, int K, unsigned active, int
   }
 }
 
+// One pass of one spot whose CTA (or grid) has few items per step: node ops
+// are split over the warps a step leaves idle, in interleaved 32-column
+// blocks.  Each hand's arithmetic is that of run_pass_multi; only the warp
+// that runs it differs.
+__device__ __noinline__ void run_pass_split(const Ctx& c, int p, const Discount dc, int mode) {
+  const SpotDev& sp = *c.sp;
+  const Step* steps = sp.steps[p];
+  const int o = p ^ 1;
+  const int warp = threadIdx.x >> 5, nw0 = blockDim.x >> 5;
+  const int nw = c.grid ? gridDim.x * nw0 : nw0;
+  const int gw = c.grid ? blockIdx.x * nw0 + warp : warp;
+  const int nb = c.grid ? gridDim.x * c.bufs : c.bufs;
+  const int gb = c.grid ? blockIdx.x * c.bufs + warp : warp;
+  const bool gen = c.owner >= 0 || c.signed_reach || c.bgrad || c.breach;
+  for (int s = 0; s < sp.nsteps[p]; ++s) {
+    const Step st = steps[s];
+    const int ng = st.n_groups, ne = st.n_elem;
+    if (warp < c.bufs)
+      for (int j = gb; j < ng; j += nb) {
+        const Op* lead = sp.ops[p] + st.begin + st.n_elem + sp.groups[p][st.gbegin + j];
+        if (gen)
+          warp_terms<true>(c, lead, lead->na, p);
+        else
+          warp_terms<false>(c, lead, lead->na, p);
+      }
+    const int busy = min(ng, nb);
+    const int P = ne > 0 ? max(1, min(8, (nw - busy) / ne)) : 1;
+    const int start = busy % nw;
+    Ctx cw = c;
+    cw.parts = P;
+    for (int i = (gw - start + nw) % nw; i < ne * P; i += nw) {
+      const Op op = sp.ops[p][st.begin + i / P];
+      cw.part = i % P;
+      switch (op.type) {
+        case OP_FWD_OPP: op_fwd_opp_t<true>(cw, op, o, mode); break;
+        case OP_FWD_CHANCE: op_fwd_chance_t<true>(cw, op, o); break;
+        case OP_BWD_TRAV: op_bwd_trav_t<true>(cw, op, p, dc, mode); break;
+        case OP_BWD_OPP: op_bwd_opp_t<true>(cw, op, p, mode); break;
+        case OP_BWD_CHANCE: op_bwd_chance_t<true>(cw, op, p, mode); break;
+        default: break;
+      }
+    }
+    step_barrier(c);
+  }
+}
+
 __device__ void run_pass(const Ctx& c, int p, const Discount dc, int mode) {
-  run_pass_multi(const_cast<Ctx*>(&c), 1, 1u, p, dc, mode);
+  if (c.split)
+    run_pass_split(c, p, dc, mode);
+  else
+    run_pass_multi(const_cast<Ctx*>(&c), 1, 1u, p, dc, mode);
+}
+
+// run_pass_multi; in the SPLIT instantiation of k_solve (launches whose CTAs
+// each hold a lone spot), run_pass_split for K == 1.  Batches run the plain
+// instantiation, whose code never reaches the split functions.
+template <bool SPLIT>
+__device__ __forceinline__ void pass_multi(Ctx* cs, int K, unsigned active, int p, const Discount dc, int mode) {
+  if (SPLIT && K == 1) {
+    if (active & 1u) run_pass_split(cs[0], p, dc, mode);
+  } else {
+    run_pass_multi(cs, K, active, p, dc, mode);
+  }
 }
 
 // sum_h w[h] * v[h] accumulated in f64 (utility.rs:118-122), result on all threads.
@@ -668,13 +763,14 @@ __device__ double root_dot(const Ctx& c, const float* w, const float* v, int n, 
 
 // Exploitability of the active spots of cs (same as spot_exploitability,
 // passes shared by the K spots); results in out[k].
+template <bool SPLIT>
 __device__ void exploitability_multi(Ctx* cs, int K, unsigned active, float* out) {
   const Discount dz{0.f, 0.f, 0.f, 0.f};
   float mes[kMaxInst][2], cur[kMaxInst][2];
   const bool raked = cs[0].sp->raked != 0;  // an instance holds spots of one rake setting
   for (int p = 0; p < 2; ++p) {
     for (int k = 0; k < K; ++k) cs[k].root_reach = cs[k].sp->w[p ^ 1];
-    run_pass_multi(cs, K, active, p, dz, M_BR);
+    pass_multi<SPLIT>(cs, K, active, p, dz, M_BR);
     for (int k = 0; k < K; ++k)
       if (active >> k & 1u) {
         const SpotDev& sp = *cs[k].sp;
@@ -684,7 +780,7 @@ __device__ void exploitability_multi(Ctx* cs, int K, unsigned active, float* out
   if (raked)
     for (int p = 0; p < 2; ++p) {
       for (int k = 0; k < K; ++k) cs[k].root_reach = cs[k].sp->w[p ^ 1];
-      run_pass_multi(cs, K, active, p, dz, M_AVG);
+      pass_multi<SPLIT>(cs, K, active, p, dz, M_AVG);
       for (int k = 0; k < K; ++k)
         if (active >> k & 1u) {
           const SpotDev& sp = *cs[k].sp;
@@ -696,10 +792,11 @@ __device__ void exploitability_multi(Ctx* cs, int K, unsigned active, float* out
       out[k] = raked ? ((mes[k][0] - cur[k][0]) + (mes[k][1] - cur[k][1])) * 0.5f : (mes[k][0] + mes[k][1]) * 0.5f;
 }
 
+template <bool SPLIT>
 __device__ void dcfr_iteration_multi(Ctx* cs, int K, unsigned active, const Discount dc) {
   for (int p = 0; p < 2; ++p) {  // alternating updates (solver.rs:144-155)
     for (int k = 0; k < K; ++k) cs[k].root_reach = cs[k].sp->w[p ^ 1];
-    run_pass_multi(cs, K, active, p, dc, M_DCFR);
+    pass_multi<SPLIT>(cs, K, active, p, dc, M_DCFR);
   }
 }
 
@@ -753,6 +850,9 @@ __device__ bool bind_ctx(Ctx& c, const SpotDev* sp, float* scratch, size_t scrat
   const int warp_id = threadIdx.x >> 5;
   c.buf = warp_id < plan.bufs ? reinterpret_cast<float*>(p) + (size_t)warp_id * 3 * plan.vstride : nullptr;
   c.bufs = plan.bufs;
+  c.split = plan.split;
+  c.part = 0;
+  c.parts = 1;
   p += (size_t)plan.bufs * 3 * plan.vstride * 4;
   c.red = reinterpret_cast<double*>(p);
   if ((size_t)sp->num_slots * sp->vstride > scratch_floats || sp->vstride > plan.vstride) {
@@ -800,6 +900,7 @@ __device__ bool bind_ctx(Ctx& c, const SpotDev* sp, float* scratch, size_t scrat
 // shape) from `counter` and run job's work on them (SolveJob): the full
 // reference solve loop (solver.rs:108-176) per spot, or a fixed iteration
 // range, then the optional average-strategy epilogue.
+template <bool SPLIT>
 __global__ void PS_SOLVE_BOUNDS k_solve(const SpotDev* __restrict__ spots, int ninst, int K,
                                         const int* __restrict__ inst, int* counter, const Discount* __restrict__ disc,
                                         SolveJob job, const float* __restrict__ target, float* scratch,
@@ -850,7 +951,7 @@ __global__ void PS_SOLVE_BOUNDS k_solve(const SpotDev* __restrict__ spots, int n
           cs[k].root_reach = pass < 2 ? cs[k].sp->w[p ^ 1] : cs[k].sp->adj_g[p ^ 1];
           cs[k].owner = pass < 2 ? -1 : (p ^ 1);
         }
-        run_pass_multi(cs, K, active, p, dz, M_AVG);
+        pass_multi<SPLIT>(cs, K, active, p, dz, M_AVG);
         for (int k = 0; k < K; ++k) {
           if (!(active >> k & 1u)) continue;
           const SpotDev& sp = *cs[k].sp;
@@ -869,14 +970,14 @@ __global__ void PS_SOLVE_BOUNDS k_solve(const SpotDev* __restrict__ spots, int n
       // || t+1 == max_iter: expl = exploitability }; a spot leaves the lockstep
       // set at the first check that meets its target
       const int max_iter = job.t1;
-      exploitability_multi(cs, K, active, expl);
+      exploitability_multi<SPLIT>(cs, K, active, expl);
       unsigned live = 0;
       for (int k = 0; k < K; ++k)
         if ((active >> k & 1u) && !(expl[k] <= tgt[k])) live |= 1u << k;
       for (t = 0; t < max_iter && live; ++t) {
-        dcfr_iteration_multi(cs, K, live, disc[t]);
+        dcfr_iteration_multi<SPLIT>(cs, K, live, disc[t]);
         if ((t + 1) % 5 == 0 || t + 1 == max_iter) {
-          exploitability_multi(cs, K, live, expl);
+          exploitability_multi<SPLIT>(cs, K, live, expl);
           for (int k = 0; k < K; ++k)
             if ((live >> k & 1u) && expl[k] <= tgt[k]) {
               iters[k] = t + 1;
@@ -888,9 +989,9 @@ __global__ void PS_SOLVE_BOUNDS k_solve(const SpotDev* __restrict__ spots, int n
         if (live >> k & 1u) iters[k] = t;
     } else {
       // a fixed iteration range (batch.rs:414-535 run_iterations)
-      for (; t < job.t1; ++t) dcfr_iteration_multi(cs, K, active, disc[t]);
+      for (; t < job.t1; ++t) dcfr_iteration_multi<SPLIT>(cs, K, active, disc[t]);
       for (int k = 0; k < K; ++k) iters[k] = t;
-      if (job.epilogue & EPI_EXPL) exploitability_multi(cs, K, active, expl);
+      if (job.epilogue & EPI_EXPL) exploitability_multi<SPLIT>(cs, K, active, expl);
     }
     if (threadIdx.x == 0 && (job.checks || (job.epilogue & EPI_EXPL)))
       for (int k = 0; k < K; ++k)
@@ -907,7 +1008,7 @@ __global__ void PS_SOLVE_BOUNDS k_solve(const SpotDev* __restrict__ spots, int n
     for (int k = 0; k < K; ++k) cs[k].breach = cs[k].sp->breach;
     for (int p = 0; p < 2; ++p) {
       for (int k = 0; k < K; ++k) cs[k].root_reach = cs[k].sp->w[p ^ 1];
-      run_pass_multi(cs, K, active, p, dz, M_AVG);
+      pass_multi<SPLIT>(cs, K, active, p, dz, M_AVG);
       for (int k = 0; k < K; ++k) {
         if (!(active >> k & 1u)) continue;
         const SpotDev& sp = *cs[k].sp;
@@ -1285,9 +1386,14 @@ cudaError_t launch_solve(const SpotDev* spots, int ninst, int K, const int* inst
       (job.adjoint && (job.checks || job.t1 != job.t0)))
     return cudaErrorInvalidValue;
   size_t smem = plan.total();
-  cudaError_t e = set_smem((const void*)k_solve, smem);
+  const void* fn = plan.split ? (const void*)k_solve<true> : (const void*)k_solve<false>;
+  cudaError_t e = set_smem(fn, smem);
   if (e != cudaSuccess) return e;
-  k_solve<<<grid, block, smem, s>>>(spots, ninst, K, inst, counter, disc, job, target, scratch, scratch_floats,
+  if (plan.split)
+    k_solve<true><<<grid, block, smem, s>>>(spots, ninst, K, inst, counter, disc, job, target, scratch, scratch_floats,
+                                     out_expl, out_iters, plan, err);
+  else
+    k_solve<false><<<grid, block, smem, s>>>(spots, ninst, K, inst, counter, disc, job, target, scratch, scratch_floats,
                                      out_expl, out_iters, plan, err);
   return cudaGetLastError();
 }
@@ -1429,8 +1535,8 @@ extern "C" int ps_debug_phase_cycles(unsigned long long* out, int n) {
 int solve_occupancy(int block, const SmemPlan& plan) {
   int n = 0;
   size_t smem = plan.total();
-  set_smem((const void*)k_solve, smem);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solve, block, smem) != cudaSuccess) return 1;
+  set_smem((const void*)k_solve<false>, smem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solve<false>, block, smem) != cudaSuccess) return 1;
   return n < 1 ? 1 : n;
 }
 

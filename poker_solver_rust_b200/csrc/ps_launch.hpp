@@ -28,6 +28,8 @@ struct SmemPlan {
   int warps;    // warps per CTA
   int bufs;     // warps 0 .. bufs-1 own a terminal scan buffer and evaluate the terminal runs
   int tables;   // bytes reserved for staged board tables (0 = tables stay in global memory)
+  int split = 0; // 1: a lone spot's node ops may be split over idle warps (launches with fewer spots
+                 // than SMs and grid mode, where latency is not hidden by other CTAs; same results)
   __host__ __device__ size_t total() const {
     return (size_t)tables + (size_t)bufs * 3 * vstride * 4 + 32 * 8;
   }
