@@ -459,7 +459,7 @@ def test_grid_mode_matches_single_cta(monkeypatch):
     arithmetic of each item does not depend on which warp runs it, so the
     state matches the one-CTA run bit for bit."""
     r, b, t = spots.turn_spot(8, weights=_sparse)
-    grid = spots.product_game(r, b, t)            # default: grid mode for trees >= 2000 nodes
+    grid = spots.product_game(r, b, t)            # default: grid mode for single trees >= 16 nodes
     assert grid.num_nodes() >= 2000
     monkeypatch.setenv("PS_GRID_NODES", "0")
     one = spots.product_game(r, b, t)
