@@ -39,10 +39,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         obj = os.path.join(OUT_DIR, src.replace(".", "_") + ".o")
         cmd = [NVCC, *ARCH, "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
                "-Xcompiler", "-ffp-contract=off", "-c", os.path.join(CSRC, src), "-o", obj]
-        if src.endswith(".cu"):
-            cmd[1:1] = ["-Xptxas", "-v"] if verbose else []
-        else:
-            cmd += ["-x", "cu"] if False else []
+        if src.endswith(".cu") and verbose:
+            cmd[1:1] = ["-Xptxas", "-v"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
