@@ -480,14 +480,17 @@ def _pack_configs(card_configs, tree_configs):
         col(traw, N.PsTreeConfig, f, np.float64)[:, 0] = [float(getattr(t, f)) for t in T]
     col(traw, N.PsTreeConfig, "max_bets", np.int32)[:, 0] = [int(t.max_bets) for t in T]
     sizes = col(traw, N.PsTreeConfig, "bet_sizes", np.uint64, 12)
-    menus = {}  # the per-street menus of one TreeConfig are usually shared objects
-    for i, t in enumerate(T):
-        key = (id(t.flop_bet_sizes), id(t.turn_bet_sizes), id(t.river_bet_sizes))
+    menus = {}  # menu strings of a spot -> their 12 addresses (spots share a few menus)
+    rows = []
+    for t in T:
+        key = tuple(s for st in (t.flop_bet_sizes, t.turn_bet_sizes, t.river_bet_sizes)
+                    for p in range(2) for s in (st[p].bet, st[p].raise_))
         row = menus.get(key)
         if row is None:
-            row = menus[key] = [addr(s) for st in (t.flop_bet_sizes, t.turn_bet_sizes, t.river_bet_sizes)
-                                for p in range(2) for s in (st[p].bet, st[p].raise_)]
-        sizes[i] = row
+            row = menus[key] = [addr(s) for s in key]
+        rows.append(row)
+    if n:
+        sizes[:] = np.asarray(rows, np.uint64)
     donk = col(traw, N.PsTreeConfig, "donk_sizes", np.uint64, 2)
     donk[:, 0] = [addr(t.turn_donk_sizes) for t in T]
     donk[:, 1] = [addr(t.river_donk_sizes) for t in T]
