@@ -391,12 +391,15 @@ bool Game::check_cards(std::string& err) {  // interpreter.rs:542-662
   for (int p = 0; p < 2; ++p) {
     cards[p].clear();
     w[p].clear();
+    cards[p].reserve(1326);
+    w[p].reserve(1326);
+    int k = 0;  // pair_index(c1, c2) in this loop order
     for (int c1 = 0; c1 < 52; ++c1)
-      for (int c2 = c1 + 1; c2 < 52; ++c2) {
-        float x = range[p][pair_index(c1, c2)];
-        pos[p][pair_index(c1, c2)] = -1;
+      for (int c2 = c1 + 1; c2 < 52; ++c2, ++k) {
+        const float x = range[p][k];
+        pos[p][k] = -1;
         if (x > 0.0f && !(dead & ((1ull << c1) | (1ull << c2)))) {
-          pos[p][pair_index(c1, c2)] = (int)cards[p].size();
+          pos[p][k] = (int)cards[p].size();
           cards[p].push_back({(uint8_t)c1, (uint8_t)c2});
           w[p].push_back(x);
         }
