@@ -389,6 +389,24 @@ __device__ __forceinline__ void board_tables(const Ctx& c, int b, Tables& t) {
 // GEN = false is the copy the solve passes use (non-negative reach, the
 // traverser's own payoffs, no boundary gradients); GEN = true adds what the
 // average-strategy passes of root_cfvalues_with_reach and the adjoint need.
+// Raked showdown (evaluation.rs:429-537) and depth-boundary (:544-605) values
+// of one hand, out of line: the solve loop of unraked full trees never takes
+// them, and the per-hand loop stays small.
+__device__ __noinline__ float raked_showdown_value(float cw, float cl, float ctie, float win, float Ple, float Q1le,
+                                                   float Q2le, float Tsum, float M1, float M2, const float* rch,
+                                                   uint32_t si) {
+  const float rs = si != 0xFFFF ? rch[si] : 0.f;
+  const float tie = Ple - Q1le - Q2le;
+  const float tot = Tsum - M1 - M2;
+  return cw * win + ctie * (tie - win + rs) + cl * (tot - tie);
+}
+
+__device__ __noinline__ float boundary_value(const SpotDev& sp, const NodeDev& nd, int p, int vstride, int h,
+                                             float adj) {
+  const float bv = sp.bcfv[((size_t)nd.boundary * 2 + p) * vstride + h];
+  return __fmul_rn(__fmul_rn(bv, nd.payoff_scale), adj);
+}
+
 template <bool GEN>
 __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int p) {
   PHASE_T0(t_scan);
@@ -530,11 +548,7 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
             const float lose = (Tsum - Ple) - (M1 - Q1le) - (M2 - Q2le);
             v = __fadd_rn(__fmul_rn(cw, win), __fmul_rn(cl, lose));
           } else {
-            const uint32_t si = t.w >> 16;
-            const float rs = si != 0xFFFF ? rch[si] : 0.f;
-            const float tie = Ple - Q1le - Q2le;
-            const float tot = Tsum - M1 - M2;
-            v = cw * win + nd.amount_tie * (tie - win + rs) + cl * (tot - tie);
+            v = raked_showdown_value(cw, cl, nd.amount_tie, win, Ple, Q1le, Q2le, Tsum, M1, M2, rch, t.w >> 16);
           }
         } else {
           const uint32_t si = t.w >> 16;
@@ -545,8 +559,7 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
           } else if (GEN && adjm) {
             v = __fmul_rn(nd.payoff_scale, adj);
           } else {
-            const float bv = sp.bcfv[((size_t)nd.boundary * 2 + p) * c.vstride + h];
-            v = __fmul_rn(__fmul_rn(bv, nd.payoff_scale), adj);
+            v = boundary_value(sp, nd, p, c.vstride, h, adj);
             if (GEN && grow) grow[h] = __fmul_rn(nd.payoff_scale, adj);
           }
         }
