@@ -157,6 +157,13 @@ __device__ __forceinline__ void prefetch_l2(const float* p, int n) { prefetch_l2
 // sigma from regret matching (DCFR) or from the normalised cumulative strategy,
 // then children's reach = sigma_a * reach.  Two sweeps over the actions: the
 // first forms the denominator, the second (L1 hits) the children.
+// finalize only (M_AVG_SAVE): IP cfvalues of the node for four hands, out of line
+__device__ __noinline__ void save_ip_cfv(const SpotDev& sp, const NodeDev& nd, int h, float4 res) {
+  const float v[4] = {res.x, res.y, res.z, res.w};
+  for (int k = 0; k < 4; ++k)
+    if (h + k < sp.H[1]) sp.ipcfv[nd.ip_off + h + k] = v[k];
+}
+
 template <bool SPLIT>
 __device__ __noinline__ void op_fwd_opp_t(const Ctx& c, const Op& op, int o, int mode) {
   // SPLIT: this item is column block c.part of c.parts (interleaved 32-column blocks)
@@ -274,11 +281,7 @@ __device__ __noinline__ void op_bwd_trav_t(const Ctx& c, const Op& op, int p, co
       }
     }
     st4(dst + h, res);
-    if (mode == M_AVG_SAVE && p == 1 && nd.ip_off != 0xFFFFFFFFu) {
-      const float v[4] = {res.x, res.y, res.z, res.w};
-      for (int k = 0; k < 4; ++k)
-        if (h + k < sp.H[1]) sp.ipcfv[nd.ip_off + h + k] = v[k];
-    }
+    if (mode == M_AVG_SAVE && p == 1 && nd.ip_off != 0xFFFFFFFFu) save_ip_cfv(sp, nd, h, res);
   }
 }
 __device__ __forceinline__ void op_bwd_trav(const Ctx& c, const Op& op, int p, const Discount dc, int mode) {
@@ -302,11 +305,7 @@ __device__ __noinline__ void op_bwd_opp_t(const Ctx& c, const Op& op, int p, int
     float4 res = ld4(cb + h);
     for (int a = 1; a < na; ++a) res = add4(res, ld4(cb + (size_t)a * c.vstride + h));
     st4(dst + h, res);
-    if (mode == M_AVG_SAVE && p == 1 && nd.ip_off != 0xFFFFFFFFu) {
-      const float v[4] = {res.x, res.y, res.z, res.w};
-      for (int k = 0; k < 4; ++k)
-        if (h + k < sp.H[1]) sp.ipcfv[nd.ip_off + h + k] = v[k];
-    }
+    if (mode == M_AVG_SAVE && p == 1 && nd.ip_off != 0xFFFFFFFFu) save_ip_cfv(sp, nd, h, res);
   }
 }
 __device__ __forceinline__ void op_bwd_opp(const Ctx& c, const Op& op, int p, int mode) {
