@@ -388,9 +388,8 @@ __device__ __forceinline__ void board_tables(const Ctx& c, int b, Tables& t) {
 // GEN = false is the copy the solve passes use (non-negative reach, the
 // traverser's own payoffs, no boundary gradients); GEN = true adds what the
 // average-strategy passes of root_cfvalues_with_reach and the adjoint need.
-// Raked showdown (evaluation.rs:429-537) and depth-boundary (:544-605) values
-// of one hand, out of line: the solve loop of unraked full trees never takes
-// them, and the per-hand loop stays small.
+// Raked showdown value of one hand (evaluation.rs:429-537), out of line: the
+// solve loop of unraked trees never takes it, and the per-hand loop stays small.
 __device__ __noinline__ float raked_showdown_value(float cw, float cl, float ctie, float win, float Ple, float Q1le,
                                                    float Q2le, float Tsum, float M1, float M2, const float* rch,
                                                    uint32_t si) {
@@ -400,12 +399,10 @@ __device__ __noinline__ float raked_showdown_value(float cw, float cl, float cti
   return cw * win + ctie * (tie - win + rs) + cl * (tot - tie);
 }
 
-__device__ __noinline__ float boundary_value(const SpotDev& sp, const NodeDev& nd, int p, int vstride, int h,
-                                             float adj) {
-  const float bv = sp.bcfv[((size_t)nd.boundary * 2 + p) * vstride + h];
-  return __fmul_rn(__fmul_rn(bv, nd.payoff_scale), adj);
-}
 
+#ifndef PS_GATHER_U
+#define PS_GATHER_U 2  // groups of four entries each lane gathers per round (2 measured best of 1-4)
+#endif
 template <bool GEN>
 __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int p) {
   PHASE_T0(t_scan);
@@ -433,25 +430,26 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
   const bool bits = GEN && (bw != nullptr || c.signed_reach != 0);
   {  // 1. gather
     const int n4 = (n3 + 3) >> 2;  // groups of four entries
-    for (int w0 = lane; w0 < n4; w0 += 32 * 4) {
-      uint2 ix[4];
-      uint32_t hb[4];
+    constexpr int kU = PS_GATHER_U;
+    for (int w0 = lane; w0 < n4; w0 += 32 * kU) {
+      uint2 ix[kU];
+      uint32_t hb[kU];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < kU; ++u) {
         const int w = w0 + 32 * u;
         ix[u] = w < n4 ? *reinterpret_cast<const uint2*>(g + 4 * w) : make_uint2(0u, 0u);
         hb[u] = w < n4 ? hd[w >> 3] >> ((4 * w) & 31) : 0u;
       }
-      float x[4][4];
+      float x[kU][4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < kU; ++u) {
         const int k = 4 * (w0 + 32 * u);
         const uint32_t id[4] = {ix[u].x & 0xFFFFu, ix[u].x >> 16, ix[u].y & 0xFFFFu, ix[u].y >> 16};
 #pragma unroll
         for (int e = 0; e < 4; ++e) x[u][e] = k + e < n3 ? (GEN && bw ? rch[id[e]] * bw[id[e]] : rch[id[e]]) : 0.f;
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < kU; ++u) {
         const int k = 4 * (w0 + 32 * u);
         if (k >= n3) continue;
         const uint32_t m = bits ? 0u : hb[u];
@@ -528,6 +526,27 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
     // the next hand's record is requested before this hand's value is stored:
     // the store may alias it, so the compiler would not issue it earlier
     uint4 tn = lane < Hp ? thr[lane] : make_uint4(THR_INVALID, 0, 0, 0);
+    if (!GEN && op.term == TERM_BOUNDARY) {
+      // depth-boundary values in a loop of their own, which keeps the fold /
+      // showdown loop of full trees small (evaluation.rs:544-605)
+      const float* brow = sp.bcfv + ((size_t)nd.boundary * 2 + p) * c.vstride;
+      for (int h = lane; h < hsp; h += 32) {
+        float v = 0.f;
+        const uint4 t = tn;
+        tn = h + 32 < Hp ? thr[h + 32] : make_uint4(THR_INVALID, 0, 0, 0);
+        if (t.x != THR_INVALID && V > 0) {
+          const int s1 = t.z & 0xFFFF, s2 = t.z >> 16, n1 = t.w & 0xFF, n2 = (t.w >> 8) & 0xFF;
+          const float M1 = n1 ? cp[s1 + n1 - 1] : 0.f;
+          const float M2 = n2 ? cp[s2 + n2 - 1] : 0.f;
+          const uint32_t si = t.w >> 16;
+          const float rs = si != 0xFFFF ? rch[si] : 0.f;
+          const float adj = Tsum + rs - M1 - M2;
+          v = __fmul_rn(__fmul_rn(brow[h], nd.payoff_scale), adj);
+        }
+        dst[h] = v;
+      }
+      continue;
+    }
     for (int h = lane; h < hsp; h += 32) {
       float v = 0.f;
       const uint4 t = tn;
@@ -557,9 +576,10 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
             v = __fmul_rn(op.fold_pl != pay ? aw : al, adj);
           } else if (GEN && adjm) {
             v = __fmul_rn(nd.payoff_scale, adj);
-          } else {
-            v = boundary_value(sp, nd, p, c.vstride, h, adj);
-            if (GEN && grow) grow[h] = __fmul_rn(nd.payoff_scale, adj);
+          } else if (GEN) {  // boundary values of the general passes (solve passes loop above)
+            const float bv = sp.bcfv[((size_t)nd.boundary * 2 + p) * c.vstride + h];
+            v = __fmul_rn(__fmul_rn(bv, nd.payoff_scale), adj);
+            if (grow) grow[h] = __fmul_rn(nd.payoff_scale, adj);
           }
         }
       }
