@@ -377,9 +377,9 @@ bool Game::check_cards(std::string& err) {  // interpreter.rs:542-662
   if (cfg.initial_state != expected) { err = "Invalid initial state of `tree_config`"; return false; }
   for (int p = 0; p < 2; ++p) {
     bool any = false, valid = true;
-    for (int i = 0; i < 1326; ++i) {
+    for (int i = 0; i < 1326; ++i) {  // bitwise, no branches: the compiler vectorises it
       any |= range[p][i] != 0.0f;
-      valid &= range[p][i] >= 0.0f && range[p][i] <= 1.0f;
+      valid &= (range[p][i] >= 0.0f) & (range[p][i] <= 1.0f);
     }
     if (!any) { err = p == 0 ? "OOP range is empty" : "IP range is empty"; return false; }
     if (!valid) { err = p == 0 ? "OOP range is invalid" : "IP range is invalid"; return false; }
@@ -387,32 +387,36 @@ bool Game::check_cards(std::string& err) {  // interpreter.rs:542-662
   uint64_t dead = (1ull << flop[0]) | (1ull << flop[1]) | (1ull << flop[2]);
   if (turn != NOT_DEALT) dead |= 1ull << turn;
   if (river != NOT_DEALT) dead |= 1ull << river;
+  // the hand lists are written without branches (every combo is stored at
+  // the running count, which advances only for a kept hand): a range's zero
+  // weights follow no pattern the branch predictor could learn
   int pos[2][1326];
   for (int p = 0; p < 2; ++p) {
-    cards[p].clear();
-    w[p].clear();
-    cards[p].reserve(1326);
-    w[p].reserve(1326);
-    int k = 0;  // pair_index(c1, c2) in this loop order
+    cards[p].resize(1326);
+    w[p].resize(1326);
+    std::array<uint8_t, 2>* cp = cards[p].data();
+    float* wp = w[p].data();
+    int k = 0, m = 0;  // k = pair_index(c1, c2) in this loop order, m = hands kept
     for (int c1 = 0; c1 < 52; ++c1)
       for (int c2 = c1 + 1; c2 < 52; ++c2, ++k) {
         const float x = range[p][k];
-        pos[p][k] = -1;
-        if (x > 0.0f && !(dead & ((1ull << c1) | (1ull << c2)))) {
-          pos[p][k] = (int)cards[p].size();
-          cards[p].push_back({(uint8_t)c1, (uint8_t)c2});
-          w[p].push_back(x);
-        }
+        const int keep = (x > 0.0f) & ((dead & ((1ull << c1) | (1ull << c2))) == 0);
+        cp[m] = {(uint8_t)c1, (uint8_t)c2};
+        wp[m] = x;
+        pos[p][k] = keep ? m : -1;
+        m += keep;
       }
-    H[p] = (int)cards[p].size();
+    cards[p].resize(m);
+    w[p].resize(m);
+    H[p] = m;
     hs[p] = (H[p] + 3) & ~3;
   }
   vstride = (std::max(hs[0], hs[1]) + 31) & ~31;
   for (int p = 0; p < 2; ++p) {
-    same[p].assign(H[p], 0xFFFF);
+    same[p].resize(H[p]);
     for (int i = 0; i < H[p]; ++i) {
-      int q = pos[p ^ 1][pair_index(cards[p][i][0], cards[p][i][1])];
-      if (q >= 0) same[p][i] = (uint16_t)q;
+      const int q = pos[p ^ 1][pair_index(cards[p][i][0], cards[p][i][1])];
+      same[p][i] = q >= 0 ? (uint16_t)q : (uint16_t)0xFFFF;
     }
   }
   // C = sum over compatible (oop, ip) pairs of w_oop * w_ip (interpreter.rs:619-635),

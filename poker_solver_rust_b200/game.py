@@ -434,16 +434,24 @@ def hand_table() -> np.ndarray:
 # ---- batched datagen path ----
 def _pack_configs(card_configs, tree_configs):
     """ps_card_config / ps_tree_config arrays for n spots, filled column by
-    column through numpy views at the structs' field offsets: the ranges are
-    stacked into one array and every distinct bet-size string is encoded once.
-    Returns the two ctypes arrays and the objects they point into."""
+    column through numpy views at the structs' field offsets: the range
+    pointers address the ranges' own float32 arrays (a range held in another
+    form is converted once), and every distinct bet-size string is encoded
+    once. Returns the two ctypes arrays and the objects they point into."""
     n = len(card_configs)
     cc = (N.PsCardConfig * n)()
     tc = (N.PsTreeConfig * n)()
-    ranges = np.empty((n, 2, 1326), np.float32)
-    for i, c in enumerate(card_configs):
-        ranges[i, 0] = c.range[0].raw_data()
-        ranges[i, 1] = c.range[1].raw_data()
+    f32 = np.dtype(np.float32)
+    addrs, converted = [], []
+    for c in card_configs:
+        for r in c.range:
+            d = r.raw_data()
+            if type(d) is not np.ndarray or d.dtype != f32 or d.shape != (1326,) or not d.flags.c_contiguous:
+                d = np.ascontiguousarray(d, np.float32)
+                if d.shape != (1326,):
+                    raise ValueError("a range holds 1326 weights")
+                converted.append(d)
+            addrs.append(d.__array_interface__["data"][0])
     craw = np.frombuffer(cc, np.uint8).reshape(n, C.sizeof(N.PsCardConfig))
     traw = np.frombuffer(tc, np.uint8).reshape(n, C.sizeof(N.PsTreeConfig))
 
@@ -451,10 +459,8 @@ def _pack_configs(card_configs, tree_configs):
         off = getattr(struct, field).offset
         return raw[:, off:off + np.dtype(dtype).itemsize * count].view(dtype)
 
-    base = ranges.ctypes.data
-    ptrs = col(craw, N.PsCardConfig, "range", np.uint64, 2)
-    ptrs[:, 0] = base + np.arange(n, dtype=np.uint64) * (2 * 1326 * 4)
-    ptrs[:, 1] = ptrs[:, 0] + 1326 * 4
+    if n:
+        col(craw, N.PsCardConfig, "range", np.uint64, 2)[:] = np.asarray(addrs, np.uint64).reshape(n, 2)
     cards = np.array([[c.flop[0], c.flop[1], c.flop[2], c.turn, c.river] for c in card_configs], np.uint8)
     col(craw, N.PsCardConfig, "flop", np.uint8, 3)[:] = cards[:, :3]
     col(craw, N.PsCardConfig, "turn", np.uint8)[:, 0] = cards[:, 3]
@@ -494,7 +500,7 @@ def _pack_configs(card_configs, tree_configs):
     donk = col(traw, N.PsTreeConfig, "donk_sizes", np.uint64, 2)
     donk[:, 0] = [addr(t.turn_donk_sizes) for t in T]
     donk[:, 1] = [addr(t.river_donk_sizes) for t in T]
-    return cc, tc, (ranges, strings, menus, T)
+    return cc, tc, (card_configs, converted, strings, menus, T)
 
 
 def _is_cuda_tensor(x) -> bool:

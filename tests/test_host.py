@@ -143,3 +143,27 @@ def test_config_errors():
     with pytest.raises(ps.SolverError) as ei:
         g.allocate_memory(True)
     assert ei.value.code == N.PS_ERR_UNSUPPORTED
+
+
+def test_batch_config_packing_points_at_ranges():
+    """The batch's card configs address each range's own float32 weights; a
+    range held in another dtype is converted, and a wrong length is refused."""
+    import ctypes as C
+
+    from poker_solver_rust_b200 import game as G
+
+    work = spots.datagen_spots(6, seed=3)
+    cc = [spots.card_config(r, b) for r, b, _ in work]
+    tcs = [t for _, _, t in work]
+    cc[2].range[1].data = cc[2].range[1].data.astype(np.float64)  # converted on packing
+    a, _, keep = G._pack_configs(cc, tcs)
+    for i, c in enumerate(cc):
+        for p in range(2):
+            got = np.ctypeslib.as_array(C.cast(a[i].range[p], C.POINTER(C.c_float)), (1326,))
+            assert np.array_equal(got, np.asarray(c.range[p].data, np.float32))
+            if (i, p) != (2, 1):
+                assert C.cast(a[i].range[p], C.c_void_p).value == c.range[p].data.ctypes.data
+        assert list(a[i].flop) == list(c.flop) and a[i].turn == c.turn and a[i].river == c.river
+    cc[0].range[0].data = np.zeros(100, np.float32)
+    with pytest.raises(ValueError):
+        G._pack_configs(cc, tcs)
