@@ -48,7 +48,9 @@ typedef struct ps_tree_config {
 } ps_tree_config;
 
 /* card.rs:19-32 CardConfig; ranges as range.rs:38-39 raw data (1326 weights in
- * card_pair_to_index order, each in [0, 1]); 255 = card not dealt. */
+ * card_pair_to_index order, each in [0, 1]); 255 = card not dealt.  The
+ * weights are read during ps_game_new / ps_batch_new only and may be freed
+ * when the call returns. */
 typedef struct ps_card_config {
   const float* range[2];
   uint8_t flop[3];
