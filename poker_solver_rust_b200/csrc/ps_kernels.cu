@@ -388,6 +388,9 @@ __device__ __forceinline__ void board_tables(const Ctx& c, int b, Tables& t) {
 // GEN = false is the copy the solve passes use (non-negative reach, the
 // traverser's own payoffs, no boundary gradients); GEN = true adds what the
 // average-strategy passes of root_cfvalues_with_reach and the adjoint need.
+// SPLIT (solve passes of launches whose CTAs hold a lone spot): the run is
+// part c.part of c.parts warps; each gathers and scans the whole list in its
+// own buffer and evaluates the hands of its interleaved 32-hand blocks.
 // Raked showdown value of one hand (evaluation.rs:429-537), out of line: the
 // solve loop of unraked trees never takes it, and the per-hand loop stays small.
 __device__ __noinline__ float raked_showdown_value(float cw, float cl, float ctie, float win, float Ple, float Q1le,
@@ -403,7 +406,7 @@ __device__ __noinline__ float raked_showdown_value(float cw, float cl, float cti
 #ifndef PS_GATHER_U
 #define PS_GATHER_U 2  // groups of four entries each lane gathers per round (2 measured best of 1-4)
 #endif
-template <bool GEN>
+template <bool GEN, bool SPLIT = false>
 __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int p) {
   PHASE_T0(t_scan);
   const SpotDev& sp = *c.sp;
@@ -512,6 +515,7 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
   const float* cp = buf + V;  // card-group part
   const float Tsum = V > 0 ? buf[V - 1] : 0.f;
   const int pay = adjm ? c.owner : p;  // whose payoffs the values are
+  const int h0 = SPLIT ? c.part * 32 + lane : lane, hstep = SPLIT ? 32 * c.parts : 32;
   for (int j = 0; j < n; ++j) {
     const Op& op = ops[j];
     const NodeDev& nd = sp.nodes[op.node];
@@ -525,15 +529,15 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
                       : nullptr;
     // the next hand's record is requested before this hand's value is stored:
     // the store may alias it, so the compiler would not issue it earlier
-    uint4 tn = lane < Hp ? thr[lane] : make_uint4(THR_INVALID, 0, 0, 0);
+    uint4 tn = h0 < Hp ? thr[h0] : make_uint4(THR_INVALID, 0, 0, 0);
     if (!GEN && op.term == TERM_BOUNDARY) {
       // depth-boundary values in a loop of their own, which keeps the fold /
       // showdown loop of full trees small (evaluation.rs:544-605)
       const float* brow = sp.bcfv + ((size_t)nd.boundary * 2 + p) * c.vstride;
-      for (int h = lane; h < hsp; h += 32) {
+      for (int h = h0; h < hsp; h += hstep) {
         float v = 0.f;
         const uint4 t = tn;
-        tn = h + 32 < Hp ? thr[h + 32] : make_uint4(THR_INVALID, 0, 0, 0);
+        tn = h + hstep < Hp ? thr[h + hstep] : make_uint4(THR_INVALID, 0, 0, 0);
         if (t.x != THR_INVALID && V > 0) {
           const int s1 = t.z & 0xFFFF, s2 = t.z >> 16, n1 = t.w & 0xFF, n2 = (t.w >> 8) & 0xFF;
           const float M1 = n1 ? cp[s1 + n1 - 1] : 0.f;
@@ -547,10 +551,10 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
       }
       continue;
     }
-    for (int h = lane; h < hsp; h += 32) {
+    for (int h = h0; h < hsp; h += hstep) {
       float v = 0.f;
       const uint4 t = tn;
-      tn = h + 32 < Hp ? thr[h + 32] : make_uint4(THR_INVALID, 0, 0, 0);
+      tn = h + hstep < Hp ? thr[h + hstep] : make_uint4(THR_INVALID, 0, 0, 0);
       if (t.x != THR_INVALID && V > 0) {
         const int s1 = t.z & 0xFFFF, s2 = t.z >> 16, n1 = t.w & 0xFF, n2 = (t.w >> 8) & 0xFF;
         const float M1 = n1 ? cp[s1 + n1 - 1] : 0.f;
@@ -715,15 +719,29 @@ __device__ __noinline__ void run_pass_split(const Ctx& c, int p, const Discount 
   for (int s = 0; s < sp.nsteps[p]; ++s) {
     const Step st = steps[s];
     const int ng = st.n_groups, ne = st.n_elem;
-    if (warp < c.bufs)
-      for (int j = gb; j < ng; j += nb) {
-        const Op* lead = sp.ops[p] + st.begin + st.n_elem + sp.groups[p][st.gbegin + j];
-        if (gen)
-          warp_terms<true>(c, lead, lead->na, p);
-        else
-          warp_terms<false>(c, lead, lead->na, p);
+    // terminal runs of the solve passes are split over the buffer warps a
+    // step leaves idle (at most 8 parts a run)
+    const int TP = gen || ng == 0 ? 1 : max(1, min(8, nb / ng));
+    if (warp < c.bufs) {
+      if (TP == 1) {
+        for (int j = gb; j < ng; j += nb) {
+          const Op* lead = sp.ops[p] + st.begin + st.n_elem + sp.groups[p][st.gbegin + j];
+          if (gen)
+            warp_terms<true>(c, lead, lead->na, p);
+          else
+            warp_terms<false>(c, lead, lead->na, p);
+        }
+      } else {
+        Ctx cr = c;
+        cr.parts = TP;
+        for (int i = gb; i < ng * TP; i += nb) {
+          const Op* lead = sp.ops[p] + st.begin + st.n_elem + sp.groups[p][st.gbegin + i / TP];
+          cr.part = i % TP;
+          warp_terms<false, true>(cr, lead, lead->na, p);
+        }
       }
-    const int busy = min(ng, nb);
+    }
+    const int busy = min(ng * TP, nb);
     const int P = ne > 0 ? max(1, min(8, (nw - busy) / ne)) : 1;
     const int start = busy % nw;
     Ctx cw = c;
