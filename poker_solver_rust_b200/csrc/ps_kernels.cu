@@ -720,8 +720,9 @@ __device__ __noinline__ void run_pass_split(const Ctx& c, int p, const Discount 
     const Step st = steps[s];
     const int ng = st.n_groups, ne = st.n_elem;
     // terminal runs of the solve passes are split over the buffer warps a
-    // step leaves idle (at most 8 parts a run)
-    const int TP = gen || ng == 0 ? 1 : max(1, min(8, nb / ng));
+    // step leaves idle (at most 8 parts a run, and at most half the warps
+    // when the step has node ops to split as well)
+    const int TP = gen || ng == 0 ? 1 : max(1, min(8, min(nb, ne > 0 ? nw / 2 : nw) / ng));
     if (warp < c.bufs) {
       if (TP == 1) {
         for (int j = gb; j < ng; j += nb) {
