@@ -391,6 +391,10 @@ __device__ __forceinline__ void board_tables(const Ctx& c, int b, Tables& t) {
 // SPLIT (solve passes of launches whose CTAs hold a lone spot): the run is
 // part c.part of c.parts warps; each gathers and scans the whole list in its
 // own buffer and evaluates the hands of its interleaved 32-hand blocks.
+// CTA (grid mode, every warp holding a buffer): the whole CTA evaluates the
+// run in warp 0's buffer.  All warps gather, warp 0 alone scans (the same
+// chunks, so the same sums), and warp w evaluates hand blocks w, w + W, ...;
+// every thread of the CTA calls it for the same runs.
 // Raked showdown value of one hand (evaluation.rs:429-537), out of line: the
 // solve loop of unraked trees never takes it, and the per-hand loop stays small.
 __device__ __noinline__ float raked_showdown_value(float cw, float cl, float ctie, float win, float Ple, float Q1le,
@@ -406,8 +410,9 @@ __device__ __noinline__ float raked_showdown_value(float cw, float cl, float cti
 #ifndef PS_GATHER_U
 #define PS_GATHER_U 2  // groups of four entries each lane gathers per round (2 measured best of 1-4)
 #endif
-template <bool GEN, bool SPLIT = false>
+template <bool GEN, bool SPLIT = false, bool CTA = false>
 __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int p) {
+  static_assert(!CTA || (SPLIT && !GEN), "CTA runs are solve-pass runs of lone spots");
   PHASE_T0(t_scan);
   const SpotDev& sp = *c.sp;
   const int o = p ^ 1;
@@ -420,7 +425,9 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
   const uint32_t* hd = T.heads[o];
   const float* rch = slot_in(c, ops[0].src);
   prefetch_l2_bytes(T.thr[p], 16 * Hp);
-  float* buf = c.buf;
+  const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  // warp 0's buffer: buffers are 3 * vstride floats apart (one spot a launch)
+  float* buf = CTA ? c.buf - (size_t)warp * 3 * c.vstride : c.buf;
   // adjoint pass at a depth boundary: the reach is weighted by the payoff
   // owner's boundary values.  Where the gathered values may be negative
   // (caller-given reach, boundary weights) segment starts come from the
@@ -434,7 +441,7 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
   {  // 1. gather
     const int n4 = (n3 + 3) >> 2;  // groups of four entries
     constexpr int kU = PS_GATHER_U;
-    for (int w0 = lane; w0 < n4; w0 += 32 * kU) {
+    for (int w0 = (CTA ? warp * 32 * kU : 0) + lane; w0 < n4; w0 += 32 * kU * (CTA ? nwarps : 1)) {
       uint2 ix[kU];
       uint32_t hb[kU];
 #pragma unroll
@@ -465,8 +472,11 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
       }
     }
   }
-  __syncwarp();
-  {  // 2. chunked segmented scan
+  if (CTA)
+    __syncthreads();
+  else
+    __syncwarp();
+  if (!CTA || warp == 0) {  // 2. chunked segmented scan
     const int C = ((n3 + 31) >> 5) | 1;
     const int lo = min(lane * C, n3), hi = min(lo + C, n3);
     float run = 0.f;
@@ -503,7 +513,10 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
     if (lane == 0) in = 0.f;
     for (int j = lo; j < first; ++j) buf[j] = __fadd_rn(buf[j], in);
   }
-  __syncwarp();
+  if (CTA)
+    __syncthreads();
+  else
+    __syncwarp();
   PHASE_ADD(PH_SCAN, t_scan);
   PHASE_T0(t_look);
   if (GEN && c.breach && ops[0].term == TERM_BOUNDARY && !adjm) {  // the opponent's reach at this boundary
@@ -515,7 +528,8 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
   const float* cp = buf + V;  // card-group part
   const float Tsum = V > 0 ? buf[V - 1] : 0.f;
   const int pay = adjm ? c.owner : p;  // whose payoffs the values are
-  const int h0 = SPLIT ? c.part * 32 + lane : lane, hstep = SPLIT ? 32 * c.parts : 32;
+  const int part = CTA ? warp : SPLIT ? c.part : 0, parts = CTA ? nwarps : SPLIT ? c.parts : 1;
+  const int h0 = part * 32 + lane, hstep = 32 * parts;
   for (int j = 0; j < n; ++j) {
     const Op& op = ops[j];
     const NodeDev& nd = sp.nodes[op.node];
@@ -596,7 +610,10 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
     const float inv = __fdiv_rn(1.0f, nd0.path_scale);
     for (int h = lane; h < sp.H[c.owner]; h += 32) grow[h] = __fmul_rn(__fmul_rn(grow[h], rch[h]), inv);
   }
-  __syncwarp();  // the buffer is free for this warp's next run
+  if (CTA)
+    __syncthreads();  // the buffer is free for the CTA's next run
+  else
+    __syncwarp();  // the buffer is free for this warp's next run
   PHASE_ADD(PH_LOOKUP, t_look);
 }
 
@@ -722,8 +739,15 @@ __device__ __noinline__ void run_pass_split(const Ctx& c, int p, const Discount 
     // terminal runs of the solve passes are split over the buffer warps a
     // step leaves idle (at most 8 parts a run, and at most half the warps
     // when the step has node ops to split as well)
+    // grid mode with few runs: a CTA a run (CTAs 0 .. ng-1)
+    const bool cta_runs = c.grid && !gen && ng > 0 && c.bufs == nw0 && 2 * ng <= (int)gridDim.x;
     const int TP = gen || ng == 0 ? 1 : max(1, min(8, min(nb, ne > 0 ? nw / 2 : nw) / ng));
-    if (warp < c.bufs) {
+    if (cta_runs) {
+      for (int j = blockIdx.x; j < ng; j += gridDim.x) {
+        const Op* lead = sp.ops[p] + st.begin + st.n_elem + sp.groups[p][st.gbegin + j];
+        warp_terms<false, true, true>(c, lead, lead->na, p);
+      }
+    } else if (warp < c.bufs) {
       if (TP == 1) {
         for (int j = gb; j < ng; j += nb) {
           const Op* lead = sp.ops[p] + st.begin + st.n_elem + sp.groups[p][st.gbegin + j];
@@ -742,7 +766,7 @@ __device__ __noinline__ void run_pass_split(const Ctx& c, int p, const Discount 
         }
       }
     }
-    const int busy = min(ng * TP, nb);
+    const int busy = cta_runs ? ng * nw0 : min(ng * TP, nb);
     const int P = ne > 0 ? max(1, min(8, (nw - busy) / ne)) : 1;
     const int start = busy % nw;
     Ctx cw = c;
