@@ -767,7 +767,9 @@ __device__ __noinline__ void run_pass_split(const Ctx& c, int p, const Discount 
       }
     }
     const int busy = cta_runs ? ng * nw0 : min(ng * TP, nb);
-    const int P = ne > 0 ? max(1, min(8, (nw - busy) / ne)) : 1;
+    // node ops in up to 16 parts: a 1128-hand row is 282 float4 columns, so 9
+    // parts cover it in one round
+    const int P = ne > 0 ? max(1, min(16, (nw - busy) / ne)) : 1;
     const int start = busy % nw;
     Ctx cw = c;
     cw.parts = P;
