@@ -720,9 +720,10 @@ __device__ __noinline__ void run_pass_multi(Ctx* cs, int K, unsigned active, int
 }
 
 // One pass of one spot whose CTA (or grid) has few items per step: node ops
-// are split over the warps a step leaves idle, in interleaved 32-column
-// blocks.  Each hand's arithmetic is that of run_pass_multi; only the warp
-// that runs it differs.
+// and terminal runs are split over the warps a step leaves idle, in
+// interleaved 32-column (32-hand) blocks, and in grid mode a step with few
+// runs gives each a whole CTA.  Each hand's arithmetic is that of
+// run_pass_multi; only the warp that runs it differs.
 __device__ __noinline__ void run_pass_split(const Ctx& c, int p, const Discount dc, int mode) {
   const SpotDev& sp = *c.sp;
   const Step* steps = sp.steps[p];
@@ -736,10 +737,10 @@ __device__ __noinline__ void run_pass_split(const Ctx& c, int p, const Discount 
   for (int s = 0; s < sp.nsteps[p]; ++s) {
     const Step st = steps[s];
     const int ng = st.n_groups, ne = st.n_elem;
-    // terminal runs of the solve passes are split over the buffer warps a
-    // step leaves idle (at most 8 parts a run, and at most half the warps
-    // when the step has node ops to split as well)
-    // grid mode with few runs: a CTA a run (CTAs 0 .. ng-1)
+    // terminal runs of the solve passes: in grid mode with few runs, a CTA a
+    // run (CTAs 0 .. ng-1); otherwise split over the buffer warps a step
+    // leaves idle (at most 8 parts a run, and at most half the warps when the
+    // step has node ops to split as well)
     const bool cta_runs = c.grid && !gen && ng > 0 && c.bufs == nw0 && 2 * ng <= (int)gridDim.x;
     const int TP = gen || ng == 0 ? 1 : max(1, min(8, min(nb, ne > 0 ? nw / 2 : nw) / ng));
     if (cta_runs) {
