@@ -72,3 +72,26 @@ def test_reference_arm_runs_on_rank_zero_only(capsys):
     args = argparse.Namespace(warmup=3, steps=1, ref_spots=1, spots=4096, seed=7)
     assert bench.run_reference(args, rank=1, world=2) is None
     assert capsys.readouterr().out == ""
+
+
+def test_reference_arm_prints_contract_line(capsys):
+    """Rank 0 of the reference arm times the oracle port on the host cores and
+    prints one JSON line with the contract's keys, its cpu_baseline and an e2e
+    equal to its own value (no device copies)."""
+    sys.path.insert(0, ROOT)
+    import argparse
+    import json
+
+    import bench
+
+    args = argparse.Namespace(warmup=1, steps=1, ref_spots=1, spots=4096, seed=7)
+    bench.run_reference(args, rank=0, world=1)
+    lines = [ln for ln in capsys.readouterr().out.splitlines() if ln.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+              "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["value"] > 0 and d["higher_is_better"] is True
+    assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["kind"] == "port"
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
