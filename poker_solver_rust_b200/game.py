@@ -489,8 +489,10 @@ def _pack_configs(card_configs, tree_configs):
     menus = {}  # menu strings of a spot -> their 12 addresses (spots share a few menus)
     rows = []
     for t in T:
-        key = tuple(s for st in (t.flop_bet_sizes, t.turn_bet_sizes, t.river_bet_sizes)
-                    for p in range(2) for s in (st[p].bet, st[p].raise_))
+        f, u, r = t.flop_bet_sizes, t.turn_bet_sizes, t.river_bet_sizes
+        f0, f1, u0, u1, r0, r1 = f[0], f[1], u[0], u[1], r[0], r[1]
+        key = (f0.bet, f0.raise_, f1.bet, f1.raise_, u0.bet, u0.raise_, u1.bet, u1.raise_,
+               r0.bet, r0.raise_, r1.bet, r1.raise_)  # street-major, then player, then bet / raise
         row = menus.get(key)
         if row is None:
             row = menus[key] = [addr(s) for s in key]

@@ -156,7 +156,7 @@ def test_batch_config_packing_points_at_ranges():
     cc = [spots.card_config(r, b) for r, b, _ in work]
     tcs = [t for _, _, t in work]
     cc[2].range[1].data = cc[2].range[1].data.astype(np.float64)  # converted on packing
-    a, _, keep = G._pack_configs(cc, tcs)
+    a, b, keep = G._pack_configs(cc, tcs)
     for i, c in enumerate(cc):
         for p in range(2):
             got = np.ctypeslib.as_array(C.cast(a[i].range[p], C.POINTER(C.c_float)), (1326,))
@@ -164,6 +164,13 @@ def test_batch_config_packing_points_at_ranges():
             if (i, p) != (2, 1):
                 assert C.cast(a[i].range[p], C.c_void_p).value == c.range[p].data.ctypes.data
         assert list(a[i].flop) == list(c.flop) and a[i].turn == c.turn and a[i].river == c.river
+        t, pt = tcs[i], b[i]
+        menus = [s for st in (t.flop_bet_sizes, t.turn_bet_sizes, t.river_bet_sizes)
+                 for q in range(2) for s in (st[q].bet, st[q].raise_)]
+        assert [None if x is None else x.decode() for x in pt.bet_sizes] == menus
+        assert (pt.starting_pot, pt.effective_stack) == (t.starting_pot, t.effective_stack)
+        assert pt.initial_state == int(t.initial_state) and pt.max_bets == int(t.max_bets)
+        assert (pt.rake_rate, pt.rake_cap) == (float(t.rake_rate), float(t.rake_cap))
     cc[0].range[0].data = np.zeros(100, np.float32)
     with pytest.raises(ValueError):
         G._pack_configs(cc, tcs)
