@@ -165,12 +165,12 @@ def turn_game_measure(ps, spots, iters: int, cpu_iters: int):
         try:
             o = spots.oracle_game(r, b, t)
             t0 = time.perf_counter()
-            for it in range(cpu_iters):
-                o.solve_step(it)
+            o.solve(cpu_iters, 0.0)  # the same loop as the GPU side: checks every 5 iterations, finalize
             out["cpu_ms_per_iteration"] = (time.perf_counter() - t0) / cpu_iters * 1e3
         finally:
             O.set_chance_threads(1)
         out["cpu"] = {"threads": threads, "kind": "port", "iterations_timed": cpu_iters,
+                      "note": "solve(): exploitability every 5 iterations and finalize, as the GPU side",
                       "parallel": "the 48 river chance children of each chance node, as solver.rs:264-326 with rayon"}
     return out
 
@@ -178,11 +178,13 @@ def turn_game_measure(ps, spots, iters: int, cpu_iters: int):
 def river_game_measure(ps, spots, iters: int, cpu_iters: int):
     """One plain river subgame (5-card board, U[0,1] ranges masked by the
     board, pot 100, stack 200, bets 50% / 100% / all-in, raise 100%) solved
-    for `iters` iterations through ps.solve on one CTA (a river game is
-    latency-bound: iterations/s and the exploitability reached), beside the
-    oracle on one host thread (river nodes never parallelise in the
-    reference, node.rs:347-349).  The tree has no bet cap: the reference's
-    tree builder has none, so both sides solve the same tree."""
+    for `iters` iterations through ps.solve in grid mode (one cooperative
+    launch over every SM; a single river game is latency-bound, so the line
+    gives iterations/s and the exploitability reached), beside the oracle on
+    one host thread (river nodes never parallelise in the reference,
+    node.rs:347-349), timed through the same solve loop (checks every 5
+    iterations, finalize).  The tree has no bet cap: the reference's tree
+    builder has none, so both sides solve the same tree."""
     import torch
 
     r, b, t = spots.river_spot(1)
@@ -203,10 +205,10 @@ def river_game_measure(ps, spots, iters: int, cpu_iters: int):
     if cpu_iters > 0:
         o = spots.oracle_game(r, b, t)
         t0 = time.perf_counter()
-        for it in range(cpu_iters):
-            o.solve_step(it)
+        o.solve(cpu_iters, 0.0)
         out["cpu_iterations_per_s"] = cpu_iters / (time.perf_counter() - t0)
-        out["cpu"] = {"threads": 1, "kind": "port", "iterations_timed": cpu_iters}
+        out["cpu"] = {"threads": 1, "kind": "port", "iterations_timed": cpu_iters,
+                      "note": "solve(): exploitability every 5 iterations and finalize, as the GPU side"}
     return out
 
 
@@ -252,7 +254,7 @@ def turn_adjoint_measure(ps, spots, n: int, iters: int, cpu_sample: int):
                                       "by the batch and the tensors at the end"}
     if cpu_sample > 0:
         threads = os.cpu_count() or 1
-        sample = sp[:max(cpu_sample, threads)]
+        sample = sp[:min(n, CPU_SPOTS_PER_THREAD * threads)]
         items = bs.boundary_items()
 
         def one(i):
@@ -326,38 +328,52 @@ def make_workload(n_spots: int, seed: int):
     return spots.datagen_spots(n_spots, seed=seed)
 
 
+CPU_SPOTS_PER_THREAD = 16  # per timed step: enough that the last spots to finish do not set the step time
+
+
+def cpu_sample(work, step: int, threads: int, per_thread: int = CPU_SPOTS_PER_THREAD):
+    """The spots of CPU step `step`: per_thread spots per host thread, taken in
+    order from the GPU arm's own spots (wrapping around)."""
+    n = per_thread * threads
+    return [work[(step * n + i) % len(work)] for i in range(n)]
+
+
 def oracle_solve_sample(sample, threads: int):
-    """Reference CPU algorithm, one spot per host thread (spot parallelism as
-    in the reference's datagen workers).  Returns (seconds, exploitabilities)."""
+    """Reference CPU algorithm, spot-parallel: each host thread takes the next
+    spot as it finishes one (the reference's datagen workers, one game per
+    thread, pipeline.rs:111-124).  Returns (seconds, iterations per spot)."""
     from tests import spots
 
     def one(spec):
         r, b, t = spec
         g = spots.oracle_game(r, b, t)
-        return g.solve(MAX_ITER, TARGET_FRAC * t.starting_pot)
+        g.solve(MAX_ITER, TARGET_FRAC * t.starting_pot)
+        return g.iterations_run
 
     t0 = time.perf_counter()
     with ThreadPoolExecutor(max_workers=threads) as ex:
         res = list(ex.map(one, sample))
-    return time.perf_counter() - t0, res
+    return time.perf_counter() - t0, np.array(res)
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    # bounded sample per step: a few spots per host thread
-    per_step = max(threads, args.ref_spots)
-    work = make_workload(per_step * (args.warmup + args.steps), seed=args.seed)
+    # each step: a bounded sample of the GPU arm's own 4096 spots (rank 0's seed)
+    work = make_workload(args.spots, seed=args.seed)
+    spt = args.cpu_spots_per_thread
+    per_step = spt * threads
     for w in range(args.warmup):
-        oracle_solve_sample(work[w * per_step:(w + 1) * per_step], threads)
-    secs = []
+        oracle_solve_sample(cpu_sample(work, w, threads, spt), threads)
+    secs, its = [], []
     for k in range(args.steps):
-        s = (args.warmup + k) * per_step
-        dt, _ = oracle_solve_sample(work[s:s + per_step], threads)
+        dt, it = oracle_solve_sample(cpu_sample(work, args.warmup + k, threads, spt), threads)
         secs.append(dt)
+        its.append(it)
     tot = sum(secs)
     value = per_step * args.steps / tot
+    mean_it = float(np.concatenate(its).mean())
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
@@ -365,9 +381,12 @@ def run_reference(args, rank, world):
         "data": "synthetic (seeded PCG64)",
         "config": {"workload": f"batched river datagen: {args.spots} spots per GPU to <=0.3% pot or "
                                f"{MAX_ITER} iterations", "parallelism": f"host threads x{threads}",
-                   "timed_sample": f"{per_step} spots of the same workload per step"},
+                   "timed_sample": f"{per_step} spots per step ({spt} per host thread), taken in "
+                                   f"order from the GPU arm's {args.spots} spots"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{per_step} spots per step, spot-parallel on {threads} threads"},
+                         "sample": f"{per_step} spots per step ({spt} per thread) of the GPU arm's "
+                                   f"spots, spot-parallel on {threads} threads",
+                         "mean_iterations": mean_it},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -381,14 +400,15 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--spots", type=int, default=4096)
     ap.add_argument("--seed", type=int, default=7)
-    ap.add_argument("--ref-spots", type=int, default=32)
-    ap.add_argument("--cpu-sample", type=int, default=32)
+    ap.add_argument("--cpu-sample", type=int, default=1, help="0 = skip the CPU baseline leg")
+    ap.add_argument("--cpu-spots-per-thread", type=int, default=CPU_SPOTS_PER_THREAD,
+                    help="spots per host thread in each CPU step (reference arm and CPU baseline leg)")
     ap.add_argument("--plain-sample", type=int, default=32)
     ap.add_argument("--block", type=int, default=-1, help="threads per CTA; -1 = autotune, 0 = library default")
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--turn-iters", type=int, default=500, help="single turn game iterations (0 = skip)")
-    ap.add_argument("--turn-cpu-iters", type=int, default=3)
+    ap.add_argument("--turn-cpu-iters", type=int, default=50)
     ap.add_argument("--river-iters", type=int, default=1000, help="single river game iterations (0 = skip)")
     ap.add_argument("--river-cpu-iters", type=int, default=200)
     ap.add_argument("--adjoint-spots", type=int, default=1024, help="depth-limited turn spots + adjoint (0 = skip)")
@@ -492,7 +512,8 @@ def main():
             ps.solve(g, MAX_ITER, TARGET_FRAC * t.starting_pot)
         plain_s = time.perf_counter() - t0
         plain = {"value": len(sample) / plain_s, "unit": UNIT, "sample": f"first {len(sample)} spots, one "
-                 "game + single-CTA solve launch per spot, host-synchronised"}
+                 "game per spot through the single-game API (grid mode: one cooperative solve launch over every "
+                 "SM per spot), host-synchronised"}
 
     # ---- single turn game (config 2 of the spec), grid mode ----
     turn = None
@@ -515,10 +536,13 @@ def main():
     cpu = None
     if rank == 0 and args.cpu_sample > 0:
         threads = os.cpu_count() or 1
-        sample = work[:max(args.cpu_sample, threads)]
-        dt, _ = oracle_solve_sample(sample, threads)
+        sample = cpu_sample(work, 0, threads, args.cpu_spots_per_thread)
+        dt, cit = oracle_solve_sample(sample, threads)
         cpu = {"value": len(sample) / dt, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"first {len(sample)} spots of the job, spot-parallel on {threads} threads"}
+               "sample": f"first {len(sample)} spots of the job ({args.cpu_spots_per_thread} per thread), spot-parallel "
+                         f"on {threads} threads",
+               "mean_iterations": float(cit.mean()),
+               "gpu_mean_iterations_same_spots": float(iters[:len(sample)].mean())}
 
     if rank == 0:
         cfg = bs.config()

@@ -89,10 +89,14 @@ int ps_compute_exploitability(ps_game* g, float* out);
  * PS_ERR_INVALID: river trees fit with room to spare, turn trees usually do
  * not (every river subtree is live at once; 100bb turn trees with one or two
  * sizes need 10-15 Mi floats) and stay on ps_compute_exploitability.  The
- * first call on a device looks the array up, so make it before any stream
- * capture on that device.  All calls share the one array: calls whose kernels
- * overlap on the GPU (different games on different streams or threads) race
- * and must be serialised by the caller. */
+ * array is part of the library's device code: every device that loads the
+ * library reserves its 16 MiB until the process exits, whether or not this
+ * function is called.  The first call in a CUDA context looks the array up,
+ * so make it before any stream capture on that device; after a device reset
+ * (a new context) the next call looks it up again.  Each call waits for its
+ * kernel and reads the result back before it returns.  All calls share the
+ * one array: calls whose kernels overlap on the GPU (different games on
+ * different streams or threads) race and must be serialised by the caller. */
 int ps_compute_exploitability_noalloc(ps_game* g, float* out);
 /* finalize (utility.rs:348) */
 int ps_finalize(ps_game* g);
@@ -345,6 +349,17 @@ int ps_parse_bet_sizes(const char* sizes, int is_raise, int32_t* kinds, double* 
 const char* ps_last_error(void);
 int ps_hand_table(int32_t* out, int cap); /* hand_table.rs values as built here */
 int ps_discount_params(uint32_t t, float out[3]); /* solver.rs:26-44 */
+
+/* ---- test hooks (no reference counterpart) ---- */
+/* The bounded grid barrier of single-game grid mode: a cooperative launch of
+ * `ctas` CTAs (2..148) in which CTA 0 enters `rounds` grid barriers that no
+ * other CTA joins.  The first wait gives up after wait_ns nanoseconds (at most
+ * 1 s) and sets the launch's error word to 4 (a barrier gave up) and its abort
+ * word; every later barrier then returns at once.  Out: the error word, the
+ * number of barriers CTA 0 got through (0 when the abort works) and the
+ * kernel's time in ms.  No kernel of this call waits without a bound. */
+int ps_debug_grid_barrier_timeout(int32_t ctas, int32_t rounds, int64_t wait_ns, int32_t* err, int32_t* passed,
+                                  float* ms);
 
 #ifdef __cplusplus
 }

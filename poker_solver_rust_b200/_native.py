@@ -77,6 +77,7 @@ P = C.POINTER
 _sig("ps_last_error", C.c_char_p)
 _sig("ps_hand_table", i32, P(i32), i32)
 _sig("ps_discount_params", i32, u32, P(f32))
+_sig("ps_debug_grid_barrier_timeout", i32, i32, i32, i64, P(i32), P(i32), P(f32))
 _sig("ps_parse_bet_sizes", i32, C.c_char_p, i32, P(i32), P(f64), P(i32), P(i32), i32)
 _sig("ps_game_new", i32, P(PsCardConfig), P(PsTreeConfig), P(vp))
 _sig("ps_game_free", None, vp)

@@ -41,37 +41,66 @@ int fail(int code, const std::string& msg) {
   } while (0)
 
 // ---- per-device constants: hand table ----
+// Every per-device cache below remembers the id of the CUDA context it was
+// made in (current_context_id): a cudaDeviceReset destroys that context and
+// everything allocated in it, so a cache from an older context is dropped
+// (its memory is already gone) and made again in the current one.
 struct DeviceConsts {
   int device = -1;
+  unsigned long long ctx = 0;
   int32_t* table = nullptr;
   int nsm = 0;
 };
 std::mutex g_dev_mu;
 std::mutex g_tune_mu;
 
+struct CtxTag {  // where a cached allocation lives
+  int dev = -1;
+  unsigned long long ctx = 0;
+};
+cudaError_t current_tag(CtxTag* t) {
+  cudaError_t e = cudaGetDevice(&t->dev);
+  if (e != cudaSuccess) return e;
+  return current_context_id(&t->ctx);
+}
+
 // Pinned host staging buffers, kept for reuse: a batch fills one, uploads it
-// and hands it back, so back-to-back batches pay for page-locking once.
+// and hands it back, so back-to-back batches pay for page-locking once.  A
+// buffer is reused only in the context that allocated it; buffers of an
+// earlier context of the current device (ended by a device reset, which freed
+// them) are forgotten.
 struct PinnedPool {
+  struct Buf {
+    char* p;
+    size_t bytes;
+    CtxTag tag;
+  };
   std::mutex mu;
-  std::vector<std::pair<char*, size_t>> free_;
-  cudaError_t acquire(size_t bytes, char** out) {
+  std::vector<Buf> free_;
+  cudaError_t acquire(size_t bytes, char** out, CtxTag* tag) {
+    cudaError_t e = current_tag(tag);
+    if (e != cudaSuccess) return e;
     {
       std::lock_guard<std::mutex> lk(mu);
+      free_.erase(std::remove_if(free_.begin(), free_.end(),
+                                 [&](const Buf& b) { return b.tag.dev == tag->dev && b.tag.ctx != tag->ctx; }),
+                  free_.end());
       for (size_t i = 0; i < free_.size(); ++i)
-        if (free_[i].second >= bytes) {
-          *out = free_[i].first;
+        if (free_[i].bytes >= bytes && free_[i].tag.ctx == tag->ctx) {
+          *out = free_[i].p;
           free_.erase(free_.begin() + (long)i);
           return cudaSuccess;
         }
     }
     return cudaMallocHost(out, bytes);
   }
-  void release(char* p, size_t bytes) {
+  void release(char* p, size_t bytes, const CtxTag& tag) {
     std::lock_guard<std::mutex> lk(mu);
-    free_.push_back({p, bytes});
+    free_.push_back({p, bytes, tag});
     if (free_.size() > 2) {  // keep the two largest
-      std::sort(free_.begin(), free_.end(), [](const auto& a, const auto& b) { return a.second > b.second; });
-      cudaFreeHost(free_.back().first);
+      std::sort(free_.begin(), free_.end(), [](const Buf& a, const Buf& b) { return a.bytes > b.bytes; });
+      CtxTag now;
+      if (current_tag(&now) == cudaSuccess && now.ctx == free_.back().tag.ctx) cudaFreeHost(free_.back().p);
       free_.pop_back();
     }
   }
@@ -87,18 +116,32 @@ struct DeviceStaging {
   std::mutex mu;
   char* buf[16] = {};
   size_t cap[16] = {};
+  unsigned long long ctx[16] = {};
 };
 DeviceStaging g_staging;
 
+// Holds the device's staging buffer until the lease ends.  A call that fails
+// after it enqueued work on a stream waits for that stream (sync_on_release)
+// before the buffer goes to the next call.
 struct StagingLease {
   std::unique_lock<std::mutex> lk;
   char* ptr = nullptr;
+  cudaStream_t pending = nullptr;
+  bool busy = false;
   cudaError_t acquire(size_t bytes) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 16) return cudaErrorInvalidDevice;
+    unsigned long long ctx = 0;
+    e = current_context_id(&ctx);
+    if (e != cudaSuccess) return e;
     lk = std::unique_lock<std::mutex>(g_staging.mu);
+    if (g_staging.ctx[dev] != ctx) {  // a buffer of an ended context is already freed
+      g_staging.buf[dev] = nullptr;
+      g_staging.cap[dev] = 0;
+      g_staging.ctx[dev] = ctx;
+    }
     if (g_staging.cap[dev] < bytes) {
       if (g_staging.buf[dev]) cudaFree(g_staging.buf[dev]);
       g_staging.buf[dev] = nullptr;
@@ -111,6 +154,15 @@ struct StagingLease {
     ptr = g_staging.buf[dev];
     return cudaSuccess;
   }
+  // work that reads or writes the buffer is now queued on s
+  void using_stream(cudaStream_t s) {
+    pending = s;
+    busy = true;
+  }
+  void done() { busy = false; }
+  ~StagingLease() {
+    if (busy) cudaStreamSynchronize(pending);  // an error path left copies in flight
+  }
 };
 std::map<long, std::pair<int, int>> g_tune;  // autotuned (CTA size, scan-buffer warps) per
                                              // (device, hand-count class, tree-size class)
@@ -120,8 +172,11 @@ int device_consts(DeviceConsts** out) {
   int dev = 0;
   CU(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 16) return fail(PS_ERR_CUDA, "device index out of range");
+  unsigned long long ctx = 0;
+  CU(current_context_id(&ctx));
   std::lock_guard<std::mutex> lk(g_dev_mu);
   DeviceConsts& d = g_dev[dev];
+  if (d.ctx != ctx) d = DeviceConsts{};  // made in an ended context: its table is gone
   if (!d.table) {
     cudaDeviceProp prop;
     CU(cudaGetDeviceProperties(&prop, dev));
@@ -134,6 +189,7 @@ int device_consts(DeviceConsts** out) {
     CU(cudaMemcpy(d.table, t.data(), sizeof(int32_t) * kHandTableSize, cudaMemcpyHostToDevice));
     d.nsm = prop.multiProcessorCount;
     d.device = dev;
+    d.ctx = ctx;
   }
   *out = &d;
   return PS_OK;
@@ -196,6 +252,7 @@ struct Batch {
   size_t static_bytes = 0, setup_bytes = 0, state_bytes = 0, bnd_bytes = 0;
   char* h_static = nullptr;  // pinned staging of the static region (from g_pinned, during build only)
   size_t h_static_cap = 0;
+  CtxTag h_static_tag;
   SpotDev* d_spots = nullptr;
   std::vector<SpotDev> h_spots;
   int2* d_work = nullptr;
@@ -245,7 +302,7 @@ struct Batch {
   ~Batch() {
     if (stream) cudaStreamSynchronize(stream);
     cudaFree(pool);
-    if (h_static) g_pinned.release(h_static, h_static_cap);
+    if (h_static) g_pinned.release(h_static, h_static_cap, h_static_tag);
     cudaFree(d_spots);
     cudaFree(d_work);
     cudaFree(d_items);
@@ -319,7 +376,7 @@ struct Batch {
     CU(cudaMalloc(&pool, static_bytes + setup_bytes + state_bytes + bnd_bytes));
     CU(cudaMemsetAsync(pool + static_bytes + setup_bytes + state_bytes, 0, bnd_bytes, stream));
     h_static_cap = std::max<size_t>(static_bytes, 16);
-    CU(g_pinned.acquire(h_static_cap, &h_static));
+    CU(g_pinned.acquire(h_static_cap, &h_static, &h_static_tag));
     // ---- fill static ----
     h_spots.resize(n);
     std::vector<int2> work;
@@ -555,7 +612,7 @@ struct Batch {
     if (!items.empty())
       CU(cudaMemcpyAsync(d_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, stream));
     CU(cudaStreamSynchronize(stream));
-    g_pinned.release(h_static, h_static_cap);  // uploaded: the staging buffer goes back to the pool
+    g_pinned.release(h_static, h_static_cap, h_static_tag);  // uploaded: the staging buffer goes back to the pool
     h_static = nullptr;
     if (tune) return autotune(order, opts ? opts->ctas_per_sm : 0);
     return PS_OK;
@@ -1227,15 +1284,17 @@ int ps_root_cfvalues_with_reach(ps_game* G, int player, const float* opp_reach, 
   float* d_out = nullptr;
   std::vector<float> r(g.hs[o], 0.f);
   for (int h = 0; h < g.H[o]; ++h) r[h] = opp_reach ? opp_reach[h] : g.w[o][h];
+  // freed on every return (cudaFree waits for the device, so an error path
+  // never frees a buffer that queued work still reads)
   CU(cudaMalloc(&d_reach, 4 * r.size()));
+  std::unique_ptr<float, decltype(&cudaFree)> k1(d_reach, &cudaFree);
   CU(cudaMalloc(&d_out, 4 * (size_t)g.hs[player]));
+  std::unique_ptr<float, decltype(&cudaFree)> k2(d_out, &cudaFree);
   CU(cudaMemcpyAsync(d_reach, r.data(), 4 * r.size(), cudaMemcpyHostToDevice, B.stream));
   CU(cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream));
   CU(B.average(0, player, d_reach, d_out, -1, nullptr));
   CU(cudaMemcpyAsync(out, d_out, 4 * (size_t)g.H[player], cudaMemcpyDeviceToHost, B.stream));
   CU(cudaStreamSynchronize(B.stream));
-  cudaFree(d_reach);
-  cudaFree(d_out);
   return B.check_err();
 }
 
@@ -1341,12 +1400,14 @@ int ps_boundary_river_reduce(int32_t n, const uint8_t* boards, const float* pots
   cudaStream_t s = (cudaStream_t)stream;
   StagingLease lease;
   CU(lease.acquire(hb.size() + 4 * dn.size() + 16));
+  lease.using_stream(s);
   char* d = lease.ptr;
   float* d_dn = (float*)(d + ((hb.size() + 15) & ~(size_t)15));
   CU(cudaMemcpyAsync(d, hb.data(), hb.size(), cudaMemcpyHostToDevice, s));
   CU(cudaMemcpyAsync(d_dn, dn.data(), 4 * dn.size(), cudaMemcpyHostToDevice, s));
   CU(launch_boundary_river_reduce(n, (const uint8_t*)d, d_dn, net, net_bf16 ? 1 : 0, reach, hands, H, out, s));
   CU(cudaStreamSynchronize(s));
+  lease.done();
   return PS_OK;
 }
 
@@ -1371,6 +1432,7 @@ int ps_boundary_first_layer(int32_t n, const uint8_t* boards, const float* pots,
   const size_t ob = (hb.size() + 15) & ~(size_t)15;
   StagingLease lease;
   CU(lease.acquire(ob + 8 * (size_t)n + 16));
+  lease.using_stream(s);
   char* d = lease.ptr;
   float* d_pot = (float*)(d + ob);
   float* d_stack = d_pot + n;
@@ -1380,6 +1442,7 @@ int ps_boundary_first_layer(int32_t n, const uint8_t* boards, const float* pots,
   CU(launch_boundary_first_layer(n, (const uint8_t*)d, d_pot, d_stack, base, percard, wcols, bias, h, out,
                                  out_bf16 ? 1 : 0, s));
   CU(cudaStreamSynchronize(s));
+  lease.done();
   return PS_OK;
 }
 
@@ -2114,12 +2177,14 @@ int ps_sample_situations(const ps_sampler_config* cfg, int64_t first, int32_t n,
   cudaStream_t s = (cudaStream_t)stream;
   StagingLease lease;
   CU(lease.acquire(sizeof(int)));
+  lease.using_stream(s);
   int* d_err = (int*)lease.ptr;
   CU(cudaMemsetAsync(d_err, 0, sizeof(int), s));
   CU(launch_sample_situations(P, n, boards, pots, stacks, ranges, d_err, s));
   int e = 0;
   CU(cudaMemcpyAsync(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
+  lease.done();
   if (e)
     return fail(PS_ERR_INVALID, "a situation could not be drawn: pot and SPR intervals infeasible for the initial "
                                 "stack (10000 attempts, as the reference)");
@@ -2145,6 +2210,7 @@ int ps_boundary_encode(int32_t n, const uint8_t* boards, const float* pots, cons
   const size_t ob = ((hb.size() + 15) & ~(size_t)15);
   StagingLease lease;
   CU(lease.acquire(ob + 8 * (size_t)n + 16));
+  lease.using_stream(s);
   char* d = lease.ptr;
   float* d_pot = (float*)(d + ob);
   float* d_stack = d_pot + n;
@@ -2153,6 +2219,7 @@ int ps_boundary_encode(int32_t n, const uint8_t* boards, const float* pots, cons
   CU(cudaMemcpyAsync(d_stack, stacks, 4 * (size_t)n, cudaMemcpyHostToDevice, s));
   CU(launch_boundary_encode(n, (const uint8_t*)d, d_pot, d_stack, reach, out, out_bf16 ? 1 : 0, s));
   CU(cudaStreamSynchronize(s));
+  lease.done();
   return PS_OK;
 }
 
@@ -2262,3 +2329,38 @@ int ps_batch_autotune_log(ps_batch* pb, int32_t* block_threads, int32_t* scan_bu
 }
 
 }  // extern "C"
+
+// ---- test hooks ----
+int ps_debug_grid_barrier_timeout(int32_t ctas, int32_t rounds, int64_t wait_ns, int32_t* err, int32_t* passed,
+                                  float* ms) {
+  if (!err || !passed || !ms || ctas < 2 || ctas > 148 || rounds < 1 || wait_ns < 0 || wait_ns > 1000000000LL)
+    return fail(PS_ERR_INVALID, "bad argument");
+  DeviceConsts* dc = nullptr;
+  int rc = device_consts(&dc);
+  if (rc) return rc;
+  char* d = nullptr;
+  CU(cudaMalloc(&d, 64));
+  std::unique_ptr<char, decltype(&cudaFree)> keep(d, &cudaFree);
+  unsigned* bar = (unsigned*)d;
+  int* d_err = (int*)(d + 16);
+  int* d_passed = (int*)(d + 20);
+  cudaStream_t s = nullptr;
+  CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  std::unique_ptr<CUstream_st, decltype(&cudaStreamDestroy)> ks(s, &cudaStreamDestroy);
+  cudaEvent_t ev[2];
+  CU(cudaEventCreate(&ev[0]));
+  CU(cudaEventCreate(&ev[1]));
+  CU(cudaMemsetAsync(d + 16, 0, 8, s));
+  CU(cudaEventRecord(ev[0], s));
+  CU(launch_debug_barrier_timeout(ctas, rounds, wait_ns, bar, d_err, d_passed, s));
+  CU(cudaEventRecord(ev[1], s));
+  int h[2] = {0, 0};
+  CU(cudaMemcpyAsync(h, d + 16, 8, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  CU(cudaEventElapsedTime(ms, ev[0], ev[1]));
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  *err = h[0];
+  *passed = h[1];
+  return PS_OK;
+}

@@ -88,6 +88,7 @@ struct Ctx {
   Tables t0;     // board-0 tables (shared memory when staged, else global)
   int split;     // 1: node ops may be split over idle warps (few items per step)
   int part, parts;  // split node op: this item's column block and the number of blocks
+  long long wait_ns;  // grid mode: how long a grid barrier waits for the other CTAs
 };
 
 __device__ __forceinline__ const float* slot_in(const Ctx& c, uint16_t id) {
@@ -620,37 +621,66 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
 // ---------------------------------------------------------------------------
 // Pass driver and root reductions
 // ---------------------------------------------------------------------------
-// Grid barrier of a cooperative launch (all CTAs resident): a counter and a
-// generation word in global memory, device-scope release / acquire.  The wait
-// gives up after kGridSpin polls and reports ERR_WAIT, so a failed launch ends
-// with an error instead of a hung GPU.
-constexpr int kGridSpin = 1 << 24;  // polls of the generation word (~1 s with the back-off)
-__device__ void grid_barrier(const Ctx& c) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    cuda::atomic_ref<unsigned, cuda::thread_scope_device> count(c.bar[0]), gen(c.bar[1]);
-    const unsigned g = gen.load(cuda::memory_order_acquire);
-    if (count.fetch_add(1u, cuda::memory_order_acq_rel) == gridDim.x - 1) {
-      count.store(0u, cuda::memory_order_relaxed);
-      gen.store(g + 1u, cuda::memory_order_release);
-    } else {
-      for (int n = 0; gen.load(cuda::memory_order_acquire) == g; ++n) {
-        if (n >= kGridSpin) {
-          atomicOr(c.err, ERR_WAIT);
-          break;
-        }
-        __nanosleep(32);
-      }
-    }
-  }
-  __syncthreads();
+// Grid barrier of a cooperative launch (all CTAs resident): a counter, a
+// generation word and an abort word in global memory (bar[0..2]), device-scope
+// release / acquire.  A wait gives up after c.wait_ns nanoseconds of the
+// global timer (or, as a backstop should the timer stall, after wait_ns / 16
+// polls), reports ERR_WAIT and sets the abort word.  From then on every
+// barrier of every CTA returns false at once - also one that was already
+// waiting - and the pass and iteration loops end, so a failed launch ends with
+// an error status instead of a hung GPU.  The result is the same on every
+// thread of the CTA (s_grid_ok, written by thread 0 between two barriers).
+constexpr long long kGridWaitNs = 1000000000LL;  // 1 s: a grid step takes microseconds
+__shared__ int s_grid_ok;  // grid mode: 0 once the launch is aborted
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
 }
 
-__device__ __forceinline__ void step_barrier(const Ctx& c) {
-  if (c.grid)
-    grid_barrier(c);
-  else
-    __syncthreads();
+__device__ bool grid_barrier(const Ctx& c) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> count(c.bar[0]), gen(c.bar[1]), abort_(c.bar[2]);
+    int ok = abort_.load(cuda::memory_order_relaxed) == 0u;
+    if (ok) {
+      const unsigned g = gen.load(cuda::memory_order_acquire);
+      if (count.fetch_add(1u, cuda::memory_order_acq_rel) == gridDim.x - 1) {
+        count.store(0u, cuda::memory_order_relaxed);
+        gen.store(g + 1u, cuda::memory_order_release);
+      } else {
+        const unsigned long long t0 = global_ns();
+        const unsigned long long max_polls = (unsigned long long)(c.wait_ns / 16) + 65536ull;
+        for (unsigned long long n = 0; gen.load(cuda::memory_order_acquire) == g; ++n) {
+          if (abort_.load(cuda::memory_order_relaxed) != 0u) {
+            ok = 0;
+            break;
+          }
+          if (n >= max_polls || ((n & 31) == 31 && (long long)(global_ns() - t0) > c.wait_ns)) {
+            atomicOr(c.err, ERR_WAIT);
+            abort_.store(1u, cuda::memory_order_relaxed);
+            ok = 0;
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
+    }
+    s_grid_ok = ok;
+  }
+  __syncthreads();
+  return s_grid_ok != 0;
+}
+
+// false once a grid-mode launch has been aborted (uniform over the CTA: read
+// only after a barrier); always true outside grid mode
+__device__ __forceinline__ bool grid_live(const Ctx& c) { return !c.grid || s_grid_ok != 0; }
+
+__device__ __forceinline__ bool step_barrier(const Ctx& c) {
+  if (c.grid) return grid_barrier(c);
+  __syncthreads();
+  return true;
 }
 
 // One pass for traverser p over the K spots cs[0..K) in lockstep (spots of
@@ -714,8 +744,9 @@ __device__ __noinline__ void run_pass_multi(Ctx* cs, int K, unsigned active, int
                 t_op);
     }
     PHASE_T0(t_bar);
-    step_barrier(c);
+    const bool live = step_barrier(c);
     PHASE_ADD(PH_BARRIER, t_bar);
+    if (!live) return;
   }
 }
 
@@ -786,7 +817,7 @@ __device__ __noinline__ void run_pass_split(const Ctx& c, int p, const Discount 
         default: break;
       }
     }
-    step_barrier(c);
+    if (!step_barrier(c)) return;
   }
 }
 
@@ -881,15 +912,15 @@ __device__ void dcfr_iteration_multi(Ctx* cs, int K, unsigned active, const Disc
 __device__ float spot_exploitability(Ctx& c) {
   const SpotDev& sp = *c.sp;
   const Discount dz{0.f, 0.f, 0.f, 0.f};
-  float mes[2];
-  for (int p = 0; p < 2; ++p) {
+  float mes[2] = {0.f, 0.f};
+  for (int p = 0; p < 2 && grid_live(c); ++p) {
     c.root_reach = sp.w[p ^ 1];
     run_pass(c, p, dz, M_BR);
     mes[p] = (float)root_dot(c, sp.w[p], slot_at(c, sp.root_slot[p]), sp.H[p], p);
   }
   if (!sp.raked) return (mes[0] + mes[1]) * 0.5f;
-  float cur[2];
-  for (int p = 0; p < 2; ++p) {
+  float cur[2] = {0.f, 0.f};
+  for (int p = 0; p < 2 && grid_live(c); ++p) {
     c.root_reach = sp.w[p ^ 1];
     run_pass(c, p, dz, M_AVG);
     cur[p] = (float)root_dot(c, sp.w[p], slot_at(c, sp.root_slot[p]), sp.H[p], 2 + p);
@@ -899,7 +930,7 @@ __device__ float spot_exploitability(Ctx& c) {
 
 __device__ void dcfr_iteration(Ctx& c, const Discount dc) {
   const SpotDev& sp = *c.sp;
-  for (int p = 0; p < 2; ++p) {  // alternating updates (solver.rs:144-155)
+  for (int p = 0; p < 2 && grid_live(c); ++p) {  // alternating updates (solver.rs:144-155)
     c.root_reach = sp.w[p ^ 1];
     run_pass(c, p, dc, M_DCFR);
   }
@@ -918,6 +949,7 @@ __device__ bool bind_ctx(Ctx& c, const SpotDev* sp, float* scratch, size_t scrat
   c.grid = 0;
   c.bar = nullptr;
   c.gred = nullptr;
+  c.wait_ns = kGridWaitNs;
   c.err = err;
   c.slots = scratch;
   char* p = smem;
@@ -1118,14 +1150,17 @@ __global__ void PS_SOLVE_BOUNDS k_grid(const SpotDev* __restrict__ spot, const D
   c.grid = 1;
   c.bar = bar;
   c.gred = gred;
+  c.wait_ns = job.wait_ns;
+  if (threadIdx.x == 0) s_grid_ok = 1;
+  __syncthreads();
   const SpotDev& sp = *spot;
   const Discount dz{0.f, 0.f, 0.f, 0.f};
   switch (job.kind) {
     case GRID_ITERATE:
-      for (int t = job.t0; t < job.t1; ++t) dcfr_iteration(c, disc[t]);
+      for (int t = job.t0; t < job.t1 && grid_live(c); ++t) dcfr_iteration(c, disc[t]);
       return;
     case GRID_FINALIZE:
-      for (int p = 0; p < 2; ++p) {
+      for (int p = 0; p < 2 && grid_live(c); ++p) {
         c.root_reach = sp.w[p ^ 1];
         run_pass(c, p, dz, M_AVG_SAVE);
       }
@@ -1149,7 +1184,7 @@ __global__ void PS_SOLVE_BOUNDS k_grid(const SpotDev* __restrict__ spot, const D
   float expl = spot_exploitability(c);
   int t = 0;
   if (job.kind == GRID_SOLVE)
-    for (; t < job.t1; ++t) {
+    for (; t < job.t1 && grid_live(c); ++t) {
       if (expl <= job.target) break;
       dcfr_iteration(c, disc[t]);
       if ((t + 1) % 5 == 0 || t + 1 == job.t1) expl = spot_exploitability(c);
@@ -1492,7 +1527,7 @@ cudaError_t launch_grid(const SpotDev* spot, const GridJob& job, const Discount*
   size_t smem = plan.total();
   cudaError_t e = set_smem((const void*)k_grid, smem);
   if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s);
+  e = cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), s);  // count, generation, abort word
   if (e != cudaSuccess) return e;
   GridJob j = job;
   SmemPlan pl = plan;
@@ -1554,22 +1589,65 @@ cudaError_t launch_eval_terminal(const SpotDev* spots, Op op, int player, float*
 static __device__ __align__(256) float g_fixed_scratch[kFixedScratchHeader + kFixedScratchFloats];
 
 static std::mutex g_fixed_mu;
-static float* g_fixed_base[64];  // per device ordinal, looked up once
+struct FixedBase {
+  unsigned long long ctx = 0;  // id of the context the address belongs to (0 = none yet)
+  float* p = nullptr;
+};
+static FixedBase g_fixed_base[64];  // per device ordinal
 
-// Looks the array up for the current device on its first use there.
+// The driver's context functions, reached through the runtime (no link to libcuda).
+using CtxGetCurrentFn = int (*)(void**);
+using CtxGetIdFn = int (*)(void*, unsigned long long*);
+static CtxGetCurrentFn g_ctx_get_current = nullptr;
+static CtxGetIdFn g_ctx_get_id = nullptr;
+static std::once_flag g_ctx_once;
+
+cudaError_t current_context_id(unsigned long long* id) {
+  std::call_once(g_ctx_once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f);
+  });
+  if (!g_ctx_get_current || !g_ctx_get_id) return cudaErrorNotSupported;
+  void* ctx = nullptr;
+  if (g_ctx_get_current(&ctx) != 0) return cudaErrorDeviceUninitialized;
+  if (!ctx) {  // no context yet on this thread: the runtime makes the device's primary context current
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaSetDevice(dev);
+    if (e != cudaSuccess) return e;
+    if (g_ctx_get_current(&ctx) != 0 || !ctx) return cudaErrorDeviceUninitialized;
+  }
+  return g_ctx_get_id(ctx, id) == 0 ? cudaSuccess : cudaErrorDeviceUninitialized;
+}
+
+// The array's address in the current context, looked up on the first call in
+// each context (a device reset ends the context that the old address belonged to).
 static cudaError_t fixed_scratch_base(float** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  unsigned long long ctx = 0;
+  e = current_context_id(&ctx);
+  if (e != cudaSuccess) return e;
   std::lock_guard<std::mutex> lk(g_fixed_mu);
-  if (!g_fixed_base[dev]) {
+  FixedBase& fb = g_fixed_base[dev];
+  if (fb.ctx != ctx || !fb.p) {
     float* p = nullptr;
     e = cudaGetSymbolAddress((void**)&p, g_fixed_scratch);
     if (e != cudaSuccess) return e;
-    g_fixed_base[dev] = p;
+    fb.p = p;
+    fb.ctx = ctx;
   }
-  *out = g_fixed_base[dev];
+  *out = fb.p;
   return cudaSuccess;
 }
 
@@ -1598,6 +1676,32 @@ cudaError_t launch_exploitability_fixed(const SpotDev* spot, size_t slot_floats,
   *host_out = head[0];
   __builtin_memcpy(host_err, &head[1], sizeof(int));
   return cudaSuccess;
+}
+
+// Test hook of the bounded grid barrier (launch_debug_barrier_timeout): CTA 0
+// enters `rounds` grid barriers that the other CTAs never join.
+__global__ void k_debug_barrier_timeout(unsigned* bar, int* err, int* passed, int rounds, long long wait_ns) {
+  Ctx c{};
+  c.grid = 1;
+  c.bar = bar;
+  c.err = err;
+  c.wait_ns = wait_ns;
+  if (threadIdx.x == 0) s_grid_ok = 1;
+  __syncthreads();
+  if (blockIdx.x != 0) return;
+  int n = 0;
+  for (int r = 0; r < rounds; ++r)
+    if (grid_barrier(c)) ++n;
+  if (threadIdx.x == 0) *passed = n;
+}
+
+cudaError_t launch_debug_barrier_timeout(int ctas, int rounds, long long wait_ns, unsigned* bar, int* err,
+                                         int* passed, cudaStream_t s) {
+  if (ctas < 2 || ctas > 148 || rounds < 1 || wait_ns < 0 || wait_ns > kGridWaitNs) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  void* args[] = {(void*)&bar, (void*)&err, (void*)&passed, (void*)&rounds, (void*)&wait_ns};
+  return cudaLaunchCooperativeKernel((const void*)k_debug_barrier_timeout, dim3(ctas), dim3(64), args, 0, s);
 }
 
 #ifdef PS_PHASE_TIMERS

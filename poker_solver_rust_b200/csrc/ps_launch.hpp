@@ -40,7 +40,8 @@ size_t setup_smem_bytes();
 int solve_occupancy(int block, const SmemPlan& plan);
 // Grid mode for one large spot: the work of one cooperative launch of k_grid
 // (every CTA on the same spot), the number of CTAs that can be co-resident for
-// it, and the launch.  bar: 2 unsigned, gred: 4 double, both device memory.
+// it, and the launch.  bar: 4 unsigned (barrier count, generation, abort
+// word), gred: 4 double, both device memory.
 enum GridKind { GRID_SOLVE = 0, GRID_ITERATE = 1, GRID_EXPL = 2, GRID_FINALIZE = 3, GRID_AVERAGE = 4 };
 struct GridJob {
   int kind;
@@ -51,6 +52,7 @@ struct GridJob {
   float* bgrad;            // GRID_AVERAGE: boundary gradient buffer or null
   float* out;              // GRID_AVERAGE: root values [H_player]
   float* breach = nullptr; // GRID_AVERAGE: boundary reach buffer or null
+  long long wait_ns = 1000000000LL;  // a grid barrier's wait limit before the launch aborts with ERR_WAIT
 };
 int grid_ctas(int block, const SmemPlan& plan);
 // Reach-weighted 48-river average of boundary-network outputs (ps_datagen.cu):
@@ -166,12 +168,28 @@ cudaError_t launch_eval_terminal(const SpotDev* spots, Op op, int player, float*
 // Exploitability of one game with its working slots in a fixed, statically
 // sized device array instead of allocated memory.  The array holds a 256-byte
 // header (result and error flag) and kFixedScratchFloats floats of slots
-// (16 MiB); a game needs num_slots * vstride of them.  The first call on a
-// device looks up the array's address (cudaGetSymbolAddress) with that device
-// current.  Every call uses the same array: calls whose kernels overlap on
-// the GPU overwrite each other's slots.
+// (16 MiB); a game needs num_slots * vstride of them.  The first call in a
+// CUDA context looks up the array's address (cudaGetSymbolAddress) with that
+// context's device current; a device reset ends the context, and the next
+// call looks the address up again in the new one.  Every call uses the same
+// array: calls whose kernels overlap on the GPU overwrite each other's slots.
 constexpr size_t kFixedScratchHeader = 64;
 constexpr size_t kFixedScratchFloats = (size_t)4 << 20;
 cudaError_t launch_exploitability_fixed(const SpotDev* spot, size_t slot_floats, int block, const SmemPlan& plan,
                                         cudaStream_t s, float* host_out, int* host_err);
+
+// Unique id of the CUDA context current on the calling thread (the driver's
+// cuCtxGetId, which never repeats within a process, unlike a context handle
+// whose address a new context may reuse).  Initialises the current device's
+// primary context when none is current.  Caches of device pointers are keyed
+// on it: a cudaDeviceReset destroys the context they were made in.
+cudaError_t current_context_id(unsigned long long* id);
+
+// Test hook for the bounded grid barrier: a cooperative launch of `ctas` CTAs
+// in which CTA 0 enters `rounds` grid barriers that no other CTA joins.  The
+// first wait gives up after wait_ns nanoseconds and reports ERR_WAIT (4) in
+// *err; every later barrier must return at once.  *passed counts the barriers
+// CTA 0 got through (0 when the abort works).  bar: 4 unsigned of device memory.
+cudaError_t launch_debug_barrier_timeout(int ctas, int rounds, long long wait_ns, unsigned* bar, int* err,
+                                         int* passed, cudaStream_t s);
 }  // namespace ps

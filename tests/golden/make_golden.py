@@ -1,7 +1,7 @@
 """Generates tests/golden/reference_pins.json from the reference sources.
 
-Run in a container where the reference checkout is present:
-    python tests/golden/make_golden.py [/path/to/poker_solver_rust]
+Run where a checkout of the reference is present, giving its root:
+    python tests/golden/make_golden.py /path/to/poker_solver_rust
 
 It reads crates/range-solver/src/hand_table.rs as text and stores only the
 table's length, a SHA-256 digest of its little-endian int32 bytes and its
@@ -21,7 +21,9 @@ import re
 import struct
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_golden.py /path/to/poker_solver_rust (the reference checkout's root)")
+REF = sys.argv[1]
 SRC = os.path.join(REF, "crates", "range-solver", "src")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_pins.json")
 

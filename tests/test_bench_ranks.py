@@ -69,7 +69,7 @@ def test_reference_arm_runs_on_rank_zero_only(capsys):
 
     import bench
 
-    args = argparse.Namespace(warmup=3, steps=1, ref_spots=1, spots=4096, seed=7)
+    args = argparse.Namespace(warmup=3, steps=1, cpu_spots_per_thread=1, spots=4096, seed=7)
     assert bench.run_reference(args, rank=1, world=2) is None
     assert capsys.readouterr().out == ""
 
@@ -84,7 +84,7 @@ def test_reference_arm_prints_contract_line(capsys):
 
     import bench
 
-    args = argparse.Namespace(warmup=1, steps=1, ref_spots=1, spots=4096, seed=7)
+    args = argparse.Namespace(warmup=1, steps=1, cpu_spots_per_thread=1, spots=64, seed=7)
     bench.run_reference(args, rank=0, world=1)
     lines = [ln for ln in capsys.readouterr().out.splitlines() if ln.strip()]
     assert len(lines) == 1
