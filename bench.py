@@ -417,6 +417,10 @@ def main():
     ap.add_argument("--stage", type=int, default=-1)
     ap.add_argument("--bufs", type=int, default=0, help="terminal scan buffers per CTA (0 = half the warps)")
     ap.add_argument("--inst", type=int, default=0, help="spots per CTA in lockstep (0 = library default)")
+    ap.add_argument("--sched", type=int, default=0, help="0 = library default, 1 = step-synchronous, 2 = dataflow")
+    ap.add_argument("--flow-threads", type=int, default=0, help="dataflow threads per CTA (0 = default/autotuned)")
+    ap.add_argument("--spots-per-cta", type=int, default=0, help="dataflow spots per CTA (0 = default/autotuned)")
+    ap.add_argument("--node-parts", type=int, default=0, help="dataflow node-op parts (0 = default/autotuned)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -454,8 +458,10 @@ def main():
     def max_over_ranks(x: float) -> float:
         return rank_max(x, dist, "cuda")
 
-    bs = ps.BatchSolver(cc, tcs, block_threads=args.block, ctas_per_sm=args.ctas_per_sm, stage_tables=args.stage,
-                        scan_buffers=args.bufs, instances_per_cta=args.inst)
+    shape = dict(block_threads=args.block, ctas_per_sm=args.ctas_per_sm, stage_tables=args.stage,
+                 scan_buffers=args.bufs, instances_per_cta=args.inst, scheduler=args.sched,
+                 flow_threads=args.flow_threads, flow_spots_per_cta=args.spots_per_cta, node_parts=args.node_parts)
+    bs = ps.BatchSolver(cc, tcs, **shape)
     for _ in range(args.warmup):
         bs.solve(MAX_ITER, targets)
 
@@ -491,8 +497,7 @@ def main():
     for k in range(min(args.steps, args.e2e_steps)):
         barrier()
         t0 = time.perf_counter()
-        b2 = ps.BatchSolver(cc, tcs, block_threads=args.block, ctas_per_sm=args.ctas_per_sm,
-                            stage_tables=args.stage, scan_buffers=args.bufs, instances_per_cta=args.inst)
+        b2 = ps.BatchSolver(cc, tcs, **shape)
         b2.solve(MAX_ITER, targets)
         e2, _ = b2.results()
         torch.cuda.synchronize()
@@ -553,11 +558,11 @@ def main():
             "config": {"workload": f"batched river datagen: {args.spots} spots per GPU to <=0.3% pot or "
                                    f"{MAX_ITER} iterations", "parallelism": f"replicas x{world}",
                        "l2": "state (regrets + strategy sums) exceeds L2; no flush needed",
-                       "block_threads": cfg["block_threads"], "ctas_per_sm": cfg["ctas_per_sm"],
-                       "grid": cfg["grid"],
-                       "scan_buffers": cfg["scan_buffers"],
-                       "autotune": [{"block_threads": b, "scan_buffers": u, "trial_ms": round(ms, 3)}
-                                    for b, u, ms in bs.autotune_log()]},
+                       "scheduler": cfg["scheduler"], "block_threads": cfg["block_threads"],
+                       "ctas_per_sm": cfg["ctas_per_sm"], "grid": cfg["grid"],
+                       "scan_buffers": cfg["scan_buffers"], "spots_per_cta": cfg["spots_per_cta"],
+                       "node_parts": cfg["node_parts"],
+                       "autotune": bs.autotune_trials()},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": 2 * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -67,6 +67,14 @@ int ps_game_new(const ps_card_config* cards, const ps_tree_config* tree, ps_game
 void ps_game_free(ps_game* g);
 /* PostFlopGame::memory_usage (interpreter.rs:188): bytes of f32 state on the device */
 int ps_game_memory_usage(ps_game* g, uint64_t* bytes);
+/* No counterpart in the reference.  The shape of the game's compiled tree
+ * program, host-side only (no GPU needed), for sizing device memory and
+ * launches: out[0] working slots, out[1] slot stride (floats), out[2..3]
+ * steps of traverser 0 / 1, out[4..5] node ops of traverser 0 / 1, out[6..7]
+ * terminal ops, out[8..9] terminal runs (terminals sharing one reach scan),
+ * out[10] S = sum over decision edges of the acting player's hands (the
+ * per-iteration state stream is 20 * S bytes), out[11] boards. */
+int ps_game_program_info(ps_game* g, int64_t out[12]);
 /* PostFlopGame::allocate_memory (interpreter.rs:212); compression -> PS_ERR_UNSUPPORTED */
 int ps_game_allocate_memory(ps_game* g, int enable_compression);
 
@@ -118,6 +126,20 @@ int ps_eval_fixed_strategy(ps_game* g, const float* w0, const float* w1, float* 
  * [H0 values for player 0][H1 values for player 1] (NULL = not wanted) */
 int ps_eval_fixed_strategy_adjoint(ps_game* g, const float* w0, const float* w1, const float* g0, const float* g1,
                                    float* dw0, float* dw1, float* dbcfv);
+/* The same two calls with every array in device memory of the game's device
+ * when on_device = 1 (host memory when 0): a trainer keeps its tensors on the
+ * GPU, and nothing passes through the host.  The call does not wait for
+ * other streams: the work that writes the inputs must be finished before it;
+ * the results are complete when it returns. */
+int ps_eval_fixed_strategy_ex(ps_game* g, const float* w0, const float* w1, float* cfv0, float* cfv1,
+                              int32_t on_device);
+int ps_eval_fixed_strategy_adjoint_ex(ps_game* g, const float* w0, const float* w1, const float* g0,
+                                      const float* g1, float* dw0, float* dw1, float* dbcfv, int32_t on_device);
+/* Every boundary value of the game in one call (set_boundary_cfvs,
+ * interpreter.rs:343, for each ordinal and player): values [n_boundary][H0 +
+ * H1], per ordinal player 0's H0 values then player 1's; device memory when
+ * on_device = 1. */
+int ps_set_boundary_cfvs_all(ps_game* g, const float* values, int32_t on_device);
 
 /* ---- game data (game/mod.rs, interpreter.rs) ---- */
 int ps_num_private_hands(ps_game* g, int player);
@@ -218,7 +240,21 @@ typedef struct ps_batch_opts {
                              autotuner then also tries all of them) */
   int32_t instances_per_cta; /* spots of one tree shape a CTA solves in lockstep, 1..4
                                 (0 = 1); they share each step's barrier */
+  int32_t scheduler;      /* PS_SCHED_DEFAULT (0): dataflow for batches of more spots than SMs,
+                             step-synchronous otherwise; PS_SCHED_STEP (1): every CTA walks
+                             its spot's steps with one barrier per step (k_solve);
+                             PS_SCHED_FLOW (2): each CTA holds several spots at once and its
+                             warps take the ready items of any of them (k_flow).  Results
+                             are the same bits either way. */
+  int32_t flow_threads;   /* dataflow: threads per CTA, a multiple of 32 from 128 to 1024
+                             (0 = 512; with block_threads = -1 the autotuner chooses) */
+  int32_t flow_spots_per_cta; /* dataflow: spots a CTA holds at once, 1..8 (0 = 2, or autotuned) */
+  int32_t node_parts;     /* dataflow: column blocks each node op is cut into, 1..16
+                             (0 = 2, or autotuned) */
 } ps_batch_opts;
+#define PS_SCHED_DEFAULT 0
+#define PS_SCHED_STEP 1
+#define PS_SCHED_FLOW 2
 int ps_batch_new(const ps_card_config* cards, const ps_tree_config* trees, int32_t n,
                  const ps_batch_opts* opts, ps_batch** out);
 void ps_batch_free(ps_batch* b);
@@ -250,6 +286,15 @@ int ps_batch_config(ps_batch* b, int32_t* block_threads, int32_t* grid, int32_t*
 int ps_batch_autotune_log(ps_batch* b, int32_t* block_threads, int32_t* scan_buffers, float* trial_ms, int cap);
 /* scan-buffer warps per CTA the batch runs with */
 int ps_batch_scan_buffers(ps_batch* b);
+/* the launch shape of the batch's solves: out[0] scheduler (PS_SCHED_STEP or
+ * PS_SCHED_FLOW), [1] threads per CTA, [2] CTAs, [3] CTAs per SM, [4]
+ * scan-buffer warps per CTA, [5] spots per CTA, [6] node-op parts, [7] 1 when
+ * a single spot runs in grid mode (every SM on it) */
+int ps_batch_schedule(ps_batch* b, int32_t out[8]);
+/* the trials of the last autotune: per trial 4 values (threads per CTA,
+ * scan-buffer warps, spots per CTA, node-op parts; the last two 0 for a
+ * step-synchronous trial) and its device ms; returns the count */
+int ps_batch_autotune_trials(ps_batch* b, int32_t* shape, float* trial_ms, int cap);
 /* bytes copied host->device by ps_batch_new and device->host by ps_batch_results */
 int ps_batch_io_bytes(ps_batch* b, uint64_t* h2d, uint64_t* d2h);
 
@@ -352,14 +397,16 @@ int ps_discount_params(uint32_t t, float out[3]); /* solver.rs:26-44 */
 
 /* ---- test hooks (no reference counterpart) ---- */
 /* The bounded grid barrier of single-game grid mode: a cooperative launch of
- * `ctas` CTAs (2..148) in which CTA 0 enters `rounds` grid barriers that no
- * other CTA joins.  The first wait gives up after wait_ns nanoseconds (at most
- * 1 s) and sets the launch's error word to 4 (a barrier gave up) and its abort
- * word; every later barrier then returns at once.  Out: the error word, the
- * number of barriers CTA 0 got through (0 when the abort works) and the
- * kernel's time in ms.  No kernel of this call waits without a bound. */
-int ps_debug_grid_barrier_timeout(int32_t ctas, int32_t rounds, int64_t wait_ns, int32_t* err, int32_t* passed,
-                                  float* ms);
+ * `ctas` CTAs (2 to the SM count) in which CTA 0 enters `rounds` grid barriers
+ * that no other CTA joins.  The first wait gives up after wait_ns nanoseconds
+ * (at most 1 s) and sets the launch's error word to 4 (a barrier gave up) and
+ * its abort word; every later barrier then returns at once.  With all_join = 1
+ * every CTA enters the barriers instead, so none runs out and the kernel time
+ * divided by rounds is the cost of one grid barrier.  Out: the error word, the
+ * number of barriers CTA 0 got through and the kernel's time in ms.  No
+ * kernel of this call waits without a bound. */
+int ps_debug_grid_barrier_timeout(int32_t ctas, int32_t rounds, int64_t wait_ns, int32_t all_join, int32_t* err,
+                                  int32_t* passed, float* ms);
 
 #ifdef __cplusplus
 }

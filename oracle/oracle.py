@@ -100,6 +100,8 @@ def lib():
                 "orc_boundary_node_indices": (i32, [vp, P(i64)]),
                 "orc_set_boundary_cfvs": (i32, [vp, i64, i32, P(f32), i64]),
                 "orc_boundary_reach": (i32, [vp, i64, i32, P(f64)]),
+                "orc_fd_central": (i32, [vp, P(f32), P(f32), P(f32), P(f32), i32, P(i32), P(i32), P(i32),
+                                         P(i32), f64, P(f64)]),
                 "orc_evaluate_node": (i32, [vp, i64, i32, P(f32), P(f64)]),
                 "orc_back_to_root": (i32, [vp]),
                 "orc_play": (i32, [vp, i64]),
@@ -362,6 +364,22 @@ class OracleGame:
     def set_boundary_cfvs(self, ordinal, p, cfvs):
         v = np.ascontiguousarray(cfvs, np.float32)
         lib().orc_set_boundary_cfvs(self.h, ordinal, p, _p(v, C.c_float), len(v))
+
+    def fd_central(self, w, cot, coords, h=1e-3):
+        """FP64 central differences of L = cot0 . cfv0 + cot1 . cfv1 under the
+        game's current average strategy (cfv_p from the opponent's weights
+        w[1-p]) at coords: rows (kind, ordinal, player, hand), kind 0 = weight
+        of player `player`, 1 = boundary value.  Each perturbed input is
+        rounded to f32 and the step actually taken is used (orc_fd_central)."""
+        c = np.ascontiguousarray(np.asarray(coords, np.int32).reshape(-1, 4))
+        cols = [np.ascontiguousarray(c[:, k]) for k in range(4)]
+        w = [np.ascontiguousarray(x, np.float32) for x in w]
+        cot = [np.ascontiguousarray(x, np.float32) for x in cot]
+        out = np.zeros(len(c), np.float64)
+        self._check(lib().orc_fd_central(self.h, _p(w[0], C.c_float), _p(w[1], C.c_float), _p(cot[0], C.c_float),
+                                         _p(cot[1], C.c_float), len(c), *[_p(x, C.c_int32) for x in cols],
+                                         float(h), _p(out, C.c_double)))
+        return out
 
     def boundary_reach(self, ordinal, p):
         out = np.zeros(2000)

@@ -394,6 +394,69 @@ int orc_set_boundary_cfvs(void* p, int64_t ordinal, int pl, const float* v, int6
   });
 }
 
+// Central differences of L = g0 . cfv0 + g1 . cfv1, where cfv_p are the root
+// cfvalues of player p under the game's current average strategy with the
+// opponent's reach w_{1-p} (root_cfvalues_with_reach, utility.rs:422-443), at n
+// coordinates: kind 0 = weight w_p[hand], kind 1 = boundary value of player p
+// at boundary `ord`, hand `hand` (set_boundary_cfvs, interpreter.rs:343).
+// L is linear in every coordinate, so a central difference is exact up to
+// rounding.  Each perturbed input is rounded to f32, as the device reads it,
+// and the step actually taken divides the difference.  Only the term that the
+// coordinate reaches is re-evaluated: a weight of p moves cfv_{1-p}, a
+// boundary value of p moves cfv_p.  Test infrastructure: FP64 games only.
+int orc_fd_central(void* p, const float* w0, const float* w1, const float* g0, const float* g1, int n,
+                   const int32_t* kind, const int32_t* ord, const int32_t* pl, const int32_t* hand, double h,
+                   double* out) {
+  auto* hd = (OrcGame*)p;
+  if (!hd || !hd->fp64) {
+    g_err = "orc_fd_central needs an FP64 game";
+    return -1;
+  }
+  try {
+    Game<double>& g = *hd->g64;
+    const float* w[2] = {w0, w1};
+    const float* gv[2] = {g0, g1};
+    std::vector<double> wd[2];
+    for (int q = 0; q < 2; ++q) wd[q].assign(w[q], w[q] + g.num_private_hands(q));
+    // value of g_q . cfv_q with opponent reach r
+    auto term = [&](int q, const std::vector<double>& r) {
+      std::vector<double> v = g.root_cfvalues_with_reach(q, r.data());
+      double acc = 0.0;
+      for (size_t i = 0; i < v.size(); ++i) acc += (double)gv[q][i] * v[i];
+      return acc;
+    };
+    for (int i = 0; i < n; ++i) {
+      const int q = pl[i], j = hand[i];
+      if (q < 0 || q > 1 || j < 0 || (size_t)j >= g.num_private_hands(q)) throw std::runtime_error("bad coordinate");
+      if (kind[i] == 0) {
+        std::vector<double> r = wd[q];
+        const double xp = (double)(float)(r[j] + h), xm = (double)(float)(r[j] - h);
+        r[j] = xp;
+        const double lp = term(q ^ 1, r);
+        r[j] = xm;
+        const double lm = term(q ^ 1, r);
+        out[i] = (lp - lm) / (xp - xm);
+      } else {
+        const size_t k = (size_t)ord[i] * 2 + q;
+        if (k >= g.boundary_cfvs.size() || (size_t)j >= g.boundary_cfvs[k].size())
+          throw std::runtime_error("bad boundary coordinate");
+        const double x0 = g.boundary_cfvs[k][j];
+        const double xp = (double)(float)(x0 + h), xm = (double)(float)(x0 - h);
+        g.boundary_cfvs[k][j] = xp;
+        const double lp = term(q, wd[q ^ 1]);
+        g.boundary_cfvs[k][j] = xm;
+        const double lm = term(q, wd[q ^ 1]);
+        g.boundary_cfvs[k][j] = x0;
+        out[i] = (lp - lm) / (xp - xm);
+      }
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
 int orc_boundary_reach(void* p, int64_t ordinal, int pl, double* out) {
   return with((OrcGame*)p, [&](auto& g) {
     const auto& r = g.boundary_reach[ordinal * 2 + pl];

@@ -1617,7 +1617,11 @@ void Game<F>::compute_cfvalue_recursive(F* result, Node* node, int player, const
     std::vector<F> upd(no);
     F scalar = (F)1 / (F)chance_factor(*node);
     for (size_t i = 0; i < no; ++i) upd[i] = cfreach[i] * scalar;
-    for (size_t a = 0; a < na; ++a) compute_cfvalue_recursive(&cfv[a * nh], child(node, a), player, upd.data(), save);
+    // chance children in parallel (utility.rs:682 for_each_child), summed in child order below
+    const std::function<void(size_t)> one = [&](size_t a) {
+      compute_cfvalue_recursive(&cfv[a * nh], child(node, a), player, upd.data(), save);
+    };
+    g_chance_pool.parallel_for(na, one);
     std::vector<double> acc(nh);
     for (size_t h = 0; h < nh; ++h) acc[h] = (double)cfv[h];
     for (size_t a = 1; a < na; ++a)
@@ -1678,7 +1682,11 @@ void Game<F>::compute_best_cfv_recursive(F* result, Node* node, int player, cons
     std::vector<F> upd(no);
     F scalar = (F)1 / (F)chance_factor(*node);
     for (size_t i = 0; i < no; ++i) upd[i] = cfreach[i] * scalar;
-    for (size_t a = 0; a < na; ++a) compute_best_cfv_recursive(&cfv[a * nh], child(node, a), player, upd.data());
+    // chance children in parallel (utility.rs:852 for_each_child), summed in child order below
+    const std::function<void(size_t)> one = [&](size_t a) {
+      compute_best_cfv_recursive(&cfv[a * nh], child(node, a), player, upd.data());
+    };
+    g_chance_pool.parallel_for(na, one);
     std::vector<double> acc(nh);
     for (size_t h = 0; h < nh; ++h) acc[h] = (double)cfv[h];
     for (size_t a = 1; a < na; ++a)

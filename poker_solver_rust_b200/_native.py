@@ -61,7 +61,14 @@ class PsBatchOpts(C.Structure):
         ("stage_tables", C.c_int32),
         ("scan_buffers", C.c_int32),
         ("instances_per_cta", C.c_int32),
+        ("scheduler", C.c_int32),
+        ("flow_threads", C.c_int32),
+        ("flow_spots_per_cta", C.c_int32),
+        ("node_parts", C.c_int32),
     ]
+
+
+PS_SCHED_DEFAULT, PS_SCHED_STEP, PS_SCHED_FLOW = 0, 1, 2
 
 
 # name -> (restype, argtypes)
@@ -77,7 +84,11 @@ P = C.POINTER
 _sig("ps_last_error", C.c_char_p)
 _sig("ps_hand_table", i32, P(i32), i32)
 _sig("ps_discount_params", i32, u32, P(f32))
-_sig("ps_debug_grid_barrier_timeout", i32, i32, i32, i64, P(i32), P(i32), P(f32))
+_sig("ps_debug_grid_barrier_timeout", i32, i32, i32, i64, i32, P(i32), P(i32), P(f32))
+_sig("ps_game_program_info", i32, vp, P(i64))
+_sig("ps_eval_fixed_strategy_ex", i32, vp, vp, vp, vp, vp, i32)
+_sig("ps_eval_fixed_strategy_adjoint_ex", i32, vp, vp, vp, vp, vp, vp, vp, vp, i32)
+_sig("ps_set_boundary_cfvs_all", i32, vp, vp, i32)
 _sig("ps_parse_bet_sizes", i32, C.c_char_p, i32, P(i32), P(f64), P(i32), P(i32), i32)
 _sig("ps_game_new", i32, P(PsCardConfig), P(PsTreeConfig), P(vp))
 _sig("ps_game_free", None, vp)
@@ -139,6 +150,8 @@ _sig("ps_batch_iteration_bytes", f64, vp, i32)
 _sig("ps_batch_config", i32, vp, P(i32), P(i32), P(i32))
 _sig("ps_batch_autotune_log", i32, vp, P(i32), P(i32), P(f32), i32)
 _sig("ps_batch_scan_buffers", i32, vp)
+_sig("ps_batch_schedule", i32, vp, P(i32))
+_sig("ps_batch_autotune_trials", i32, vp, P(i32), P(f32), i32)
 _sig("ps_batch_io_bytes", i32, vp, P(u64), P(u64))
 _sig("ps_batch_run_iterations", i32, vp, u32, u32, i32)
 _sig("ps_batch_reset", i32, vp)

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -167,6 +168,8 @@ struct StagingLease {
 std::map<long, std::pair<int, int>> g_tune;  // autotuned (CTA size, scan-buffer warps) per
                                              // (device, hand-count class, tree-size class)
 DeviceConsts g_dev[16];
+std::map<long, std::array<int, 4>> g_flow_tune;  // autotuned dataflow shape (threads, scan buffers, spots per
+                                                 // CTA, node parts) per (device, hand-count, tree-size class)
 
 int device_consts(DeviceConsts** out) {
   int dev = 0;
@@ -289,9 +292,15 @@ struct Batch {
   int grid_blocks = 0;
   unsigned* d_bar = nullptr;
   double* d_gred = nullptr;
+  // dataflow scheduler (k_flow) for solve and run_iterations; the adjoint
+  // and single spots keep the step-synchronous k_solve
+  bool flow = false;
+  int flow_block = 512, flow_grid = 0, flow_cps = 0, flow_lanes = 2, flow_parts = 1;
+  SmemPlan flow_plan{};
   struct Trial {
     int block, bufs;
     float ms;
+    int lanes = 0, parts = 0;  // dataflow trials: spots per CTA and node-op parts (0 = step-synchronous)
   };
   std::vector<Trial> tune_log;  // trials of the last autotune
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -531,8 +540,23 @@ struct Batch {
     grid = std::max(1, std::min(n, dc->nsm * ctas_per_sm));
     for (auto& gp : games) scratch_floats = std::max(scratch_floats, (size_t)gp->num_slots * gp->vstride);
     scratch_floats = (scratch_floats + 63) & ~(size_t)63;
-    scratch_ctas = grid;
-    CU(cudaMalloc(&d_scratch, sizeof(float) * scratch_floats * scratch_ctas * inst_k));
+    {
+      const int sched = opts ? opts->scheduler : PS_SCHED_DEFAULT;
+      if (sched < PS_SCHED_DEFAULT || sched > PS_SCHED_FLOW) return fail(PS_ERR_INVALID, "unknown scheduler");
+      flow = sched == PS_SCHED_FLOW || (sched == PS_SCHED_DEFAULT && n > dc->nsm);
+      if (flow) {
+        int fb = opts && opts->flow_threads > 0 ? opts->flow_threads : 512;
+        fb = std::max(128, std::min(kMaxFlowThreads, (fb / 32) * 32));
+        const int fl = opts && opts->flow_spots_per_cta > 0 ? opts->flow_spots_per_cta : 2;
+        const int fp = opts && opts->node_parts > 0 ? opts->node_parts : 2;
+        if (fl > kMaxFlowLanes || fp > 16) return fail(PS_ERR_INVALID, "flow_spots_per_cta 1..8, node_parts 1..16");
+        const int rc = adopt_flow(fb, opts && opts->scan_buffers > 0 ? opts->scan_buffers : fb / 64, fl, fp,
+                                  opts ? opts->ctas_per_sm : 0);
+        if (rc) return rc;
+      }
+    }
+    scratch_ctas = std::max(grid * inst_k, flow ? flow_grid * flow_lanes : 0);
+    CU(cudaMalloc(&d_scratch, sizeof(float) * scratch_floats * scratch_ctas));
     // a single tree of at least PS_GRID_NODES nodes (default 16; 0 = never)
     // is solved by all SMs at once: a lone game is latency-bound, and even a
     // 33-node river tree iterates 1.5x faster on every SM than on one
@@ -614,8 +638,172 @@ struct Batch {
     CU(cudaStreamSynchronize(stream));
     g_pinned.release(h_static, h_static_cap, h_static_tag);  // uploaded: the staging buffer goes back to the pool
     h_static = nullptr;
-    if (tune) return autotune(order, opts ? opts->ctas_per_sm : 0);
+    if (tune) return flow ? autotune_flow(order, opts ? opts->ctas_per_sm : 0) : autotune(order, opts ? opts->ctas_per_sm : 0);
     return PS_OK;
+  }
+
+  // Dataflow launch shape: CTAs of b threads with `bufs` scan-buffer warps,
+  // `lanes` spots per CTA, node ops in `parts` column blocks, as many CTAs as
+  // fit (at most cap_ctas per SM) but no more than the spots need.
+  bool flow_shape(int b, int bufs, int lanes, int cap_ctas, int nspots, SmemPlan& pl, int& occ, int& g) const {
+    pl = plan;
+    pl.warps = b / 32;
+    pl.bufs = std::max(1, std::min(pl.warps, bufs));
+    pl.split = 0;
+    occ = flow_occupancy(b, pl);
+    if (occ < 1 || lanes > pl.warps) return false;
+    if (cap_ctas > 0) occ = std::min(occ, cap_ctas);
+    g = std::max(1, std::min((nspots + lanes - 1) / lanes, dc->nsm * occ));
+    return true;
+  }
+
+  int adopt_flow(int b, int bufs, int lanes, int parts, int cap_ctas) {
+    SmemPlan pl;
+    int occ, g;
+    if (!flow_shape(b, bufs, lanes, cap_ctas, (int)games.size(), pl, occ, g))
+      return fail(PS_ERR_INVALID, "dataflow launch shape does not fit: " + std::to_string(b) + " threads, " +
+                                      std::to_string(bufs) + " scan buffers, " + std::to_string(lanes) + " spots");
+    if (d_scratch && (size_t)g * lanes > (size_t)scratch_ctas) {
+      cudaFree(d_scratch);
+      d_scratch = nullptr;
+      CU(cudaMalloc(&d_scratch, sizeof(float) * scratch_floats * g * lanes));
+      scratch_ctas = g * lanes;
+    }
+    flow_block = b;
+    flow_plan = pl;
+    flow_cps = occ;
+    flow_grid = g;
+    flow_lanes = lanes;
+    flow_parts = parts;
+    return PS_OK;
+  }
+
+  // Autotuner of the dataflow shape: times the real solve job (the reference
+  // loop with its exploitability checks: one before the first iteration, after
+  // the fifth and after the sixth) on a sample of the batch's spots taken
+  // evenly from the cost order, for CTA sizes x scan buffers x spots per CTA x
+  // node-op parts, and keeps the fastest.  The choice is cached per device and
+  // tree-size class; the state the trials touched is cleared.
+  int autotune_flow(const std::vector<int>& order, int cap_ctas) {
+    const int n = (int)games.size();
+    int hs_max = 4;
+    double nodes = 0;
+    for (auto& gp : games) {
+      hs_max = std::max(hs_max, std::max(gp->hs[0], gp->hs[1]));
+      nodes += (double)gp->arena.size();
+    }
+    const long key = (1l << 62) | ((long)dc->device << 40) | ((long)(req_bufs & 0xFF) << 32) |
+                     ((long)(hs_max / 64) << 20) |
+                     (long)std::min(1 << 19, (int)std::lround(std::log2(1.0 + nodes / n) * 4));
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_flow_tune.find(key);
+      if (it != g_flow_tune.end()) {
+        const auto& c = it->second;
+        return adopt_flow(c[0], c[1], c[2], c[3], cap_ctas);
+      }
+    }
+    struct Cand {
+      int b, bufs, lanes, parts;
+    };
+    std::vector<Cand> cands;
+    for (int b : {256, 512, 1024})
+      for (int lanes : {1, 2, 3, 4})
+        for (int parts : {1, 2}) {
+          const int w = b / 32;
+          if (req_bufs > 0) {
+            cands.push_back({b, std::min(w, req_bufs), lanes, parts});
+          } else {
+            cands.push_back({b, std::max(1, w / 2), lanes, parts});
+            cands.push_back({b, w, lanes, parts});
+          }
+        }
+    int ns = 1;
+    for (const auto& c : cands) {
+      SmemPlan pl;
+      int occ, g;
+      if (flow_shape(c.b, c.bufs, c.lanes, cap_ctas, n, pl, occ, g)) ns = std::max(ns, g * c.lanes);
+    }
+    ns = std::min(n, ns);
+    std::vector<SpotDev> sample(ns);
+    std::vector<int> ids(ns);
+    for (int i = 0; i < ns; ++i) {
+      sample[i] = h_spots[order[(size_t)i * n / ns]];
+      ids[i] = i;
+    }
+    int rc = run_setup();
+    if (rc) return rc;
+    constexpr int kTrialIters = 6;
+    if ((rc = ensure_disc(kTrialIters + 1))) return rc;
+    size_t max_scr = 0;
+    for (const auto& c : cands) {
+      SmemPlan pl;
+      int occ, g;
+      if (flow_shape(c.b, c.bufs, c.lanes, cap_ctas, ns, pl, occ, g))
+        max_scr = std::max(max_scr, (size_t)g * c.lanes);
+    }
+    char* tmp = nullptr;
+    const size_t tb = align256(sizeof(SpotDev) * ns) + align256(16 * (size_t)ns) + 256;
+    CU(cudaMalloc(&tmp, tb));
+    std::unique_ptr<char, decltype(&cudaFree)> k1(tmp, &cudaFree);
+    SpotDev* d_sample = (SpotDev*)tmp;
+    int* d_ids = (int*)(tmp + align256(sizeof(SpotDev) * ns));
+    float* d_tz = (float*)(d_ids + ns);      // targets 0: every sampled spot runs all trial iterations
+    float* d_te = d_tz + ns;
+    int* d_ti = (int*)(d_te + ns);
+    int* d_cnt = (int*)(tmp + tb - 256);
+    float* d_tscratch = nullptr;
+    CU(cudaMalloc(&d_tscratch, sizeof(float) * scratch_floats * std::max<size_t>(1, max_scr)));
+    std::unique_ptr<float, decltype(&cudaFree)> k2(d_tscratch, &cudaFree);
+    CU(cudaMemcpyAsync(d_sample, sample.data(), sizeof(SpotDev) * ns, cudaMemcpyHostToDevice, stream));
+    CU(cudaMemcpyAsync(d_ids, ids.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, stream));
+    CU(cudaMemsetAsync(d_tz, 0, sizeof(float) * ns, stream));
+    const SolveJob job{0, kTrialIters, 1, 0};
+    Cand best{flow_block, flow_plan.bufs, flow_lanes, flow_parts};
+    float best_ms = 0;
+    for (const auto& c : cands) {
+      SmemPlan pl;
+      int occ, g;
+      if (!flow_shape(c.b, c.bufs, c.lanes, cap_ctas, ns, pl, occ, g)) continue;
+      for (int rep = 0; rep < 2; ++rep) {  // the first run warms the shape up, the second is timed
+        CU(cudaMemsetAsync(d_cnt, 0, sizeof(int), stream));
+        CU(cudaEventRecord(ev[2], stream));
+        CU(launch_flow(d_sample, ns, d_ids, d_cnt, d_disc, job, d_tz, d_tscratch, scratch_floats, d_te, d_ti, d_err,
+                       g, c.b, c.lanes, c.parts, pl, stream));
+        CU(cudaEventRecord(ev[3], stream));
+      }
+      CU(cudaStreamSynchronize(stream));
+      float ms = 0;
+      CU(cudaEventElapsedTime(&ms, ev[2], ev[3]));
+      Trial t{c.b, pl.bufs, ms, c.lanes, c.parts};
+      tune_log.push_back(t);
+      if (best_ms == 0 || ms < best_ms) {
+        best_ms = ms;
+        best = {c.b, pl.bufs, c.lanes, c.parts};
+      }
+    }
+    if ((rc = check_err())) return rc;
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      g_flow_tune[key] = {best.b, best.bufs, best.lanes, best.parts};
+    }
+    CU(cudaMemsetAsync(pool + static_bytes + setup_bytes, 0, state_bytes, stream));
+    ready = true;  // the trials' state is cleared and the board tables stay built
+    rc = adopt_flow(best.b, best.bufs, best.lanes, best.parts, cap_ctas);
+    if (rc) return rc;
+    CU(cudaStreamSynchronize(stream));
+    return PS_OK;
+  }
+
+  // The batch's solve-type job (iterations, checks, epilogue) on every spot,
+  // with the scheduler the batch runs.
+  cudaError_t launch_job(const SolveJob& job) {
+    if (flow)
+      return launch_flow(d_spots, (int)games.size(), d_order, d_counter, d_disc, job, d_target, d_scratch,
+                         scratch_floats, d_expl, d_iters, d_err, flow_grid, flow_block, flow_lanes, flow_parts,
+                         flow_plan, stream);
+    return launch_solve(d_spots, ninst, inst_k, d_inst, d_counter, d_disc, job, d_target, d_scratch, scratch_floats,
+                        d_expl, d_iters, d_err, grid, block, plan, stream);
   }
 
   // Launch shape for a CTA of `b` threads: shared-memory plan, CTAs per SM
@@ -718,11 +906,11 @@ struct Batch {
     SmemPlan pl;
     int occ, g;
     shape_for(b, bufs, cap_ctas, n, pl, occ, g);
-    if (g > scratch_ctas) {
+    if (g * inst_k > scratch_ctas) {
       cudaFree(d_scratch);
       d_scratch = nullptr;
       CU(cudaMalloc(&d_scratch, sizeof(float) * scratch_floats * g * inst_k));
-      scratch_ctas = g;
+      scratch_ctas = g * inst_k;
     }
     block = b;
     plan = pl;
@@ -816,8 +1004,7 @@ struct Batch {
     if (!fresh) CU(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
     CU(cudaEventRecord(ev[2], stream));
     const SolveJob job{0, (int)max_iter, 1, EPI_ROOT};
-    CU(launch_solve(d_spots, ninst, inst_k, d_inst, d_counter, d_disc, job, d_target, d_scratch, scratch_floats,
-                    d_expl, d_iters, d_err, grid, block, plan, stream));
+    CU(launch_job(job));
     CU(cudaEventRecord(ev[3], stream));
     h_expl.resize(n);
     h_iters.resize(n);
@@ -961,8 +1148,7 @@ struct Batch {
     } else {
       CU(cudaMemsetAsync(d_counter, 0, sizeof(int), stream));
       const SolveJob job{(int)t0, (int)t1, 0, epilogue};
-      CU(launch_solve(d_spots, ninst, inst_k, d_inst, d_counter, d_disc, job, d_target, d_scratch, scratch_floats,
-                      d_expl, d_iters, d_err, grid, block, plan, stream));
+      CU(launch_job(job));
     }
     CU(cudaEventRecord(ev[3], stream));
     if (epilogue & EPI_EXPL) {
@@ -999,6 +1185,15 @@ struct ps_game {
   int32_t total_bet[2] = {0, 0};
   std::vector<float> weights[2], normalized[2], cfv_cache[2];
   std::vector<std::vector<float>> bcfv_host;  // [ordinal*2+player]
+  std::vector<char> bcfv_set;                 // [ordinal*2+player]: values set (from host or device)
+  float* fs_block = nullptr;                  // fixed-strategy evaluation vectors (grow-only, freed with the game)
+  size_t fs_cap = 0;
+  ~ps_game() {
+    if (fs_block) {
+      if (b && b->stream) cudaStreamSynchronize(b->stream);
+      cudaFree(fs_block);
+    }
+  }
 };
 
 namespace {
@@ -1027,7 +1222,7 @@ int need_ready(ps_game* G) {
 
 int need_boundaries(ps_game* G) {
   for (int k = 0; k < G->g->num_boundary * 2; ++k)
-    if (G->bcfv_host[k].empty())
+    if (!G->bcfv_set[k])
       return fail(PS_ERR_STATE, "boundary cfvs empty at ordinal " + std::to_string(k / 2) + ", player " +
                                     std::to_string(k % 2) + " (set_boundary_cfvs not called)");
   return PS_OK;
@@ -1151,6 +1346,7 @@ int ps_game_new(const ps_card_config* cc, const ps_tree_config* tc, ps_game** ou
   G->g = g.get();
   G->b->games.push_back(std::move(g));
   G->bcfv_host.assign((size_t)G->g->num_boundary * 2, {});
+  G->bcfv_set.assign((size_t)G->g->num_boundary * 2, 0);
   for (int p = 0; p < 2; ++p) {
     G->weights[p].assign(G->g->H[p], 0.f);
     G->normalized[p].assign(G->g->H[p], 0.f);
@@ -1166,6 +1362,32 @@ int ps_game_memory_usage(ps_game* G, uint64_t* bytes) {
   if (!G || !bytes) return fail(PS_ERR_INVALID, "null argument");
   Game& g = *G->g;
   *bytes = 4 * (2 * g.num_storage + g.num_storage_ip + g.num_storage_chance);
+  return PS_OK;
+}
+
+int ps_game_program_info(ps_game* G, int64_t out[12]) {
+  if (!G || !out) return fail(PS_ERR_INVALID, "null argument");
+  const Game& g = *G->g;
+  out[0] = g.num_slots;
+  out[1] = g.vstride;
+  int64_t S = 0;
+  for (const auto& n : g.arena)
+    if (!n.terminal() && !n.chance()) S += (int64_t)n.nch * g.H[n.player];
+  for (int p = 0; p < 2; ++p) {
+    const Program& P = g.prog[p];
+    int64_t ne = 0, nt = 0, ng = 0;
+    for (const auto& st : P.steps) {
+      ne += st.n_elem;
+      nt += st.n_term;
+      ng += st.n_groups;
+    }
+    out[2 + p] = (int64_t)P.steps.size();
+    out[4 + p] = ne;
+    out[6 + p] = nt;
+    out[8 + p] = ng;
+  }
+  out[10] = S;
+  out[11] = (int64_t)g.boards.size();
   return PS_OK;
 }
 
@@ -1302,7 +1524,7 @@ int ps_root_cfvalues_with_reach(ps_game* G, int player, const float* opp_reach, 
 // reference has no gradients).  Both passes use the average strategy, the
 // boundary values as set, and the given initial weights instead of the game's.
 static int fixed_strategy_run(ps_game* G, const float* w0, const float* w1, const float* g0, const float* g1,
-                              float* cfv0, float* cfv1, float* dw0, float* dw1, float* dbcfv) {
+                              float* cfv0, float* cfv1, float* dw0, float* dw1, float* dbcfv, bool on_device) {
   if (!G || !w0 || !w1) return fail(PS_ERR_INVALID, "null argument");
   if (G->state == GState::TreeBuilt) return fail(PS_ERR_STATE, "Game is not ready");
   int rc = need_boundaries(G);
@@ -1314,22 +1536,31 @@ static int fixed_strategy_run(ps_game* G, const float* w0, const float* w1, cons
                                     "isomorphic chance pruning (its suit swaps assume the game's own ranges)");
   const bool adjoint = dw0 || dw1 || dbcfv;
   const size_t hs0 = g.hs[0], hs1 = g.hs[1], nb = (size_t)g.num_boundary;
-  // one device block: w0 w1 c0 c1 (g0 g1 a0 a1 when adjoint) then the boundary gradients
+  const size_t H0 = g.H[0], H1 = g.H[1];
+  // one device block, kept by the game: w0 w1 c0 c1 (g0 g1 a0 a1 when adjoint) then the boundary gradients
   const size_t nvec = adjoint ? 8 : 4;
   const size_t vec = std::max(hs0, hs1);
   const size_t nbg = adjoint ? nb * 2 * (size_t)g.vstride : 0;
-  float* d = nullptr;
-  CU(cudaMalloc(&d, 4 * (nvec * vec + nbg + 4)));
-  std::unique_ptr<float, decltype(&cudaFree)> keep(d, &cudaFree);
+  const size_t need = 4 * (nvec * vec + nbg + 4);
+  if (G->fs_cap < need) {
+    cudaFree(G->fs_block);
+    G->fs_block = nullptr;
+    G->fs_cap = 0;
+    CU(cudaMalloc(&G->fs_block, need));
+    G->fs_cap = need;
+  }
+  float* d = G->fs_block;
   float* dv[8];
   for (size_t k = 0; k < nvec; ++k) dv[k] = d + k * vec;
   float* d_bg = nbg ? d + nvec * vec : nullptr;
+  const cudaMemcpyKind in = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  const cudaMemcpyKind out = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   CU(cudaMemsetAsync(d, 0, 4 * (nvec * vec + nbg), B.stream));
-  CU(cudaMemcpyAsync(dv[0], w0, 4 * (size_t)g.H[0], cudaMemcpyHostToDevice, B.stream));
-  CU(cudaMemcpyAsync(dv[1], w1, 4 * (size_t)g.H[1], cudaMemcpyHostToDevice, B.stream));
+  CU(cudaMemcpyAsync(dv[0], w0, 4 * H0, in, B.stream));
+  CU(cudaMemcpyAsync(dv[1], w1, 4 * H1, in, B.stream));
   if (adjoint) {
-    if (g0) CU(cudaMemcpyAsync(dv[4], g0, 4 * (size_t)g.H[0], cudaMemcpyHostToDevice, B.stream));
-    if (g1) CU(cudaMemcpyAsync(dv[5], g1, 4 * (size_t)g.H[1], cudaMemcpyHostToDevice, B.stream));
+    if (g0) CU(cudaMemcpyAsync(dv[4], g0, 4 * H0, in, B.stream));
+    if (g1) CU(cudaMemcpyAsync(dv[5], g1, 4 * H1, in, B.stream));
   }
   CU(cudaMemsetAsync(B.d_err, 0, sizeof(int), B.stream));
   // forward: cfv_p from the opponent's weights (utility.rs:422-443)
@@ -1340,15 +1571,14 @@ static int fixed_strategy_run(ps_game* G, const float* w0, const float* w1, cons
     CU(B.average(0, 1, dv[4], dv[7], 0, d_bg));
     CU(B.average(0, 0, dv[5], dv[6], 1, d_bg));
   }
-  if (cfv0) CU(cudaMemcpyAsync(cfv0, dv[2], 4 * (size_t)g.H[0], cudaMemcpyDeviceToHost, B.stream));
-  if (cfv1) CU(cudaMemcpyAsync(cfv1, dv[3], 4 * (size_t)g.H[1], cudaMemcpyDeviceToHost, B.stream));
-  if (dw0) CU(cudaMemcpyAsync(dw0, dv[6], 4 * (size_t)g.H[0], cudaMemcpyDeviceToHost, B.stream));
-  if (dw1) CU(cudaMemcpyAsync(dw1, dv[7], 4 * (size_t)g.H[1], cudaMemcpyDeviceToHost, B.stream));
-  if (dbcfv)
-    for (size_t k = 0; k < nb; ++k)
-      for (int p = 0; p < 2; ++p)
-        CU(cudaMemcpyAsync(dbcfv + k * (g.H[0] + g.H[1]) + (p ? g.H[0] : 0), d_bg + (k * 2 + p) * g.vstride,
-                           4 * (size_t)g.H[p], cudaMemcpyDeviceToHost, B.stream));
+  if (cfv0) CU(cudaMemcpyAsync(cfv0, dv[2], 4 * H0, out, B.stream));
+  if (cfv1) CU(cudaMemcpyAsync(cfv1, dv[3], 4 * H1, out, B.stream));
+  if (dw0) CU(cudaMemcpyAsync(dw0, dv[6], 4 * H0, out, B.stream));
+  if (dw1) CU(cudaMemcpyAsync(dw1, dv[7], 4 * H1, out, B.stream));
+  if (dbcfv && nb) {  // [nb][2][vstride] -> [nb][H0 + H1], one strided copy per player
+    CU(cudaMemcpy2DAsync(dbcfv, (H0 + H1) * 4, d_bg, 2 * g.vstride * 4, H0 * 4, nb, out, B.stream));
+    CU(cudaMemcpy2DAsync(dbcfv + H0, (H0 + H1) * 4, d_bg + g.vstride, 2 * g.vstride * 4, H1 * 4, nb, out, B.stream));
+  }
   CU(cudaStreamSynchronize(B.stream));
   return B.check_err();
 }
@@ -1447,13 +1677,24 @@ int ps_boundary_first_layer(int32_t n, const uint8_t* boards, const float* pots,
 }
 
 int ps_eval_fixed_strategy(ps_game* G, const float* w0, const float* w1, float* cfv0, float* cfv1) {
-  return fixed_strategy_run(G, w0, w1, nullptr, nullptr, cfv0, cfv1, nullptr, nullptr, nullptr);
+  return fixed_strategy_run(G, w0, w1, nullptr, nullptr, cfv0, cfv1, nullptr, nullptr, nullptr, false);
 }
 
 int ps_eval_fixed_strategy_adjoint(ps_game* G, const float* w0, const float* w1, const float* g0, const float* g1,
                                    float* dw0, float* dw1, float* dbcfv) {
   if (!dw0 || !dw1) return fail(PS_ERR_INVALID, "null argument");
-  return fixed_strategy_run(G, w0, w1, g0, g1, nullptr, nullptr, dw0, dw1, dbcfv);
+  return fixed_strategy_run(G, w0, w1, g0, g1, nullptr, nullptr, dw0, dw1, dbcfv, false);
+}
+
+int ps_eval_fixed_strategy_ex(ps_game* G, const float* w0, const float* w1, float* cfv0, float* cfv1,
+                              int32_t on_device) {
+  return fixed_strategy_run(G, w0, w1, nullptr, nullptr, cfv0, cfv1, nullptr, nullptr, nullptr, on_device != 0);
+}
+
+int ps_eval_fixed_strategy_adjoint_ex(ps_game* G, const float* w0, const float* w1, const float* g0,
+                                      const float* g1, float* dw0, float* dw1, float* dbcfv, int32_t on_device) {
+  if (!dw0 || !dw1) return fail(PS_ERR_INVALID, "null argument");
+  return fixed_strategy_run(G, w0, w1, g0, g1, nullptr, nullptr, dw0, dw1, dbcfv, on_device != 0);
 }
 
 int ps_num_private_hands(ps_game* G, int p) { return G ? G->g->H[p & 1] : fail(PS_ERR_INVALID, "null game"); }
@@ -1633,6 +1874,31 @@ int ps_set_boundary_cfvs(ps_game* G, int64_t ordinal, int p, const float* cfvs, 
   G->bcfv_host[ordinal * 2 + p].assign(cfvs, cfvs + n);
   const SpotDev& s = G->b->h_spots[0];
   CU(cudaMemcpy((float*)s.bcfv + ((size_t)ordinal * 2 + p) * g.vstride, cfvs, 4 * (size_t)n, cudaMemcpyHostToDevice));
+  G->bcfv_set[ordinal * 2 + p] = 1;
+  return PS_OK;
+}
+
+int ps_set_boundary_cfvs_all(ps_game* G, const float* values, int32_t on_device) {
+  if (!G || (!values && G && G->g->num_boundary > 0)) return fail(PS_ERR_INVALID, "bad argument");
+  if (G->state == GState::TreeBuilt) return fail(PS_ERR_STATE, "allocate memory before setting boundary values");
+  Game& g = *G->g;
+  const size_t nb = (size_t)g.num_boundary, H0 = g.H[0], H1 = g.H[1];
+  if (nb == 0) return PS_OK;
+  Batch& B = *G->b;
+  const SpotDev& s = B.h_spots[0];
+  // [nb][H0 + H1] rows -> the device layout [nb][2][vstride], one strided copy per player
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  CU(cudaMemcpy2DAsync((float*)s.bcfv, 2 * g.vstride * 4, values, (H0 + H1) * 4, H0 * 4, nb, kind, B.stream));
+  CU(cudaMemcpy2DAsync((float*)s.bcfv + g.vstride, 2 * g.vstride * 4, values + H0, (H0 + H1) * 4, H1 * 4, nb, kind,
+                       B.stream));
+  CU(cudaStreamSynchronize(B.stream));
+  for (size_t k = 0; k < nb; ++k) {
+    if (!on_device) {
+      G->bcfv_host[k * 2].assign(values + k * (H0 + H1), values + k * (H0 + H1) + H0);
+      G->bcfv_host[k * 2 + 1].assign(values + k * (H0 + H1) + H0, values + (k + 1) * (H0 + H1));
+    }
+    G->bcfv_set[k * 2] = G->bcfv_set[k * 2 + 1] = 1;
+  }
   return PS_OK;
 }
 
@@ -2311,10 +2577,40 @@ int ps_batch_scan_buffers(ps_batch* pb) { return pb ? pb->b->plan.bufs : fail(PS
 
 int ps_batch_config(ps_batch* pb, int32_t* block, int32_t* grid, int32_t* cps) {
   if (!pb) return fail(PS_ERR_INVALID, "null batch");
-  if (block) *block = pb->b->block;
-  if (grid) *grid = pb->b->grid;
-  if (cps) *cps = pb->b->ctas_per_sm;
+  const Batch& B = *pb->b;
+  if (block) *block = B.flow ? B.flow_block : B.block;
+  if (grid) *grid = B.flow ? B.flow_grid : B.grid;
+  if (cps) *cps = B.flow ? B.flow_cps : B.ctas_per_sm;
   return PS_OK;
+}
+
+int ps_batch_schedule(ps_batch* pb, int32_t out[8]) {
+  if (!pb || !out) return fail(PS_ERR_INVALID, "null argument");
+  const Batch& B = *pb->b;
+  out[0] = B.flow ? PS_SCHED_FLOW : PS_SCHED_STEP;
+  out[1] = B.flow ? B.flow_block : B.block;
+  out[2] = B.flow ? B.flow_grid : B.grid;
+  out[3] = B.flow ? B.flow_cps : B.ctas_per_sm;
+  out[4] = B.flow ? B.flow_plan.bufs : B.plan.bufs;
+  out[5] = B.flow ? B.flow_lanes : B.inst_k;
+  out[6] = B.flow ? B.flow_parts : 1;
+  out[7] = B.grid_mode ? 1 : 0;
+  return PS_OK;
+}
+
+int ps_batch_autotune_trials(ps_batch* pb, int32_t* shape, float* trial_ms, int cap) {
+  if (!pb) return fail(PS_ERR_INVALID, "null batch");
+  const auto& L = pb->b->tune_log;
+  for (int i = 0; i < (int)L.size() && i < cap; ++i) {
+    if (shape) {
+      shape[4 * i] = L[i].block;
+      shape[4 * i + 1] = L[i].bufs;
+      shape[4 * i + 2] = L[i].lanes;
+      shape[4 * i + 3] = L[i].parts;
+    }
+    if (trial_ms) trial_ms[i] = L[i].ms;
+  }
+  return (int)L.size();
 }
 
 int ps_batch_autotune_log(ps_batch* pb, int32_t* block_threads, int32_t* scan_buffers, float* trial_ms, int cap) {
@@ -2331,9 +2627,9 @@ int ps_batch_autotune_log(ps_batch* pb, int32_t* block_threads, int32_t* scan_bu
 }  // extern "C"
 
 // ---- test hooks ----
-int ps_debug_grid_barrier_timeout(int32_t ctas, int32_t rounds, int64_t wait_ns, int32_t* err, int32_t* passed,
-                                  float* ms) {
-  if (!err || !passed || !ms || ctas < 2 || ctas > 148 || rounds < 1 || wait_ns < 0 || wait_ns > 1000000000LL)
+int ps_debug_grid_barrier_timeout(int32_t ctas, int32_t rounds, int64_t wait_ns, int32_t all_join, int32_t* err,
+                                  int32_t* passed, float* ms) {
+  if (!err || !passed || !ms || ctas < 2 || rounds < 1 || wait_ns < 0 || wait_ns > 1000000000LL)
     return fail(PS_ERR_INVALID, "bad argument");
   DeviceConsts* dc = nullptr;
   int rc = device_consts(&dc);
@@ -2352,7 +2648,7 @@ int ps_debug_grid_barrier_timeout(int32_t ctas, int32_t rounds, int64_t wait_ns,
   CU(cudaEventCreate(&ev[1]));
   CU(cudaMemsetAsync(d + 16, 0, 8, s));
   CU(cudaEventRecord(ev[0], s));
-  CU(launch_debug_barrier_timeout(ctas, rounds, wait_ns, bar, d_err, d_passed, s));
+  CU(launch_debug_barrier_timeout(ctas, rounds, wait_ns, all_join, bar, d_err, d_passed, s));
   CU(cudaEventRecord(ev[1], s));
   int h[2] = {0, 0};
   CU(cudaMemcpyAsync(h, d + 16, 8, cudaMemcpyDeviceToHost, s));

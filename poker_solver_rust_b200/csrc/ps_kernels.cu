@@ -78,7 +78,7 @@ struct Ctx {
   unsigned* bar; // grid mode: barrier counter and generation
   double* gred;  // grid mode: root reductions shared by all CTAs
   int* err;
-  float* buf;    // smem: this warp's scan buffer [3 * vstride] (null for warps >= bufs)
+  float* buf;    // smem: this warp's scan buffer [scan_buf_floats(vstride)] (null for warps >= bufs)
   int bufs;      // warps 0 .. bufs-1 own a scan buffer
   int owner;     // >= 0: adjoint pass, terminal values are player owner's payoffs (see warp_terms)
   int signed_reach;  // reach may be negative: terminal scans take segment starts from the bitmap
@@ -103,6 +103,28 @@ __device__ __forceinline__ float fmax_ref(float x, float y) { return x > y ? x :
 
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+
+// The last touch of a regret / strategy-sum row in a pass (its update store,
+// or an opponent row's second read): the streaming cache operator (.cs,
+// evict-first), so the state stream - read once and written once per pass,
+// far larger than L2 - leaves L2 first and the working slots stay.
+#ifndef PS_L2_STREAM
+#define PS_L2_STREAM 1
+#endif
+__device__ __forceinline__ float4 ld4_last(const float* p) {
+#if PS_L2_STREAM
+  return __ldcs(reinterpret_cast<const float4*>(p));
+#else
+  return ld4(p);
+#endif
+}
+__device__ __forceinline__ void st4_last(float* p, float4 v) {
+#if PS_L2_STREAM
+  __stcs(reinterpret_cast<float4*>(p), v);
+#else
+  st4(p, v);
+#endif
+}
 
 __device__ __forceinline__ float4 max0(float4 a) {
   return make_float4(fmax_ref(a.x, 0.f), fmax_ref(a.y, 0.f), fmax_ref(a.z, 0.f), fmax_ref(a.w, 0.f));
@@ -186,7 +208,7 @@ __device__ __noinline__ void op_fwd_opp_t(const Ctx& c, const Op& op, int o, int
     }
     const float4 r = ld4(src + h);
     for (int a = 0; a < na; ++a) {
-      float4 x = ld4(base + a * hso + h);
+      float4 x = ld4_last(base + a * hso + h);
       if (mode == M_DCFR) x = max0(x);
       st4(dst + (size_t)a * c.vstride + h, mul4(sigma4(x, d, def), r));
     }
@@ -265,7 +287,7 @@ __device__ __noinline__ void op_bwd_trav_t(const Ctx& c, const Op& op, int p, co
         res = a == 0 ? t : add4(res, t);
         if (mode == M_DCFR) {
           const float4 g = make_float4(dc.gamma, dc.gamma, dc.gamma, dc.gamma);
-          st4(S + a * hsp + h, add4(mul4(ld4(S + a * hsp + h), g), s));
+          st4_last(S + a * hsp + h, add4(mul4(ld4(S + a * hsp + h), g), s));
         } else if (mode == M_AVG_SAVE) {
           st4(R + a * hsp + h, cv);
         }
@@ -274,7 +296,7 @@ __device__ __noinline__ void op_bwd_trav_t(const Ctx& c, const Op& op, int p, co
         for (int a = 0; a < na; ++a) {
           const float4 r = ld4(R + a * hsp + h);
           const float4 cv = ld4(cb + (size_t)a * c.vstride + h);
-          st4(R + a * hsp + h, make_float4(regret_upd(r.x, cv.x, res.x, dc.alpha, dc.beta),
+          st4_last(R + a * hsp + h, make_float4(regret_upd(r.x, cv.x, res.x, dc.alpha, dc.beta),
                                            regret_upd(r.y, cv.y, res.y, dc.alpha, dc.beta),
                                            regret_upd(r.z, cv.z, res.z, dc.alpha, dc.beta),
                                            regret_upd(r.w, cv.w, res.w, dc.alpha, dc.beta)));
@@ -359,6 +381,12 @@ __device__ __forceinline__ void op_bwd_chance(const Ctx& c, const Op& op, int p,
 //   win  = P(lt) - Q_c1(ltc1) - Q_c2(ltc2)       (strictly weaker, not blocked)
 //   lose = (T - P(le)) - (M_c1 - Q_c1(lec1)) - (M_c2 - Q_c2(lec2))
 //   fold = T + r_same - M_c1 - M_c2               (inclusion-exclusion)
+// The scan buffer holds entry j of the list at kScanBase + j above four zeros,
+// so every prefix is one load at a position k_setup precomputes (an empty
+// prefix points at a zero): the hand's 16-byte record is eight u16 positions,
+//   x = P(lt) | P(le) << 16, y = Q_c1(ltc1) | Q_c1(lec1) << 16,
+//   z = M_c1 | Q_c2(ltc2) << 16, w = Q_c2(lec2) | M_c2 << 16,
+// and T is the prefix of all V entries.
 __device__ __forceinline__ void board_tables(const Ctx& c, int b, Tables& t) {
   if (b == 0) {
     t = c.t0;
@@ -427,8 +455,11 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
   const float* rch = slot_in(c, ops[0].src);
   prefetch_l2_bytes(T.thr[p], 16 * Hp);
   const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  // warp 0's buffer: buffers are 3 * vstride floats apart (one spot a launch)
-  float* buf = CTA ? c.buf - (size_t)warp * 3 * c.vstride : c.buf;
+  // the scan buffer (in CTA mode warp 0's: buffers are scan_buf_floats apart,
+  // one spot a launch); entry j of the gathered list lives at e[j]
+  float* buf = CTA ? c.buf - (size_t)warp * scan_buf_floats(c.vstride) : c.buf;
+  float* e = buf + kScanBase;
+  if (lane == 0 && (!CTA || warp == 0)) st4(buf, make_float4(0.f, 0.f, 0.f, 0.f));  // what empty prefixes read
   // adjoint pass at a depth boundary: the reach is weighted by the payoff
   // owner's boundary values.  Where the gathered values may be negative
   // (caller-given reach, boundary weights) segment starts come from the
@@ -469,7 +500,7 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
         v.y = (m & 2u) ? -x[u][1] : x[u][1];
         v.z = (m & 4u) ? -x[u][2] : x[u][2];
         v.w = (m & 8u) ? -x[u][3] : x[u][3];
-        st4(buf + k, v);  // entries past n3 are never read
+        st4(e + k, v);  // entries past n3 are never read
       }
     }
   }
@@ -483,7 +514,7 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
     float run = 0.f;
     int first = hi;
     for (int j = lo; j < hi; ++j) {
-      float x = buf[j];
+      float x = e[j];
       bool head;
       if (bits) {
         head = (hd[j >> 5] >> (j & 31)) & 1u;
@@ -497,7 +528,7 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
       } else {
         run = __fadd_rn(run, x);
       }
-      buf[j] = run;
+      e[j] = run;
     }
     float v = run;
     bool f = first < hi;
@@ -512,7 +543,7 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
     }
     float in = __shfl_up_sync(0xffffffffu, v, 1);
     if (lane == 0) in = 0.f;
-    for (int j = lo; j < first; ++j) buf[j] = __fadd_rn(buf[j], in);
+    for (int j = lo; j < first; ++j) e[j] = __fadd_rn(e[j], in);
   }
   if (CTA)
     __syncthreads();
@@ -524,10 +555,10 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
     float* row = c.breach + ((size_t)nd0.boundary * 2 + o) * c.vstride;
     for (int h = lane; h < sp.H[o]; h += 32) row[h] = rch[h];
   }
-  // 3. lookups
+  // 3. lookups: every prefix is one load at a position of the hand's record
   const uint4* thr = T.thr[p];
-  const float* cp = buf + V;  // card-group part
-  const float Tsum = V > 0 ? buf[V - 1] : 0.f;
+  const uint16_t* same = sp.same[p];
+  const float Tsum = buf[kScanBase - 1 + V];  // all V entries (0 when V = 0)
   const int pay = adjm ? c.owner : p;  // whose payoffs the values are
   const int part = CTA ? warp : SPLIT ? c.part : 0, parts = CTA ? nwarps : SPLIT ? c.parts : 1;
   const int h0 = part * 32 + lane, hstep = 32 * parts;
@@ -553,11 +584,9 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
         float v = 0.f;
         const uint4 t = tn;
         tn = h + hstep < Hp ? thr[h + hstep] : make_uint4(THR_INVALID, 0, 0, 0);
-        if (t.x != THR_INVALID && V > 0) {
-          const int s1 = t.z & 0xFFFF, s2 = t.z >> 16, n1 = t.w & 0xFF, n2 = (t.w >> 8) & 0xFF;
-          const float M1 = n1 ? cp[s1 + n1 - 1] : 0.f;
-          const float M2 = n2 ? cp[s2 + n2 - 1] : 0.f;
-          const uint32_t si = t.w >> 16;
+        if (t.x != THR_INVALID) {
+          const float M1 = buf[t.z & 0xFFFF], M2 = buf[t.w >> 16];
+          const uint32_t si = same[h];
           const float rs = si != 0xFFFF ? rch[si] : 0.f;
           const float adj = Tsum + rs - M1 - M2;
           v = __fmul_rn(__fmul_rn(brow[h], nd.payoff_scale), adj);
@@ -570,25 +599,21 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
       float v = 0.f;
       const uint4 t = tn;
       tn = h + hstep < Hp ? thr[h + hstep] : make_uint4(THR_INVALID, 0, 0, 0);
-      if (t.x != THR_INVALID && V > 0) {
-        const int s1 = t.z & 0xFFFF, s2 = t.z >> 16, n1 = t.w & 0xFF, n2 = (t.w >> 8) & 0xFF;
-        const float M1 = n1 ? cp[s1 + n1 - 1] : 0.f;
-        const float M2 = n2 ? cp[s2 + n2 - 1] : 0.f;
+      if (t.x != THR_INVALID) {
+        const float M1 = buf[t.z & 0xFFFF], M2 = buf[t.w >> 16];
         if (op.term == TERM_SHOWDOWN) {
-          const int lt = t.x & 0xFFFF, le = t.x >> 16;
-          const int ltc1 = t.y & 0xFF, lec1 = (t.y >> 8) & 0xFF, ltc2 = (t.y >> 16) & 0xFF, lec2 = t.y >> 24;
-          const float Plt = lt ? buf[lt - 1] : 0.f, Ple = le ? buf[le - 1] : 0.f;
-          const float Q1lt = ltc1 ? cp[s1 + ltc1 - 1] : 0.f, Q1le = lec1 ? cp[s1 + lec1 - 1] : 0.f;
-          const float Q2lt = ltc2 ? cp[s2 + ltc2 - 1] : 0.f, Q2le = lec2 ? cp[s2 + lec2 - 1] : 0.f;
+          const float Plt = buf[t.x & 0xFFFF], Ple = buf[t.x >> 16];
+          const float Q1lt = buf[t.y & 0xFFFF], Q1le = buf[t.y >> 16];
+          const float Q2lt = buf[t.z >> 16], Q2le = buf[t.w & 0xFFFF];
           const float win = Plt - Q1lt - Q2lt;
           if (!sp.raked) {
             const float lose = (Tsum - Ple) - (M1 - Q1le) - (M2 - Q2le);
             v = __fadd_rn(__fmul_rn(cw, win), __fmul_rn(cl, lose));
           } else {
-            v = raked_showdown_value(cw, cl, nd.amount_tie, win, Ple, Q1le, Q2le, Tsum, M1, M2, rch, t.w >> 16);
+            v = raked_showdown_value(cw, cl, nd.amount_tie, win, Ple, Q1le, Q2le, Tsum, M1, M2, rch, same[h]);
           }
         } else {
-          const uint32_t si = t.w >> 16;
+          const uint32_t si = same[h];
           const float rs = si != 0xFFFF ? (GEN && bw ? rch[si] * bw[si] : rch[si]) : 0.f;
           const float adj = Tsum + rs - M1 - M2;
           if (op.term == TERM_FOLD) {
@@ -602,7 +627,7 @@ __device__ __noinline__ void warp_terms(const Ctx& c, const Op* ops, int n, int 
           }
         }
       }
-      if (GEN && grow && !(t.x != THR_INVALID && V > 0)) grow[h] = 0.f;
+      if (GEN && grow && t.x == THR_INVALID) grow[h] = 0.f;
       dst[h] = v;
     }
   }
@@ -840,18 +865,34 @@ __device__ __forceinline__ void pass_multi(Ctx* cs, int K, unsigned active, int 
   }
 }
 
-// sum_h w[h] * v[h] accumulated in f64 (utility.rs:118-122), result on all threads.
-__device__ double block_dot_f64(const Ctx& c, const float* w, const float* v, int n) {
-  double acc = 0.0;
-  for (int h = threadIdx.x; h < n; h += blockDim.x) acc += (double)w[h] * (double)v[h];
-#pragma unroll
-  for (int s = 16; s > 0; s >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, s);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  __syncthreads();
-  if (lane == 0) c.red[warp] = acc;
-  __syncthreads();
+// sum_h w[h] * v[h] accumulated in f64 (utility.rs:118-122) in one fixed
+// order, whatever the caller's thread count: 256 strided partial sums
+// (h = j, j + 256, ...), the 32 partials of each group j / 32 combined by a
+// shuffle tree, the 8 group sums added in order.  One warp computes it
+// (result on all its lanes), so a CTA of any size and a single warp of the
+// dataflow solve produce the same bits.
+__device__ double warp_dot_f64(const float* w, const float* v, int n) {
+  const int lane = threadIdx.x & 31;
   double tot = 0.0;
-  for (int i = 0; i < nw; ++i) tot += c.red[i];
+  for (int k = 0; k < 8; ++k) {
+    double acc = 0.0;
+    for (int h = 32 * k + lane; h < n; h += 256) acc += (double)w[h] * (double)v[h];
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, s);
+    tot += __shfl_sync(0xffffffffu, acc, 0);
+  }
+  return tot;
+}
+
+// warp_dot_f64 for a whole CTA: warp 0 computes it, every thread gets it.
+__device__ double block_dot_f64(const Ctx& c, const float* w, const float* v, int n) {
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const double d = warp_dot_f64(w, v, n);
+    if (threadIdx.x == 0) c.red[0] = d;
+  }
+  __syncthreads();
+  const double tot = c.red[0];
   __syncthreads();
   return tot;
 }
@@ -958,12 +999,12 @@ __device__ bool bind_ctx(Ctx& c, const SpotDev* sp, float* scratch, size_t scrat
   char* tables = p;
   p += plan.tables;
   const int warp_id = threadIdx.x >> 5;
-  c.buf = warp_id < plan.bufs ? reinterpret_cast<float*>(p) + (size_t)warp_id * 3 * plan.vstride : nullptr;
+  c.buf = warp_id < plan.bufs ? reinterpret_cast<float*>(p) + (size_t)warp_id * scan_buf_floats(plan.vstride) : nullptr;
   c.bufs = plan.bufs;
   c.split = plan.split;
   c.part = 0;
   c.parts = 1;
-  p += (size_t)plan.bufs * 3 * plan.vstride * 4;
+  p += (size_t)plan.bufs * scan_buf_floats(plan.vstride) * 4;
   c.red = reinterpret_cast<double*>(p);
   if ((size_t)sp->num_slots * sp->vstride > scratch_floats || sp->vstride > plan.vstride) {
     if (threadIdx.x == 0) atomicOr(err, ERR_SCRATCH);
@@ -1128,6 +1169,429 @@ __global__ void PS_SOLVE_BOUNDS k_solve(const SpotDev* __restrict__ spots, int n
       }
       __syncthreads();
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Dataflow batched solve: per-spot steps claimed from a work queue
+// ---------------------------------------------------------------------------
+// k_flow holds up to kMaxLanes spots per CTA at once ("lanes").  Each lane is
+// at its own point of its spot's solve - a pass and a step of that pass - and
+// the step's items (terminal runs, and node ops cut into `parts` interleaved
+// column blocks) are claimed by warps from two counters per lane: terminal
+// runs by the warps that own a scan buffer, node ops by any warp.  The warp
+// that finishes a step's last item moves the lane on: to the next step, or at
+// the end of a pass to the pass's root work (the exploitability dot products
+// and the stop decision of the reference loop, solver.rs:108-176; the root
+// values of the epilogue) and the next pass, or - when the spot is solved - to
+// the next spot of the batch queue.  So no warp waits at a CTA barrier for the
+// slowest item of a step: it takes an item of another lane.  Every item runs
+// the same arithmetic as in k_solve, so results are the same bits.
+//
+// Claims: a 64-bit word per lane and item kind holds (count << 20 | next) of
+// the current step.  A claim is an atomicAdd of 1; it is valid when the old
+// next < count.  Only the finisher of a step rewrites the words (after the new
+// step's fields), and a step cannot end while one of its items is claimed but
+// unfinished, so a valid claim always refers to the step whose fields the
+// claimer then reads.  Ordering: an item's writes (global and shared) are
+// fenced at CTA scope before its completion is counted; the finisher fences
+// after the count and before publishing the next step; a claimer fences after
+// its claim.
+constexpr int kMaxLanes = 8;
+constexpr int kMaxFlowBlock = 1024;
+#ifndef PS_DISCARD
+#define PS_DISCARD 1  // the flow finisher drops a lane's dead working slots from L2 at each pass end
+#endif
+enum LanePhase : int { LP_BR0 = 0, LP_BR1, LP_AVG0, LP_AVG1, LP_DCFR0, LP_DCFR1, LP_EPI0, LP_EPI1, LP_RETIRED };
+
+struct Lane {
+  unsigned long long wt, wn;  // claims of terminal runs / node-op parts: count << 20 | next
+  int done, total;            // finished items of the current step, and its item count
+  int begin, n_elem, gbegin, parts;  // the current step (node ops are cut into `parts` column blocks)
+  int spot, phase, step, t;   // spot id, pass (LanePhase), step of the pass, iterations done
+  float expl, target, mes0, mes1, cur0;
+  int iters;
+  float* slots;               // the lane's scratch slots
+};
+
+__device__ __forceinline__ int lane_player(int phase) { return (phase - LP_BR0) & 1; }
+__device__ __forceinline__ int lane_mode(int phase) {
+  return phase <= LP_BR1 ? M_BR : phase <= LP_AVG1 ? M_AVG : phase <= LP_DCFR1 ? M_DCFR : M_AVG;
+}
+
+__device__ __forceinline__ unsigned long long claim_word(int count) {
+  return (unsigned long long)count << 20;
+}
+// one claim from w (lane 0 of the warp); -1 if none is left
+__device__ __forceinline__ int try_claim(unsigned long long* w) {
+  const unsigned long long v = *reinterpret_cast<volatile unsigned long long*>(w);
+  if ((v & 0xFFFFFull) >= ((v >> 20) & 0xFFFFFull)) return -1;
+  const unsigned long long old = atomicAdd(w, 1ull);
+  const unsigned nxt = (unsigned)(old & 0xFFFFFull), cnt = (unsigned)((old >> 20) & 0xFFFFFull);
+  return nxt < cnt ? (int)nxt : -1;
+}
+
+struct FlowArgs {
+  const SpotDev* spots;
+  int ninst;
+  const int* inst;
+  int* counter;
+  const Discount* disc;
+  SolveJob job;
+  const float* target;
+  float* scratch;
+  size_t scratch_floats;
+  float* out_expl;
+  int* out_iters;
+  int* err;
+  int lanes;       // lanes per CTA
+  int node_parts;  // column blocks per node op (1 = whole ops)
+};
+
+// Publishes step L.step of the lane's current pass (finisher / binder only).
+__device__ void lane_publish_step(Lane& L, const SpotDev& sp, int node_parts) {
+  const int p = lane_player(L.phase);
+  const Step st = sp.steps[p][L.step];
+  L.begin = st.begin;
+  L.n_elem = st.n_elem;
+  L.gbegin = st.gbegin;
+  L.parts = node_parts;
+  L.total = st.n_groups + st.n_elem * node_parts;
+  L.done = 0;
+  __threadfence_block();
+  // The step can end once every item is claimed and done, after which its
+  // finisher publishes the next step.  So an empty kind's word (count 0, no
+  // claims) goes first and the other last: no exchange of this step can land
+  // after a later step's.  With both kinds present, the step cannot end before
+  // the second word is out.
+  const unsigned long long t = claim_word(st.n_groups), n = claim_word(st.n_elem * node_parts);
+  if (st.n_groups == 0) {
+    atomicExch(&L.wt, t);
+    atomicExch(&L.wn, n);
+  } else {
+    atomicExch(&L.wn, n);
+    atomicExch(&L.wt, t);
+  }
+}
+
+// The reference loop's decision after a completed exploitability check
+// (solver.rs:137-159): stop at the target or at the iteration limit; a
+// fixed-range job's closing check ends the spot.  -1 = the spot is finished.
+__device__ int lane_after_check(const Lane& L, const FlowArgs& A) {
+  if (A.job.checks && !(L.expl <= L.target) && L.t < A.job.t1) return LP_DCFR0;
+  return -1;
+}
+
+// After an iteration's second pass: a check every 5 iterations and after the
+// last one (solve loop), or the next iteration of a fixed range.
+__device__ int lane_after_iterations(const Lane& L, const FlowArgs& A) {
+  const SolveJob& j = A.job;
+  if (j.checks) return (L.t % 5 == 0 || L.t >= j.t1) ? LP_BR0 : LP_DCFR0;
+  if (L.t < j.t1) return LP_DCFR0;
+  return (j.epilogue & EPI_EXPL) ? LP_BR0 : -1;
+}
+
+// Binds the lane to the next spot of the queue (lane 0 of the calling warp);
+// false when the queue is empty and the lane retires.  The lane starts before
+// the first step of its first pass (step -1).
+__device__ bool lane_bind(Lane& L, const FlowArgs& A, float* my_scratch, const SmemPlan& plan) {
+  for (;;) {
+    const int q = atomicAdd(A.counter, 1);
+    if (q >= A.ninst) {
+      L.phase = LP_RETIRED;
+      return false;
+    }
+    const int id = A.inst[q];
+    if (id < 0) continue;
+    const SpotDev& sp = A.spots[id];
+    if ((size_t)sp.num_slots * sp.vstride > A.scratch_floats || sp.vstride > plan.vstride) {
+      atomicOr(A.err, ERR_SCRATCH);
+      continue;
+    }
+    const SolveJob& j = A.job;
+    int phase;
+    if (j.checks) {
+      L.t = 0;
+      phase = LP_BR0;  // the exploitability before the first iteration
+    } else {
+      L.t = j.t0;
+      phase = L.t < j.t1 ? LP_DCFR0 : (j.epilogue & EPI_EXPL) ? LP_BR0 : (j.epilogue & EPI_ROOT) ? LP_EPI0 : -1;
+      if (phase < 0) continue;  // nothing to run for this spot
+    }
+    L.spot = id;
+    L.slots = my_scratch;
+    L.target = A.target[id];
+    L.expl = 0.f;
+    L.mes0 = L.mes1 = L.cur0 = 0.f;
+    L.iters = 0;
+    L.phase = phase;
+    L.step = -1;
+    return true;
+  }
+}
+
+// The root work of the pass that just finished and the lane's next phase
+// (whole warp; lane 0 owns the scalar state).  -1 = the spot is finished.
+__device__ int lane_pass_end(Lane& L, const FlowArgs& A) {
+  const SpotDev& sp = A.spots[L.spot];
+  const int lane = threadIdx.x & 31;
+  const int p = lane_player(L.phase);
+  const float* root = L.slots + (size_t)sp.root_slot[p] * sp.vstride;
+  int next = -1;
+  if (L.phase <= LP_AVG1) {  // a pass of an exploitability check (utility.rs:380-392)
+    const float v = (float)warp_dot_f64(sp.w[p], root, sp.H[p]);
+    if (lane == 0) {
+      bool complete = false;
+      if (L.phase == LP_BR0) {
+        L.mes0 = v;
+        next = LP_BR1;
+      } else if (L.phase == LP_BR1) {
+        L.mes1 = v;
+        if (sp.raked) {
+          next = LP_AVG0;
+        } else {
+          L.expl = (L.mes0 + L.mes1) * 0.5f;
+          complete = true;
+        }
+      } else if (L.phase == LP_AVG0) {
+        L.cur0 = v;
+        next = LP_AVG1;
+      } else {
+        L.expl = ((L.mes0 - L.cur0) + (L.mes1 - v)) * 0.5f;
+        complete = true;
+      }
+      if (complete) {
+        next = lane_after_check(L, A);
+        if (next < 0) L.iters = L.t;
+      }
+    }
+    next = __shfl_sync(0xffffffffu, next, 0);
+  } else if (L.phase == LP_DCFR0) {
+    next = LP_DCFR1;
+  } else if (L.phase == LP_DCFR1) {
+    if (lane == 0) {
+      L.t += 1;
+      next = lane_after_iterations(L, A);
+      if (next < 0) L.iters = L.t;
+    }
+    next = __shfl_sync(0xffffffffu, next, 0);
+  } else {  // LP_EPI0 / LP_EPI1: root values under the average strategy
+    if (sp.root_out[p])
+      for (int h = lane; h < sp.hs[p]; h += 32) sp.root_out[p][h] = root[h];
+    return L.phase == LP_EPI0 ? LP_EPI1 : -1;
+  }
+  if (next < 0 && (A.job.epilogue & EPI_ROOT)) next = LP_EPI0;
+  return next;
+}
+
+// The finisher's move (whole warp): from the step that just ended (L.step;
+// -1 = before a pass) to the next step with items, through the root work of
+// any pass that ends and to the next spot when this one is finished.  Leaves
+// the lane published (false) or retired (true).  Once a step is published
+// other warps own the lane again, so nothing of it is read afterwards.
+__device__ bool lane_move(Lane& L, const FlowArgs& A, const SmemPlan& plan) {
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    __syncwarp();
+    const SpotDev& sp = A.spots[L.spot];
+    const int p = lane_player(L.phase);
+    if (L.step + 1 < sp.nsteps[p]) {
+      __syncwarp();  // every lane has read the fields above before lane 0 publishes
+      if (lane == 0) {
+        L.step += 1;
+        lane_publish_step(L, sp, A.node_parts);
+      }
+      return false;
+    }
+    const int next = lane_pass_end(L, A);
+    __syncwarp();
+#if PS_DISCARD
+    {  // every working slot of the lane is dead now (each pass writes a slot before it reads it): drop the
+       // lines from L2 without writing them back
+      const char* b = reinterpret_cast<const char*>(L.slots);
+      const size_t bytes = (size_t)sp.num_slots * sp.vstride * 4;
+      for (size_t i = (size_t)lane * 128; i < bytes; i += 32 * 128)
+        asm volatile("discard.global.L2 [%0], 128;" ::"l"(__cvta_generic_to_global(b + i)) : "memory");
+      __syncwarp();
+    }
+#endif
+    if (next < 0) {  // the spot is finished: its results, then the next spot
+      int bound = 0;
+      if (lane == 0) {
+        if (A.job.checks || (A.job.epilogue & EPI_EXPL)) {
+          A.out_expl[L.spot] = L.expl;
+          A.out_iters[L.spot] = L.iters;
+        }
+        bound = lane_bind(L, A, L.slots, plan);
+      }
+      if (!__shfl_sync(0xffffffffu, bound, 0)) return true;
+      continue;
+    }
+    if (lane == 0) {
+      L.phase = next;
+      L.step = -1;
+    }
+  }
+}
+
+// Runs item `idx` of the lane's current step: a terminal run (term) or a
+// node-op column block.
+__device__ void lane_item(const Lane& L, const FlowArgs& A, int term, int idx, float* buf, int bufs) {
+  const SpotDev& sp = A.spots[L.spot];
+  const int p = lane_player(L.phase), o = p ^ 1, mode = lane_mode(L.phase);
+  Ctx c;
+  c.sp = &sp;
+  c.slots = L.slots;
+  c.vstride = sp.vstride;
+  c.root_reach = sp.w[o];
+  c.grid = 0;
+  c.bar = nullptr;
+  c.gred = nullptr;
+  c.wait_ns = 0;
+  c.err = A.err;
+  c.buf = buf;
+  c.bufs = bufs;
+  c.owner = -1;
+  c.signed_reach = 0;
+  c.bgrad = nullptr;
+  c.breach = L.phase >= LP_EPI0 ? sp.breach : nullptr;
+  c.red = nullptr;
+  c.split = 0;
+  c.part = 0;
+  c.parts = 1;
+  for (int q = 0; q < 2; ++q) {
+    c.t0.gidx[q] = sp.gidx[q];
+    c.t0.heads[q] = sp.heads[q];
+    c.t0.thr[q] = reinterpret_cast<const uint4*>(sp.thr[q]);
+    c.t0.nvalid[q] = sp.nvalid[q][0];
+  }
+  const Discount dc = mode == M_DCFR ? A.disc[L.t] : Discount{0.f, 0.f, 0.f, 0.f};
+  if (term) {
+    const Op* lead = sp.ops[p] + L.begin + L.n_elem + sp.groups[p][L.gbegin + idx];
+    if (c.breach)
+      warp_terms<true>(c, lead, lead->na, p);
+    else
+      warp_terms<false>(c, lead, lead->na, p);
+    return;
+  }
+  const int P = L.parts;
+  const Op op = sp.ops[p][L.begin + idx / P];
+  if (P == 1) {
+    switch (op.type) {
+      case OP_FWD_OPP: op_fwd_opp(c, op, o, mode); break;
+      case OP_FWD_CHANCE: op_fwd_chance(c, op, o); break;
+      case OP_BWD_TRAV: op_bwd_trav(c, op, p, dc, mode); break;
+      case OP_BWD_OPP: op_bwd_opp(c, op, p, mode); break;
+      case OP_BWD_CHANCE: op_bwd_chance(c, op, p, mode); break;
+      default: break;
+    }
+  } else {
+    c.part = idx % P;
+    c.parts = P;
+    switch (op.type) {
+      case OP_FWD_OPP: op_fwd_opp_t<true>(c, op, o, mode); break;
+      case OP_FWD_CHANCE: op_fwd_chance_t<true>(c, op, o); break;
+      case OP_BWD_TRAV: op_bwd_trav_t<true>(c, op, p, dc, mode); break;
+      case OP_BWD_OPP: op_bwd_opp_t<true>(c, op, p, mode); break;
+      case OP_BWD_CHANCE: op_bwd_chance_t<true>(c, op, p, mode); break;
+      default: break;
+    }
+  }
+}
+
+constexpr long long kFlowIdleNs = 2000000000LL;  // 2 s without any finished step in the CTA: give up
+
+__global__ void __launch_bounds__(kMaxFlowBlock, 1) k_flow(FlowArgs A, SmemPlan plan) {
+  extern __shared__ float4 smem4[];
+  char* smem = reinterpret_cast<char*>(smem4);
+  __shared__ Lane lanes[kMaxLanes];
+  __shared__ int s_retired;
+  __shared__ unsigned s_progress;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int K = A.lanes;
+  float* buf = warp < plan.bufs
+                   ? reinterpret_cast<float*>(smem + plan.tables) + (size_t)warp * scan_buf_floats(plan.vstride)
+                   : nullptr;
+  // bind every lane to its first spot (warp k binds lane k)
+  if (threadIdx.x == 0) {
+    s_retired = 0;
+    s_progress = 0;
+  }
+  if (warp < K) {
+    Lane& L = lanes[warp];
+    int bound = 0;
+    if (lane == 0) {
+      L.wt = L.wn = 0ull;
+      L.done = L.total = 0;
+      bound = lane_bind(L, A, A.scratch + ((size_t)blockIdx.x * K + warp) * A.scratch_floats, plan);
+      if (!bound) atomicAdd(&s_retired, 1);
+    }
+    if (__shfl_sync(0xffffffffu, bound, 0) && lane_move(L, A, plan) && lane == 0) atomicAdd(&s_retired, 1);
+  }
+  __syncthreads();
+  unsigned seen = 0;
+  unsigned long long idle_since = global_ns();
+  int start = warp % K;
+  for (;;) {
+    int k = -1, idx = -1, term = 0;
+    if (lane == 0) {
+      for (int r = 0; r < K && idx < 0; ++r) {
+        k = start + r < K ? start + r : start + r - K;
+        Lane& L = lanes[k];
+        if (buf) {
+          idx = try_claim(&L.wt);
+          term = idx >= 0;
+        }
+        if (idx < 0) idx = try_claim(&L.wn);
+      }
+      __threadfence_block();  // acquire: the claimed step's fields and inputs
+    }
+    idx = __shfl_sync(0xffffffffu, idx, 0);
+    if (idx >= 0) {
+      k = __shfl_sync(0xffffffffu, k, 0);
+      term = __shfl_sync(0xffffffffu, term, 0);
+      __syncwarp();
+      Lane& L = lanes[k];
+      lane_item(L, A, term, idx, buf, plan.bufs);
+      __threadfence_block();  // every lane's writes of the item before its count
+      __syncwarp();
+      int last = 0;
+      if (lane == 0) {
+        // the step's item count is read before this item is counted: until then
+        // the step cannot end, so it is this step's (read after the count, it
+        // could be the next step's, published by the real finisher meanwhile)
+        const int total = L.total;
+        const int d = atomicAdd(&L.done, 1);
+        last = d + 1 == total;
+        if (last) __threadfence_block();  // acquire: every item of the step
+      }
+      if (__shfl_sync(0xffffffffu, last, 0)) {
+        const bool retired = lane_move(L, A, plan);
+        if (lane == 0) {
+          if (retired) atomicAdd(&s_retired, 1);
+          atomicAdd(&s_progress, 1u);
+        }
+      }
+      start = k;  // stay with this lane while it has work (its rows are warm)
+      idle_since = global_ns();
+      continue;
+    }
+    // nothing to claim: finished, or wait for a step to end
+    int stop = 0;
+    if (lane == 0) {
+      const unsigned pr = *reinterpret_cast<volatile unsigned*>(&s_progress);
+      if (*reinterpret_cast<volatile int*>(&s_retired) >= K) {
+        stop = 1;
+      } else if (pr != seen) {
+        seen = pr;
+        idle_since = global_ns();
+      } else if ((long long)(global_ns() - idle_since) > kFlowIdleNs) {
+        atomicOr(A.err, ERR_WAIT);
+        stop = 1;
+      }
+    }
+    if (__shfl_sync(0xffffffffu, stop, 0)) return;
+    __nanosleep(64);
   }
 }
 
@@ -1439,11 +1903,15 @@ __global__ void k_setup(const SpotDev* __restrict__ spots, const int2* __restric
       }
       __syncthreads();
     }
-    // lookup records of player p's hands against opponent o = p ^ 1, 16 bytes per hand:
-    //   x = lt | le << 16  (opponent hands strictly weaker / weaker-or-tied)
-    //   y = ltc1 | lec1 << 8 | ltc2 << 16 | lec2 << 24  (the same inside each card group)
-    //   z = start of card group c1 | start of c2 << 16  (within the card part of the list)
-    //   w = size of c1 | size of c2 << 8 | same-hand index << 16;  x = ~0 if blocked
+    // lookup records of player p's hands against opponent o = p ^ 1, 16 bytes per
+    // hand: the scan-buffer positions of the hand's eight prefixes (see the
+    // terminal evaluation above); x = ~0 if the hand is blocked on this board.
+    // With lt / le the opponent hands strictly weaker / weaker-or-tied and l / e
+    // the same counts inside card group c (starting at a_c, n_c entries):
+    //   P(k)    = kScanBase - 1 + k           (k = 0 reads the zero below the list)
+    //   Q_c(k)  = k ? kScanBase - 1 + V + a_c + k : 0
+    //   x = P(lt) | P(le) << 16, y = Q_c1(l1) | Q_c1(e1) << 16,
+    //   z = Q_c1(n_c1) | Q_c2(l2) << 16, w = Q_c2(e2) | Q_c2(n_c2) << 16
     for (int p = 0; p < 2; ++p) {
       const int o = p ^ 1;
       const int Hp = sp.H[p], hsp = sp.hs[p], Vo = S.nvalid[o];
@@ -1460,10 +1928,12 @@ __global__ void k_setup(const SpotDev* __restrict__ spots, const int2* __restric
             const int a2 = S.coff[o][c2], n2 = S.coff[o][c2 + 1] - a2;
             const uint32_t l1 = lower_bound_u16(S.istr[o] + a1, n1, s), e1 = upper_bound_u16(S.istr[o] + a1, n1, s);
             const uint32_t l2 = lower_bound_u16(S.istr[o] + a2, n2, s), e2 = upper_bound_u16(S.istr[o] + a2, n2, s);
-            v.x = lt | (le << 16);
-            v.y = l1 | (e1 << 8) | (l2 << 16) | (e2 << 24);
-            v.z = (uint32_t)a1 | ((uint32_t)a2 << 16);
-            v.w = (uint32_t)n1 | ((uint32_t)n2 << 8) | ((uint32_t)sp.same[p][h] << 16);
+            const uint32_t pb = kScanBase - 1, cb = kScanBase - 1 + Vo;
+            auto Q = [&](int a, uint32_t k) { return k ? cb + (uint32_t)a + k : 0u; };
+            v.x = (pb + lt) | ((pb + le) << 16);
+            v.y = Q(a1, l1) | (Q(a1, e1) << 16);
+            v.z = Q(a1, (uint32_t)n1) | (Q(a2, l2) << 16);
+            v.w = Q(a2, e2) | (Q(a2, (uint32_t)n2) << 16);
           }
         }
         thr[h] = v;
@@ -1509,6 +1979,31 @@ cudaError_t launch_solve(const SpotDev* spots, int ninst, int K, const int* inst
     k_solve<false><<<grid, block, smem, s>>>(spots, ninst, K, inst, counter, disc, job, target, scratch, scratch_floats,
                                      out_expl, out_iters, plan, err);
   return cudaGetLastError();
+}
+
+cudaError_t launch_flow(const SpotDev* spots, int ninst, const int* inst, int* counter, const Discount* disc,
+                        const SolveJob& job, const float* target, float* scratch, size_t scratch_floats,
+                        float* out_expl, int* out_iters, int* err, int grid, int block, int lanes, int node_parts,
+                        const SmemPlan& plan, cudaStream_t s) {
+  if (block < 64 || block > kMaxFlowBlock || block % 32 || lanes < 1 || lanes > kMaxLanes || lanes > block / 32 ||
+      node_parts < 1 || node_parts > 16 || plan.bufs < 1 || plan.bufs > block / 32 || job.adjoint || job.t0 < 0 ||
+      job.t1 < job.t0 || (job.checks && job.t0 != 0))
+    return cudaErrorInvalidValue;
+  size_t smem = plan.total();
+  cudaError_t e = set_smem((const void*)k_flow, smem);
+  if (e != cudaSuccess) return e;
+  FlowArgs A{spots, ninst, inst, counter, disc, job, target, scratch, scratch_floats, out_expl, out_iters, err,
+             lanes, node_parts};
+  k_flow<<<grid, block, smem, s>>>(A, plan);
+  return cudaGetLastError();
+}
+
+int flow_occupancy(int block, const SmemPlan& plan) {
+  int n = 0;
+  size_t smem = plan.total();
+  if (set_smem((const void*)k_flow, smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_flow, block, smem) != cudaSuccess) return 0;
+  return n;
 }
 
 int grid_ctas(int block, const SmemPlan& plan) {
@@ -1615,16 +2110,17 @@ cudaError_t current_context_id(unsigned long long* id) {
       g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f);
   });
   if (!g_ctx_get_current || !g_ctx_get_id) return cudaErrorNotSupported;
+  // cudaSetDevice makes the device's primary context current, creating it
+  // first when there is none: on a new thread, or after a cudaDeviceReset,
+  // which leaves the destroyed context current until the runtime's next call
+  // that needs one
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  e = cudaSetDevice(dev);
+  if (e != cudaSuccess) return e;
   void* ctx = nullptr;
-  if (g_ctx_get_current(&ctx) != 0) return cudaErrorDeviceUninitialized;
-  if (!ctx) {  // no context yet on this thread: the runtime makes the device's primary context current
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    e = cudaSetDevice(dev);
-    if (e != cudaSuccess) return e;
-    if (g_ctx_get_current(&ctx) != 0 || !ctx) return cudaErrorDeviceUninitialized;
-  }
+  if (g_ctx_get_current(&ctx) != 0 || !ctx) return cudaErrorDeviceUninitialized;
   return g_ctx_get_id(ctx, id) == 0 ? cudaSuccess : cudaErrorDeviceUninitialized;
 }
 
@@ -1679,8 +2175,10 @@ cudaError_t launch_exploitability_fixed(const SpotDev* spot, size_t slot_floats,
 }
 
 // Test hook of the bounded grid barrier (launch_debug_barrier_timeout): CTA 0
-// enters `rounds` grid barriers that the other CTAs never join.
-__global__ void k_debug_barrier_timeout(unsigned* bar, int* err, int* passed, int rounds, long long wait_ns) {
+// enters `rounds` grid barriers that the other CTAs never join - or, with
+// all_join, that every CTA joins (the cost of a grid barrier).
+__global__ void k_debug_barrier_timeout(unsigned* bar, int* err, int* passed, int rounds, long long wait_ns,
+                                        int all_join) {
   Ctx c{};
   c.grid = 1;
   c.bar = bar;
@@ -1688,19 +2186,25 @@ __global__ void k_debug_barrier_timeout(unsigned* bar, int* err, int* passed, in
   c.wait_ns = wait_ns;
   if (threadIdx.x == 0) s_grid_ok = 1;
   __syncthreads();
-  if (blockIdx.x != 0) return;
+  if (blockIdx.x != 0 && !all_join) return;
   int n = 0;
   for (int r = 0; r < rounds; ++r)
     if (grid_barrier(c)) ++n;
-  if (threadIdx.x == 0) *passed = n;
+  if (threadIdx.x == 0 && blockIdx.x == 0) *passed = n;
 }
 
-cudaError_t launch_debug_barrier_timeout(int ctas, int rounds, long long wait_ns, unsigned* bar, int* err,
-                                         int* passed, cudaStream_t s) {
-  if (ctas < 2 || ctas > 148 || rounds < 1 || wait_ns < 0 || wait_ns > kGridWaitNs) return cudaErrorInvalidValue;
-  cudaError_t e = cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), s);
+cudaError_t launch_debug_barrier_timeout(int ctas, int rounds, long long wait_ns, int all_join, unsigned* bar,
+                                         int* err, int* passed, cudaStream_t s) {
+  int dev = 0, nsm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  void* args[] = {(void*)&bar, (void*)&err, (void*)&passed, (void*)&rounds, (void*)&wait_ns};
+  e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  // at most one 64-thread CTA per SM: every CTA of the cooperative launch is resident
+  if (ctas < 2 || ctas > nsm || rounds < 1 || wait_ns < 0 || wait_ns > kGridWaitNs) return cudaErrorInvalidValue;
+  e = cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  void* args[] = {(void*)&bar, (void*)&err, (void*)&passed, (void*)&rounds, (void*)&wait_ns, (void*)&all_join};
   return cudaLaunchCooperativeKernel((const void*)k_debug_barrier_timeout, dim3(ctas), dim3(64), args, 0, s);
 }
 

@@ -19,9 +19,14 @@ __host__ __device__ inline int table_bytes_for(int hs0, int hs1) {
   return (b + 15) & ~15;
 }
 
+// A terminal scan buffer: four zero floats (what an empty prefix reads), then
+// the 3V entries of the gathered list, rounded up to whole float4s.
+constexpr int kScanBase = 4;
+__host__ __device__ inline int scan_buf_floats(int vstride) { return 3 * vstride + 2 * kScanBase; }
+
 // Shared-memory plan of one solve CTA (computed on the host per launch): one
-// terminal scan buffer (3 * vstride floats) per warp, optional staged board
-// tables, and a small reduction area.
+// terminal scan buffer (scan_buf_floats(vstride) floats) per scan warp,
+// optional staged board tables, and a small reduction area.
 struct SmemPlan {
   int vstride;  // max slot stride of the launch (floats)
   int hs_max;   // max padded hand count
@@ -31,7 +36,7 @@ struct SmemPlan {
   int split = 0; // 1: a lone spot's node ops may be split over idle warps (launches with fewer spots
                  // than SMs and grid mode, where latency is not hidden by other CTAs; same results)
   __host__ __device__ size_t total() const {
-    return (size_t)tables + (size_t)bufs * 3 * vstride * 4 + 32 * 8;
+    return (size_t)tables + (size_t)bufs * scan_buf_floats(vstride) * 4 + 32 * 8;
   }
 };
 
@@ -153,6 +158,19 @@ cudaError_t launch_solve(const SpotDev* spots, int ninst, int K, const int* inst
                          const Discount* disc, const SolveJob& job, const float* target, float* scratch,
                          size_t scratch_floats, float* out_expl, int* out_iters, int* err, int grid, int block,
                          const SmemPlan& plan, cudaStream_t s);
+// Dataflow batched solve (k_flow): each CTA holds `lanes` spots at once, each
+// at its own step; warps claim the steps' items (terminal runs; node ops cut
+// into node_parts column blocks) instead of waiting at per-step barriers.
+// The same jobs as launch_solve except the adjoint; inst: [ninst] spot ids in
+// the order they are handed out; scratch holds lanes * scratch_floats floats
+// per CTA.  Results equal launch_solve's bit for bit.
+constexpr int kMaxFlowThreads = 1024;
+constexpr int kMaxFlowLanes = 8;
+cudaError_t launch_flow(const SpotDev* spots, int ninst, const int* inst, int* counter, const Discount* disc,
+                        const SolveJob& job, const float* target, float* scratch, size_t scratch_floats,
+                        float* out_expl, int* out_iters, int* err, int grid, int block, int lanes, int node_parts,
+                        const SmemPlan& plan, cudaStream_t s);
+int flow_occupancy(int block, const SmemPlan& plan);  // CTAs per SM (0 = does not fit)
 cudaError_t launch_iterate(const SpotDev* spots, int nspots, const Discount* disc, int t0, int t1,
                            float* scratch, size_t scratch_floats, int* err, int grid, int block,
                            const SmemPlan& plan, cudaStream_t s);
@@ -186,10 +204,13 @@ cudaError_t launch_exploitability_fixed(const SpotDev* spot, size_t slot_floats,
 cudaError_t current_context_id(unsigned long long* id);
 
 // Test hook for the bounded grid barrier: a cooperative launch of `ctas` CTAs
-// in which CTA 0 enters `rounds` grid barriers that no other CTA joins.  The
-// first wait gives up after wait_ns nanoseconds and reports ERR_WAIT (4) in
-// *err; every later barrier must return at once.  *passed counts the barriers
-// CTA 0 got through (0 when the abort works).  bar: 4 unsigned of device memory.
-cudaError_t launch_debug_barrier_timeout(int ctas, int rounds, long long wait_ns, unsigned* bar, int* err,
-                                         int* passed, cudaStream_t s);
+// (at most one per SM) in which CTA 0 enters `rounds` grid barriers that no
+// other CTA joins.  The first wait gives up after wait_ns nanoseconds and
+// reports ERR_WAIT (4) in *err; every later barrier must return at once.
+// *passed counts the barriers CTA 0 got through (0 when the abort works).
+// With all_join every CTA enters the barriers (no wait runs out; the kernel
+// time / rounds is the cost of one grid barrier).  bar: 4 unsigned of device
+// memory.
+cudaError_t launch_debug_barrier_timeout(int ctas, int rounds, long long wait_ns, int all_join, unsigned* bar,
+                                         int* err, int* passed, cudaStream_t s);
 }  // namespace ps

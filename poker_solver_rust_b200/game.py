@@ -175,6 +175,17 @@ class PostFlopGame:
         N.check(N.lib().ps_game_memory_usage(self._h, C.byref(v)))
         return int(v.value)
 
+    def program_info(self) -> dict:
+        """The compiled tree program's shape (ps_game_program_info; host-side,
+        no GPU needed): working slots and their stride, steps / node ops /
+        terminal ops / terminal runs per traverser, S (sum over decision edges
+        of the acting player's hands) and the number of boards."""
+        v = (C.c_int64 * 12)()
+        N.check(N.lib().ps_game_program_info(self._h, v))
+        return {"slots": int(v[0]), "slot_stride": int(v[1]), "steps": [int(v[2]), int(v[3])],
+                "node_ops": [int(v[4]), int(v[5])], "terminal_ops": [int(v[6]), int(v[7])],
+                "terminal_runs": [int(v[8]), int(v[9])], "S": int(v[10]), "boards": int(v[11])}
+
     def allocate_memory(self, enable_compression: bool = False) -> None:
         N.check(N.lib().ps_game_allocate_memory(self._h, int(enable_compression)))
 
@@ -516,11 +527,17 @@ class BatchSolver:
 
     def __init__(self, card_configs: Sequence[CardConfig], tree_configs: Sequence[TreeConfig],
                  block_threads: int = 0, ctas_per_sm: int = 0, sort_by_cost: bool = True,
-                 stage_tables: int = -1, scan_buffers: int = 0, instances_per_cta: int = 0):
+                 stage_tables: int = -1, scan_buffers: int = 0, instances_per_cta: int = 0,
+                 scheduler: int = 0, flow_threads: int = 0, flow_spots_per_cta: int = 0, node_parts: int = 0):
+        """Options as ps_batch_opts (include/ps_range_solver.h).  scheduler:
+        0 = default (dataflow for batches of more spots than SMs), 1 =
+        step-synchronous (one barrier per step), 2 = dataflow; flow_threads,
+        flow_spots_per_cta, node_parts shape the dataflow launch (0 = default,
+        or autotuned with block_threads = -1)."""
         n = len(card_configs)
         cc, tc, keep = _pack_configs(card_configs, tree_configs)
         opts = N.PsBatchOpts(block_threads, ctas_per_sm, int(sort_by_cost), stage_tables, scan_buffers,
-                             instances_per_cta)
+                             instances_per_cta, scheduler, flow_threads, flow_spots_per_cta, node_parts)
         h = C.c_void_p()
         N.check(N.lib().ps_batch_new(cc, tc, n, C.byref(opts), C.byref(h)))
         self._h = h
@@ -588,11 +605,26 @@ class BatchSolver:
         n = N.check(N.lib().ps_batch_autotune_log(self._h, b, u, t, 32))
         return [(int(b[i]), int(u[i]), float(t[i])) for i in range(min(n, 32))]
 
+    def autotune_trials(self):
+        """Every trial of the last autotune: dicts of threads per CTA,
+        scan-buffer warps, spots per CTA and node-op parts (0 for a
+        step-synchronous trial) and the trial's device ms."""
+        cap = 256
+        shape = (C.c_int32 * (4 * cap))()
+        t = (C.c_float * cap)()
+        n = min(N.check(N.lib().ps_batch_autotune_trials(self._h, shape, t, cap)), cap)
+        return [{"block_threads": int(shape[4 * i]), "scan_buffers": int(shape[4 * i + 1]),
+                 "spots_per_cta": int(shape[4 * i + 2]), "node_parts": int(shape[4 * i + 3]),
+                 "trial_ms": float(t[i])} for i in range(n)]
+
     def config(self):
-        a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
-        N.check(N.lib().ps_batch_config(self._h, C.byref(a), C.byref(b), C.byref(c)))
-        return {"block_threads": a.value, "grid": b.value, "ctas_per_sm": c.value,
-                "scan_buffers": N.check(N.lib().ps_batch_scan_buffers(self._h))}
+        """The launch shape of the batch's solves (ps_batch_schedule)."""
+        v = (C.c_int32 * 8)()
+        N.check(N.lib().ps_batch_schedule(self._h, v))
+        return {"scheduler": "dataflow" if v[0] == N.PS_SCHED_FLOW else "step-synchronous",
+                "block_threads": int(v[1]), "grid": int(v[2]), "ctas_per_sm": int(v[3]),
+                "scan_buffers": int(v[4]), "spots_per_cta": int(v[5]), "node_parts": int(v[6]),
+                "grid_mode": bool(v[7])}
 
     # ---- depth-limited spots: iteration ranges and boundary values
     #      (gpu-range-solver batch.rs:279-585) ----

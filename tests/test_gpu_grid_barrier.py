@@ -23,7 +23,7 @@ ERR_WAIT = 4
 def test_grid_barrier_gives_up_and_aborts(ctas):
     err, passed, ms = C.c_int32(), C.c_int32(), C.c_float()
     rounds, wait_ns = 1000, 20_000_000
-    N.check(N.lib().ps_debug_grid_barrier_timeout(ctas, rounds, wait_ns, C.byref(err), C.byref(passed),
+    N.check(N.lib().ps_debug_grid_barrier_timeout(ctas, rounds, wait_ns, 0, C.byref(err), C.byref(passed),
                                                   C.byref(ms)))
     assert err.value == ERR_WAIT
     assert passed.value == 0  # the first barrier failed, and the 999 after it returned at once
@@ -33,5 +33,22 @@ def test_grid_barrier_gives_up_and_aborts(ctas):
 
 def test_grid_barrier_hook_rejects_unbounded_waits():  # argument check only: no GPU needed
     err, passed, ms = C.c_int32(), C.c_int32(), C.c_float()
-    rc = N.lib().ps_debug_grid_barrier_timeout(2, 1, 2_000_000_000, C.byref(err), C.byref(passed), C.byref(ms))
+    rc = N.lib().ps_debug_grid_barrier_timeout(2, 1, 2_000_000_000, 0, C.byref(err), C.byref(passed), C.byref(ms))
     assert rc == -1
+
+
+@pytest.mark.gpu
+def test_grid_barrier_cost_when_every_cta_joins():
+    """Every CTA (one per SM) joins every barrier: none times out, all pass,
+    and the time per barrier is reported for the grid-mode step cost."""
+    import torch
+
+    nsm = torch.cuda.get_device_properties(0).multi_processor_count
+    err, passed, ms = C.c_int32(), C.c_int32(), C.c_float()
+    rounds = 2000
+    N.check(N.lib().ps_debug_grid_barrier_timeout(nsm, rounds, 1_000_000_000, 1, C.byref(err), C.byref(passed),
+                                                  C.byref(ms)))
+    assert err.value == 0 and passed.value == rounds
+    us = 1e3 * ms.value / rounds
+    print(f"grid barrier over {nsm} CTAs: {us:.2f} us")
+    assert us < 50.0

@@ -399,3 +399,69 @@ def test_oracle_chance_threads_keep_results():
         finally:
             O.set_chance_threads(1)
     assert out[0][0] == out[1][0] and np.array_equal(out[0][1], out[1][1])
+
+
+def test_oracle_fd_central_matches_python_differences():
+    """The oracle's C++ central differences (used at the spec's adjoint size)
+    equal the loop over full loss evaluations that the small adjoint test
+    runs: weights and boundary values of a depth-limited turn spot."""
+    import numpy as np
+
+    from tests import spots
+
+    rng = np.random.default_rng(3)
+
+    def sparse(rng, board):
+        out = []
+        for _ in range(2):
+            w = rng.random(1326).astype(np.float32)
+            w[rng.random(1326) < 0.93] = 0.0
+            out.append(spots._mask_board(w, board))
+        return out
+
+    r, b, t = spots.turn_spot(9, weights=sparse)
+    t.depth_limit = 0
+    o = spots.oracle_game(r, b, t, fp64=True)
+    nb = o.num_boundary_nodes()
+    assert nb > 0
+    B = [[rng.normal(0, 1, o.num_private_hands(p)).astype(np.float32) for p in range(2)] for _ in range(nb)]
+    for k in range(nb):
+        for p in range(2):
+            o.set_boundary_cfvs(k, p, B[k][p])
+    for it in range(8):
+        o.solve_step(it)
+    H = [o.num_private_hands(0), o.num_private_hands(1)]
+    w = [rng.random(H[p]).astype(np.float32) for p in range(2)]
+    cot = [rng.normal(0, 1, H[p]).astype(np.float32) for p in range(2)]
+
+    def loss():
+        c0 = o.root_cfvalues_with_reach(0, w[1])
+        c1 = o.root_cfvalues_with_reach(1, w[0])
+        return float(np.dot(cot[0].astype(np.float64), c0) + np.dot(cot[1].astype(np.float64), c1))
+
+    coords, ref = [], []
+    for p in range(2):
+        for j in rng.choice(H[p], 4, replace=False):
+            x0 = w[p][j]
+            w[p][j] = np.float32(x0 + 1e-3)
+            lp, xp = loss(), float(w[p][j])
+            w[p][j] = np.float32(x0 - 1e-3)
+            lm, xm = loss(), float(w[p][j])
+            w[p][j] = x0
+            coords.append((0, 0, p, j))
+            ref.append((lp - lm) / (xp - xm))
+        for _ in range(4):
+            k, j = int(rng.integers(nb)), int(rng.integers(H[p]))
+            v = B[k][p].copy()
+            v[j] = np.float32(B[k][p][j] + 1e-3)
+            o.set_boundary_cfvs(k, p, v)
+            lp, xp = loss(), float(v[j])
+            v[j] = np.float32(B[k][p][j] - 1e-3)
+            o.set_boundary_cfvs(k, p, v)
+            lm, xm = loss(), float(v[j])
+            o.set_boundary_cfvs(k, p, B[k][p])
+            coords.append((1, k, p, j))
+            ref.append((lp - lm) / (xp - xm))
+    got = o.fd_central(w, cot, coords)
+    ref = np.asarray(ref)
+    assert np.abs(got - ref).max() <= 1e-9 * max(1.0, np.abs(ref).max()), (got, ref)
