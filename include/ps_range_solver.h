@@ -75,6 +75,15 @@ int ps_game_memory_usage(ps_game* g, uint64_t* bytes);
  * out[10] S = sum over decision edges of the acting player's hands (the
  * per-iteration state stream is 20 * S bytes), out[11] boards. */
 int ps_game_program_info(ps_game* g, int64_t out[12]);
+/* No counterpart in the reference.  Chooses the game's tree program before
+ * allocate_memory (host-side only): 1 evaluates every terminal of a pass in
+ * one step after the forward sweep, 0 the terminals of each depth in that
+ * depth's backward step.  Results are the same bits either way; the first
+ * has fewer long steps (one per pass) and keeps more vectors alive at once.
+ * Without a choice, a game that runs in grid mode (one game of at least 16
+ * nodes) takes 1 and every other game 0.  The compiler replays each program
+ * against its slot assignment and rejects one that fails (PS_ERR_INVALID). */
+int ps_game_set_terminals_first(ps_game* g, int enable);
 /* PostFlopGame::allocate_memory (interpreter.rs:212); compression -> PS_ERR_UNSUPPORTED */
 int ps_game_allocate_memory(ps_game* g, int enable_compression);
 
@@ -250,7 +259,7 @@ typedef struct ps_batch_opts {
                              (0 = 512; with block_threads = -1 the autotuner chooses) */
   int32_t flow_spots_per_cta; /* dataflow: spots a CTA holds at once, 1..8 (0 = 2, or autotuned) */
   int32_t node_parts;     /* dataflow: column blocks each node op is cut into, 1..16
-                             (0 = 2, or autotuned) */
+                             (0 = 3, or autotuned) */
 } ps_batch_opts;
 #define PS_SCHED_DEFAULT 0
 #define PS_SCHED_STEP 1

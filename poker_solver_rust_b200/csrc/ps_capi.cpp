@@ -339,6 +339,19 @@ struct Batch {
     CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     for (auto& e : ev) CU(cudaEventCreate(&e));
     const int n = (int)games.size();
+    // a single game large enough for grid mode (below) evaluates all of a
+    // pass's terminals in one step unless its caller chose the program
+    // (ps_game_set_terminals_first): one long step per pass instead of one
+    // per depth, each ended by a grid barrier
+    {
+      const char* env = std::getenv("PS_GRID_NODES");
+      const long thr = env ? std::atol(env) : 16;
+      if (n == 1 && games[0]->program_choice < 0 && thr > 0 && (long)games[0]->arena.size() >= thr &&
+          !games[0]->terminals_first) {
+        std::string err;
+        if (!games[0]->recompile(true, err)) return fail(PS_ERR_INVALID, err);
+      }
+    }
     lay.resize(n);
     // ---- layout ----
     size_t so = 0, su = 0, st = 0, sb = 0;
@@ -548,7 +561,7 @@ struct Batch {
         int fb = opts && opts->flow_threads > 0 ? opts->flow_threads : 512;
         fb = std::max(128, std::min(kMaxFlowThreads, (fb / 32) * 32));
         const int fl = opts && opts->flow_spots_per_cta > 0 ? opts->flow_spots_per_cta : 2;
-        const int fp = opts && opts->node_parts > 0 ? opts->node_parts : 2;
+        const int fp = opts && opts->node_parts > 0 ? opts->node_parts : 3;
         if (fl > kMaxFlowLanes || fp > 16) return fail(PS_ERR_INVALID, "flow_spots_per_cta 1..8, node_parts 1..16");
         const int rc = adopt_flow(fb, opts && opts->scan_buffers > 0 ? opts->scan_buffers : fb / 64, fl, fp,
                                   opts ? opts->ctas_per_sm : 0);
@@ -709,7 +722,7 @@ struct Batch {
     std::vector<Cand> cands;
     for (int b : {256, 512, 1024})
       for (int lanes : {1, 2, 3, 4})
-        for (int parts : {1, 2}) {
+        for (int parts : {1, 2, 3}) {
           const int w = b / 32;
           if (req_bufs > 0) {
             cands.push_back({b, std::min(w, req_bufs), lanes, parts});
@@ -1362,6 +1375,15 @@ int ps_game_memory_usage(ps_game* G, uint64_t* bytes) {
   if (!G || !bytes) return fail(PS_ERR_INVALID, "null argument");
   Game& g = *G->g;
   *bytes = 4 * (2 * g.num_storage + g.num_storage_ip + g.num_storage_chance);
+  return PS_OK;
+}
+
+int ps_game_set_terminals_first(ps_game* G, int enable) {
+  if (!G) return fail(PS_ERR_INVALID, "null game");
+  if (G->state != GState::TreeBuilt) return fail(PS_ERR_STATE, "choose the program before allocate_memory");
+  std::string err;
+  if (!G->g->recompile(enable != 0, err)) return fail(PS_ERR_INVALID, err);
+  G->g->program_choice = enable != 0;
   return PS_OK;
 }
 

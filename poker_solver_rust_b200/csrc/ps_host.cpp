@@ -3,6 +3,7 @@
 #include "ps_host.hpp"
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -665,7 +666,14 @@ void Game::build_arena(const ATree& t) {  // interpreter.rs:708-947
 }
 
 // Level-ordered program for traverser p (see ps_device.hpp for the op set).
-void Game::compile(int p) {
+// terminals_first: every terminal of the pass is evaluated in one step right
+// after the forward sweep (a terminal reads only reach vectors the forward
+// sweep wrote), so the backward steps hold node ops alone.  A pass then has
+// one step of terminal runs - the long items - instead of one per depth,
+// which shortens a lone game's chain of grid barriers; the price is that
+// every cfv block with a terminal child lives from that step on.  Each op's
+// arithmetic is the same either way.
+void Game::compile(int p, bool terminals_first) {
   Program& P = prog[p];
   P.ops.clear();
   P.steps.clear();
@@ -692,8 +700,9 @@ void Game::compile(int p) {
   }
   int D = 0;
   for (size_t n : order) D = std::max(D, depth[n]);
+  const int T = D + 1;  // terminals_first: the step of every terminal
   auto tf = [&](int d) { return d; };
-  auto tb = [&](int d) { return (D + 1) + (D - d); };
+  auto tb = [&](int d) { return (terminals_first ? D + 2 : D + 1) + (D - d); };
   // slot blocks
   struct Blk { int size, birth, death, base; };
   std::vector<Blk> blks;
@@ -709,7 +718,9 @@ void Game::compile(int p) {
       blks.push_back({chance ? 1 : (int)a.nch, tf(depth[n]), -1, -1});
     }
     cb[n] = (int)blks.size();
-    blks.push_back({(int)a.nch, tb(depth[n] + 1), tb(depth[n]), -1});
+    bool term_child = false;
+    for (int c = 0; c < a.nch && terminals_first; ++c) term_child |= arena[eff(n + a.child_off + c)].terminal();
+    blks.push_back({(int)a.nch, term_child ? T : tb(depth[n] + 1), tb(depth[n]), -1});
     for (int c = 0; c < a.nch; ++c) {
       size_t e = eff(n + a.child_off + c);
       if (chance) { reach_blk[e] = rb[n]; reach_idx[e] = 0; }
@@ -727,7 +738,7 @@ void Game::compile(int p) {
     int b = reach_blk[n];
     if (b < 0) continue;
     const ArenaNode& a = arena[n];
-    int use = a.terminal() ? tb(depth[n]) : (a.chance() || a.player != p) ? tf(depth[n]) : -1;
+    int use = a.terminal() ? (terminals_first ? T : tb(depth[n])) : (a.chance() || a.player != p) ? tf(depth[n]) : -1;
     blks[b].death = std::max(blks[b].death, use);
   }
   for (auto& b : blks)
@@ -756,6 +767,12 @@ void Game::compile(int p) {
     return reach_blk[n] < 0 ? SLOT_ROOT_REACH : (uint16_t)(blks[reach_blk[n]].base + reach_idx[n]);
   };
   auto cfv_slot = [&](size_t n) { return (uint16_t)(blks[cfv_blk[n]].base + cfv_idx[n]); };
+  // semantic keys of slot contents, for the verification below: reach vector
+  // (block, index) or cfv vector (block, index); -1 = the opponent's weights
+  auto reach_key = [&](size_t n) -> int64_t {
+    return reach_blk[n] < 0 ? -1 : ((int64_t)reach_blk[n] << 17) | ((int64_t)reach_idx[n] << 1);
+  };
+  auto cfv_key = [&](int blk, int idx) -> int64_t { return ((int64_t)blk << 17) | ((int64_t)idx << 1) | 1; };
   // emit
   std::vector<std::vector<size_t>> at(D + 1);
   for (size_t n : order) at[depth[n]].push_back(n);
@@ -804,6 +821,38 @@ void Game::compile(int p) {
     }
     push_step(begin, (int)P.ops.size() - begin, 0);
   }
+  // terminals of the step `range` (all depths when terminals_first), runs of
+  // the same (board, reach) adjacent, so a batch scans that reach once
+  auto emit_terminals = [&](const std::vector<size_t>& terms_in) {
+    std::vector<size_t> terms = terms_in;
+    std::stable_sort(terms.begin(), terms.end(), [&](size_t x, size_t y) {
+      int bx = node_board[x], by = node_board[y];
+      if (bx != by) return bx < by;
+      return reach_slot(x) < reach_slot(y);
+    });
+    for (size_t n : terms) {
+      const ArenaNode& a = arena[n];
+      Op o{};
+      o.type = OP_TERM;
+      o.node = (uint32_t)n;
+      o.src = reach_slot(n);
+      o.dst = cfv_slot(n);
+      o.board = (uint16_t)node_board[n];
+      if (a.boundary()) o.term = TERM_BOUNDARY;
+      else if (a.fold()) { o.term = TERM_FOLD; o.fold_pl = a.player & PL_MASK; }
+      else o.term = TERM_SHOWDOWN;
+      P.ops.push_back(o);
+    }
+  };
+  if (terminals_first) {
+    std::vector<size_t> all;
+    for (int d = D; d >= 0; --d)
+      for (size_t n : at[d])
+        if (arena[n].terminal()) all.push_back(n);
+    int begin = (int)P.ops.size();
+    emit_terminals(all);
+    push_step(begin, 0, (int)P.ops.size() - begin);
+  }
   for (int d = D; d >= 0; --d) {
     int begin = (int)P.ops.size();
     for (size_t n : at[d]) {
@@ -824,31 +873,72 @@ void Game::compile(int p) {
       P.ops.push_back(o);
     }
     int ne = (int)P.ops.size() - begin;
-    std::vector<size_t> terms;
-    for (size_t n : at[d])
-      if (arena[n].terminal()) terms.push_back(n);
-    // terminals reading the same reach on the same board are adjacent, so a
-    // batch scans that reach once
-    std::stable_sort(terms.begin(), terms.end(), [&](size_t x, size_t y) {
-      int bx = node_board[x], by = node_board[y];
-      if (bx != by) return bx < by;
-      return reach_slot(x) < reach_slot(y);
-    });
-    for (size_t n : terms) {
-      const ArenaNode& a = arena[n];
-      Op o{};
-      o.type = OP_TERM;
-      o.node = (uint32_t)n;
-      o.src = reach_slot(n);
-      o.dst = cfv_slot(n);
-      o.board = (uint16_t)node_board[n];
-      if (a.boundary()) o.term = TERM_BOUNDARY;
-      else if (a.fold()) { o.term = TERM_FOLD; o.fold_pl = a.player & PL_MASK; }
-      else o.term = TERM_SHOWDOWN;
-      P.ops.push_back(o);
+    if (!terminals_first) {
+      std::vector<size_t> terms;
+      for (size_t n : at[d])
+        if (arena[n].terminal()) terms.push_back(n);
+      emit_terminals(terms);
     }
     push_step(begin, ne, (int)P.ops.size() - begin - ne);
   }
+  // Verification: replay the pass step by step with the meaning of every
+  // slot.  Each read must find the vector the op expects; within a step no
+  // two ops write one slot and no op reads a slot another op of the step
+  // writes (the ops of a step run concurrently).
+  {
+    std::vector<int64_t> content(P.num_slots, INT64_MIN);
+    std::vector<int> wstep(P.num_slots, -1);
+    P.verified = true;
+    for (size_t si = 0; si < P.steps.size() && P.verified; ++si) {
+      const Step& st = P.steps[si];
+      std::vector<std::pair<int, int64_t>> writes;
+      std::vector<std::pair<int, int64_t>> reads;
+      for (int k = st.begin; k < st.begin + st.n_elem + st.n_term; ++k) {
+        const Op& o = P.ops[k];
+        const size_t n = o.node;
+        const ArenaNode& a = arena[n];
+        if (o.type == OP_FWD_OPP || o.type == OP_FWD_CHANCE || o.type == OP_TERM)
+          if (o.src != SLOT_ROOT_REACH) reads.push_back({o.src, reach_key(n)});
+        if (o.type == OP_FWD_OPP)
+          for (int c = 0; c < a.nch; ++c) writes.push_back({o.blk + c, ((int64_t)rb[n] << 17) | ((int64_t)c << 1)});
+        else if (o.type == OP_FWD_CHANCE)
+          writes.push_back({o.blk, (int64_t)rb[n] << 17});
+        else if (o.type == OP_TERM)
+          writes.push_back({o.dst, cfv_key(cfv_blk[n], cfv_idx[n])});
+        else {  // backward node ops read every child's cfv
+          for (int c = 0; c < a.nch; ++c) reads.push_back({o.blk + c, cfv_key(cb[n], c)});
+          writes.push_back({o.dst, cfv_key(cfv_blk[n], cfv_idx[n])});
+        }
+      }
+      for (auto [slot, key] : reads)
+        if (slot >= P.num_slots || content[slot] != key) P.verified = false;
+      for (auto [slot, key] : writes) {
+        if (slot >= P.num_slots || wstep[slot] == (int)si) P.verified = false;
+        else wstep[slot] = (int)si;
+      }
+      for (auto [slot, key] : reads)
+        if (slot < P.num_slots && wstep[slot] == (int)si) P.verified = false;
+      for (auto [slot, key] : writes)
+        if (slot < P.num_slots) content[slot] = key;
+    }
+    const int root_key_ok = P.root_slot >= 0 && P.root_slot < P.num_slots &&
+                            content[P.root_slot] == cfv_key(out_blk, 0);
+    if (!root_key_ok) P.verified = false;
+  }
+}
+
+// Recompiles both traversers' programs (terminals_first: see compile).
+bool Game::recompile(bool tf, std::string& err) {
+  terminals_first = tf;
+  compile(0, tf);
+  compile(1, tf);
+  if (!prog[0].verified || !prog[1].verified) { err = "tree program failed its slot verification"; return false; }
+  num_slots = std::max(prog[0].num_slots, prog[1].num_slots);
+  if (num_slots >= 0xFFF0) { err = "Tree too wide for the slot allocator"; return false; }
+  for (int p = 0; p < 2; ++p)
+    for (const auto& st : prog[p].steps)
+      if (st.n_elem > 32000 || st.n_term > 32000) { err = "Tree level too wide"; return false; }
+  return true;
 }
 
 bool Game::init(const float* r0, const float* r1, const uint8_t b[5], const TreeCfg& c, std::string& err) {
@@ -871,14 +961,7 @@ bool Game::init(const float* r0, const float* r1, const uint8_t b[5], const Tree
       err = "Too many actions at one node (max " + std::to_string(kMaxActions) + ")";
       return false;
     }
-  compile(0);
-  compile(1);
-  num_slots = std::max(prog[0].num_slots, prog[1].num_slots);
-  if (num_slots >= 0xFFF0) { err = "Tree too wide for the slot allocator"; return false; }
-  for (int p = 0; p < 2; ++p)
-    for (const auto& st : prog[p].steps)
-      if (st.n_elem > 32000 || st.n_term > 32000) { err = "Tree level too wide"; return false; }
-  return true;
+  return recompile(false, err);
 }
 
 }  // namespace ps

@@ -89,6 +89,7 @@ struct Program {
   std::vector<uint16_t> groups;
   int root_slot = -1;
   int num_slots = 0;
+  bool verified = false;  // the slot replay of compile found every read intact
 };
 
 struct IsoEntry {
@@ -131,15 +132,20 @@ struct Game {
   Program prog[2];
   int num_slots = 0;
 
+  bool terminals_first = false;  // the programs evaluate every terminal of a pass in one step
+  int program_choice = -1;       // -1: terminals-first when the game runs in grid mode; 0 / 1: as chosen
+
   bool init(const float* r0, const float* r1, const uint8_t board[5], const TreeCfg& cfg,
             std::string& err);
   int chance_factor(const ArenaNode& n) const { return n.turn == NOT_DEALT ? 45 : 44; }
+  // recompiles both traversers' programs (terminals_first: see compile)
+  bool recompile(bool terminals_first, std::string& err);
 
  private:
   bool check_cards(std::string& err);
   void init_isomorphism();
   void build_arena(const ATree& t);
-  void compile(int p);
+  void compile(int p, bool terminals_first = false);
 };
 
 // f64 discount schedule of DCFR (crates/range-solver/src/solver.rs:26-44)

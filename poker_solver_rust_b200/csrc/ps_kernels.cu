@@ -104,28 +104,6 @@ __device__ __forceinline__ float fmax_ref(float x, float y) { return x > y ? x :
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
 
-// The last touch of a regret / strategy-sum row in a pass (its update store,
-// or an opponent row's second read): the streaming cache operator (.cs,
-// evict-first), so the state stream - read once and written once per pass,
-// far larger than L2 - leaves L2 first and the working slots stay.
-#ifndef PS_L2_STREAM
-#define PS_L2_STREAM 1
-#endif
-__device__ __forceinline__ float4 ld4_last(const float* p) {
-#if PS_L2_STREAM
-  return __ldcs(reinterpret_cast<const float4*>(p));
-#else
-  return ld4(p);
-#endif
-}
-__device__ __forceinline__ void st4_last(float* p, float4 v) {
-#if PS_L2_STREAM
-  __stcs(reinterpret_cast<float4*>(p), v);
-#else
-  st4(p, v);
-#endif
-}
-
 __device__ __forceinline__ float4 max0(float4 a) {
   return make_float4(fmax_ref(a.x, 0.f), fmax_ref(a.y, 0.f), fmax_ref(a.z, 0.f), fmax_ref(a.w, 0.f));
 }
@@ -208,7 +186,7 @@ __device__ __noinline__ void op_fwd_opp_t(const Ctx& c, const Op& op, int o, int
     }
     const float4 r = ld4(src + h);
     for (int a = 0; a < na; ++a) {
-      float4 x = ld4_last(base + a * hso + h);
+      float4 x = ld4(base + a * hso + h);
       if (mode == M_DCFR) x = max0(x);
       st4(dst + (size_t)a * c.vstride + h, mul4(sigma4(x, d, def), r));
     }
@@ -287,7 +265,7 @@ __device__ __noinline__ void op_bwd_trav_t(const Ctx& c, const Op& op, int p, co
         res = a == 0 ? t : add4(res, t);
         if (mode == M_DCFR) {
           const float4 g = make_float4(dc.gamma, dc.gamma, dc.gamma, dc.gamma);
-          st4_last(S + a * hsp + h, add4(mul4(ld4(S + a * hsp + h), g), s));
+          st4(S + a * hsp + h, add4(mul4(ld4(S + a * hsp + h), g), s));
         } else if (mode == M_AVG_SAVE) {
           st4(R + a * hsp + h, cv);
         }
@@ -296,7 +274,7 @@ __device__ __noinline__ void op_bwd_trav_t(const Ctx& c, const Op& op, int p, co
         for (int a = 0; a < na; ++a) {
           const float4 r = ld4(R + a * hsp + h);
           const float4 cv = ld4(cb + (size_t)a * c.vstride + h);
-          st4_last(R + a * hsp + h, make_float4(regret_upd(r.x, cv.x, res.x, dc.alpha, dc.beta),
+          st4(R + a * hsp + h, make_float4(regret_upd(r.x, cv.x, res.x, dc.alpha, dc.beta),
                                            regret_upd(r.y, cv.y, res.y, dc.alpha, dc.beta),
                                            regret_upd(r.z, cv.z, res.z, dc.alpha, dc.beta),
                                            regret_upd(r.w, cv.w, res.w, dc.alpha, dc.beta)));
@@ -1500,6 +1478,13 @@ __device__ void lane_item(const Lane& L, const FlowArgs& A, int term, int idx, f
 }
 
 constexpr long long kFlowIdleNs = 2000000000LL;  // 2 s without any finished step in the CTA: give up
+#ifndef PS_FLOW_SLEEP_MIN
+#define PS_FLOW_SLEEP_MIN 32
+#endif
+#ifndef PS_FLOW_SLEEP_MAX
+#define PS_FLOW_SLEEP_MAX 512
+#endif
+constexpr unsigned kFlowSleepMinNs = PS_FLOW_SLEEP_MIN, kFlowSleepMaxNs = PS_FLOW_SLEEP_MAX;  // idle back-off
 
 __global__ void __launch_bounds__(kMaxFlowBlock, 1) k_flow(FlowArgs A, SmemPlan plan) {
   extern __shared__ float4 smem4[];
@@ -1531,6 +1516,7 @@ __global__ void __launch_bounds__(kMaxFlowBlock, 1) k_flow(FlowArgs A, SmemPlan 
   __syncthreads();
   unsigned seen = 0;
   unsigned long long idle_since = global_ns();
+  unsigned backoff = kFlowSleepMinNs, polls = 0;
   int start = warp % K;
   for (;;) {
     int k = -1, idx = -1, term = 0;
@@ -1573,25 +1559,32 @@ __global__ void __launch_bounds__(kMaxFlowBlock, 1) k_flow(FlowArgs A, SmemPlan 
         }
       }
       start = k;  // stay with this lane while it has work (its rows are warm)
-      idle_since = global_ns();
+      backoff = kFlowSleepMinNs;
+      polls = 0;
       continue;
     }
-    // nothing to claim: finished, or wait for a step to end
+    // nothing to claim: finished, or wait for a step to end.  Idle warps back
+    // off (32 ns doubling to 512 ns) so their polls take few issue slots from
+    // the working ones; the wait bound is checked every 16 polls.
     int stop = 0;
     if (lane == 0) {
-      const unsigned pr = *reinterpret_cast<volatile unsigned*>(&s_progress);
       if (*reinterpret_cast<volatile int*>(&s_retired) >= K) {
         stop = 1;
-      } else if (pr != seen) {
-        seen = pr;
-        idle_since = global_ns();
-      } else if ((long long)(global_ns() - idle_since) > kFlowIdleNs) {
-        atomicOr(A.err, ERR_WAIT);
-        stop = 1;
+      } else if ((++polls & 15) == 0) {
+        const unsigned pr = *reinterpret_cast<volatile unsigned*>(&s_progress);
+        const unsigned long long now = global_ns();
+        if (pr != seen) {
+          seen = pr;
+          idle_since = now;
+        } else if ((long long)(now - idle_since) > kFlowIdleNs) {
+          atomicOr(A.err, ERR_WAIT);
+          stop = 1;
+        }
       }
     }
     if (__shfl_sync(0xffffffffu, stop, 0)) return;
-    __nanosleep(64);
+    __nanosleep(backoff);
+    backoff = min(2 * backoff, kFlowSleepMaxNs);
   }
 }
 

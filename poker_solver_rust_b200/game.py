@@ -175,6 +175,12 @@ class PostFlopGame:
         N.check(N.lib().ps_game_memory_usage(self._h, C.byref(v)))
         return int(v.value)
 
+    def set_terminals_first(self, enable: bool) -> None:
+        """Chooses the tree program before allocate_memory
+        (ps_game_set_terminals_first): every terminal of a pass in one step
+        (True) or each depth's terminals in that depth's step (False)."""
+        N.check(N.lib().ps_game_set_terminals_first(self._h, int(enable)))
+
     def program_info(self) -> dict:
         """The compiled tree program's shape (ps_game_program_info; host-side,
         no GPU needed): working slots and their stride, steps / node ops /

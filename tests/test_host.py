@@ -174,3 +174,34 @@ def test_batch_config_packing_points_at_ranges():
     cc[0].range[0].data = np.zeros(100, np.float32)
     with pytest.raises(ValueError):
         G._pack_configs(cc, tcs)
+
+
+def test_program_forms_pass_slot_replay():
+    """Both tree-program forms compile and pass the compiler's slot replay
+    (every read finds the vector it expects) on river, turn, depth-limited
+    and isomorphic trees; the terminals-first form has one terminal step per
+    pass and keeps the op counts."""
+    import numpy as np
+
+    from tests import spots
+
+    cases = [spots.river_spot(1), spots.turn_spot(2), spots.datagen_spot(np.random.default_rng(5))]
+    r, b, t = spots.turn_spot(9)
+    t.depth_limit = 0
+    cases.append((r, b, t))
+    r0 = ps.Range.from_str("AA,KK,QQ,AKs,AQs,KQo").raw_data()
+    r1 = ps.Range.from_str("JJ-99,AJs,KJs,QJs,T9s").raw_data()
+    board = ps.board_from_str("Kh Qh 7h 2s")
+    sz = ps.BetSizeOptions("50%, a", "100%")
+    tc = ps.TreeConfig(initial_state=ps.BoardState.Turn, starting_pot=100, effective_stack=150,
+                       turn_bet_sizes=[sz, sz], river_bet_sizes=[sz, sz])
+    cases.append(([spots._mask_board(r0.copy(), board), spots._mask_board(r1.copy(), board)], board, tc))
+    for r, b, t in cases:
+        g = spots.product_game(r, b, t, allocate=False)
+        base = g.program_info()
+        g.set_terminals_first(True)
+        tf = g.program_info()
+        assert tf["node_ops"] == base["node_ops"] and tf["terminal_ops"] == base["terminal_ops"]
+        assert tf["terminal_runs"] == base["terminal_runs"]
+        g.set_terminals_first(False)
+        assert g.program_info() == base
