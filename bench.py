@@ -105,10 +105,11 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def profiled_traffic_per_spot_iteration():
+def profiled_traffic_per_spot_iteration(kernel: str):
     """DRAM read + write bytes per spot-iteration of the committed ncu capture
-    of k_solve (profiles/k_solve_river_datagen_1024.md), or None."""
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "k_solve_river_datagen_1024.md")
+    of the batched solve kernel that ran (profiles/<kernel>_river_datagen_1024.md),
+    or None."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", f"{kernel}_river_datagen_1024.md")
     try:
         with open(path) as f:
             m = re.search(r"^traffic_bytes_per_spot_iteration:\s*([0-9.]+)", f.read(), re.M)
@@ -488,7 +489,8 @@ def main():
     kernel_s = statistics.median(solve_ms) / 1e3
     achieved = alg_bytes / kernel_s / 1e9
     peak, peak_kind = _peaks()
-    tps = profiled_traffic_per_spot_iteration()
+    kernel = "k_flow" if bs.config()["scheduler"] == "dataflow" else "k_solve"
+    tps = profiled_traffic_per_spot_iteration(kernel)
     traffic = float(tps * np.sum(iters)) if tps else None
 
     # ---- end to end through the public API (host buffers) ----
@@ -567,9 +569,9 @@ def main():
             "gpu_launches": 2 * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "k_solve", "alg_bytes_per_launch": alg_bytes,
+                         "kernel": kernel, "alg_bytes_per_launch": alg_bytes,
                          "traffic_note": "DRAM bytes per launch, scaled from the 1024-spot ncu capture by "
-                                         "spot-iterations (profiles/k_solve_river_datagen_1024.md)"},
+                                         f"spot-iterations (profiles/{kernel}_river_datagen_1024.md)"},
             "cpu_baseline": cpu,
             "plain_gpu": plain,
             "river_game": river,

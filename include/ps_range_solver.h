@@ -256,8 +256,8 @@ typedef struct ps_batch_opts {
                              warps take the ready items of any of them (k_flow).  Results
                              are the same bits either way. */
   int32_t flow_threads;   /* dataflow: threads per CTA, a multiple of 32 from 128 to 1024
-                             (0 = 512; with block_threads = -1 the autotuner chooses) */
-  int32_t flow_spots_per_cta; /* dataflow: spots a CTA holds at once, 1..8 (0 = 2, or autotuned) */
+                             (0 = 1024; with block_threads = -1 the autotuner chooses) */
+  int32_t flow_spots_per_cta; /* dataflow: spots a CTA holds at once, 1..8 (0 = 3, or autotuned) */
   int32_t node_parts;     /* dataflow: column blocks each node op is cut into, 1..16
                              (0 = 3, or autotuned) */
 } ps_batch_opts;

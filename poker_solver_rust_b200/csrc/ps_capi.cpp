@@ -558,9 +558,9 @@ struct Batch {
       if (sched < PS_SCHED_DEFAULT || sched > PS_SCHED_FLOW) return fail(PS_ERR_INVALID, "unknown scheduler");
       flow = sched == PS_SCHED_FLOW || (sched == PS_SCHED_DEFAULT && n > dc->nsm);
       if (flow) {
-        int fb = opts && opts->flow_threads > 0 ? opts->flow_threads : 512;
+        int fb = opts && opts->flow_threads > 0 ? opts->flow_threads : 1024;
         fb = std::max(128, std::min(kMaxFlowThreads, (fb / 32) * 32));
-        const int fl = opts && opts->flow_spots_per_cta > 0 ? opts->flow_spots_per_cta : 2;
+        const int fl = opts && opts->flow_spots_per_cta > 0 ? opts->flow_spots_per_cta : 3;
         const int fp = opts && opts->node_parts > 0 ? opts->node_parts : 3;
         if (fl > kMaxFlowLanes || fp > 16) return fail(PS_ERR_INVALID, "flow_spots_per_cta 1..8, node_parts 1..16");
         const int rc = adopt_flow(fb, opts && opts->scan_buffers > 0 ? opts->scan_buffers : fb / 64, fl, fp,

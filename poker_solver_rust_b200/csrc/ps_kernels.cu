@@ -1367,7 +1367,14 @@ __device__ int lane_pass_end(Lane& L, const FlowArgs& A) {
 // any pass that ends and to the next spot when this one is finished.  Leaves
 // the lane published (false) or retired (true).  Once a step is published
 // other warps own the lane again, so nothing of it is read afterwards.
+#ifndef PS_FLOW_MOVE_OUTLINE
+#define PS_FLOW_MOVE_OUTLINE 0
+#endif
+#if PS_FLOW_MOVE_OUTLINE
+__device__ __noinline__ bool lane_move(Lane& L, const FlowArgs& A, const SmemPlan& plan) {
+#else
 __device__ bool lane_move(Lane& L, const FlowArgs& A, const SmemPlan& plan) {
+#endif
   const int lane = threadIdx.x & 31;
   for (;;) {
     __syncwarp();
@@ -1482,7 +1489,7 @@ constexpr long long kFlowIdleNs = 2000000000LL;  // 2 s without any finished ste
 #define PS_FLOW_SLEEP_MIN 32
 #endif
 #ifndef PS_FLOW_SLEEP_MAX
-#define PS_FLOW_SLEEP_MAX 512
+#define PS_FLOW_SLEEP_MAX 2048
 #endif
 constexpr unsigned kFlowSleepMinNs = PS_FLOW_SLEEP_MIN, kFlowSleepMaxNs = PS_FLOW_SLEEP_MAX;  // idle back-off
 
@@ -1564,7 +1571,7 @@ __global__ void __launch_bounds__(kMaxFlowBlock, 1) k_flow(FlowArgs A, SmemPlan 
       continue;
     }
     // nothing to claim: finished, or wait for a step to end.  Idle warps back
-    // off (32 ns doubling to 512 ns) so their polls take few issue slots from
+    // off (32 ns doubling to 2048 ns) so their polls take few issue slots from
     // the working ones; the wait bound is checked every 16 polls.
     int stop = 0;
     if (lane == 0) {
