@@ -1177,9 +1177,6 @@ __global__ void PS_SOLVE_BOUNDS k_solve(const SpotDev* __restrict__ spots, int n
 // its claim.
 constexpr int kMaxLanes = 8;
 constexpr int kMaxFlowBlock = 1024;
-#ifndef PS_DISCARD
-#define PS_DISCARD 1  // the flow finisher drops a lane's dead working slots from L2 at each pass end
-#endif
 enum LanePhase : int { LP_BR0 = 0, LP_BR1, LP_AVG0, LP_AVG1, LP_DCFR0, LP_DCFR1, LP_EPI0, LP_EPI1, LP_RETIRED };
 
 struct Lane {
@@ -1390,16 +1387,6 @@ __device__ bool lane_move(Lane& L, const FlowArgs& A, const SmemPlan& plan) {
     }
     const int next = lane_pass_end(L, A);
     __syncwarp();
-#if PS_DISCARD
-    {  // every working slot of the lane is dead now (each pass writes a slot before it reads it): drop the
-       // lines from L2 without writing them back
-      const char* b = reinterpret_cast<const char*>(L.slots);
-      const size_t bytes = (size_t)sp.num_slots * sp.vstride * 4;
-      for (size_t i = (size_t)lane * 128; i < bytes; i += 32 * 128)
-        asm volatile("discard.global.L2 [%0], 128;" ::"l"(__cvta_generic_to_global(b + i)) : "memory");
-      __syncwarp();
-    }
-#endif
     if (next < 0) {  // the spot is finished: its results, then the next spot
       int bound = 0;
       if (lane == 0) {
