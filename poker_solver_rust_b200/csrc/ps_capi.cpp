@@ -239,7 +239,7 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 struct Layout {  // byte offsets inside the pool
   size_t cards[2], w[2], same[2], ops[2], steps[2], groups[2], nodes, board_cards, iso_perm[2], iso_off, iso_ent;  // static
   size_t gidx[2], coff[2], thr[2], nvalid[2], heads[2];                                                       // setup
-  size_t R, S, ipcfv, chcfv, rootv[2];                                                                // state
+  size_t R, S, SG, ipcfv, chcfv, rootv[2];                                                              // state
   size_t bcfv, breach;  // boundary values and boundary reach (kept across state resets)
 };
 
@@ -384,6 +384,7 @@ struct Batch {
       L.iso_ent = take(so, g.iso_list.size() * 8 + 16);
       L.R = take(st, g.num_storage * 4 + 16);
       L.S = take(st, g.num_storage * 4 + 16);
+      L.SG = take(st, g.num_storage * 4 + 16);  // strategy cache of the DCFR passes
       L.ipcfv = take(st, g.num_storage_ip * 4 + 16);
       L.chcfv = take(st, g.num_storage_chance * 4 + 16);
       for (int p = 0; p < 2; ++p) L.rootv[p] = take(st, (size_t)g.hs[p] * 4);
@@ -501,6 +502,7 @@ struct Batch {
       for (int p = 0; p < 2; ++p) s.root_out[p] = (float*)(dT + L.rootv[p]);
       s.R = (float*)(dT + L.R);
       s.S = (float*)(dT + L.S);
+      s.SG = (float*)(dT + L.SG);
       s.ipcfv = (float*)(dT + L.ipcfv);
       s.chcfv = (float*)(dT + L.chcfv);
     };

@@ -95,6 +95,7 @@ struct SpotDev {
   const int32_t* iso_ent;      // pairs (reference child index, perm id)
   float* R;            // regrets / saved cfvalues
   float* S;            // cumulative strategy
+  float* SG;           // strategy cache of the DCFR passes, laid out like R, or null
   float* ipcfv;        // IP cfvalues at root / chance children (finalize)
   float* chcfv;        // chance-node cfvalues (finalize)
   float* slots;        // [num_slots][vstride] scratch vectors
