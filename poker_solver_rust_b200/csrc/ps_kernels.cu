@@ -522,22 +522,33 @@ __device__ __forceinline__ void warp_terms_inl(const Ctx& c, const Op* ops, int 
     const int lo = min(lane * C, n3), hi = min(lo + C, n3);
     float run = 0.f;
     int first = hi;
-    for (int j = lo; j < hi; ++j) {
-      float x = e[j];
-      bool head;
-      if (bits) {
-        head = (hd[j >> 5] >> (j & 31)) & 1u;
-      } else {
-        head = signbit(x);
-        if (head) x = -x;
+    if (bits) {
+      for (int j = lo; j < hi; ++j) {
+        const float x = e[j];
+        if ((hd[j >> 5] >> (j & 31)) & 1u) {
+          run = x;
+          first = min(first, j);
+        } else {
+          run = __fadd_rn(run, x);
+        }
+        e[j] = run;
       }
-      if (head) {
-        run = x;
-        first = min(first, j);
-      } else {
-        run = __fadd_rn(run, x);
+    } else {
+      // a segment start carries the sign bit of its non-negative value
+#pragma unroll 2
+      for (int j = lo; j < hi; ++j) {
+        const float x = e[j], y = fabsf(x);
+        run = signbit(x) ? y : __fadd_rn(run, y);
+        e[j] = run;
       }
-      e[j] = run;
+      // the chunk's first segment start, from the bitmap the signs came from
+      for (int w = lo >> 5; lo < hi && w <= (hi - 1) >> 5; ++w) {
+        const uint32_t m = hd[w] & (w == lo >> 5 ? ~0u << (lo & 31) : ~0u);
+        if (m) {
+          first = min(hi, (w << 5) + __ffs(m) - 1);
+          break;
+        }
+      }
     }
     float v = run;
     bool f = first < hi;
@@ -599,6 +610,44 @@ __device__ __forceinline__ void warp_terms_inl(const Ctx& c, const Op* ops, int 
           const float rs = si != 0xFFFF ? rch[si] : 0.f;
           const float adj = Tsum + rs - M1 - M2;
           v = __fmul_rn(__fmul_rn(brow[h], nd.payoff_scale), adj);
+        }
+        dst[h] = v;
+      }
+      continue;
+    }
+    // whole-warp runs (no split copies: those of the lone-spot grid ran slower so)
+    if (!GEN && !SPLIT && op.term == TERM_SHOWDOWN && !sp.raked) {  // unraked showdowns in a loop of their own
+#pragma unroll 2
+      for (int h = h0; h < hsp; h += hstep) {
+        float v = 0.f;
+        const uint4 t = tn;
+        tn = h + hstep < Hp ? thr[h + hstep] : make_uint4(THR_INVALID, 0, 0, 0);
+        if (t.x != THR_INVALID) {
+          const float M1 = buf[t.z & 0xFFFF], M2 = buf[t.w >> 16];
+          const float Plt = buf[t.x & 0xFFFF], Ple = buf[t.x >> 16];
+          const float Q1lt = buf[t.y & 0xFFFF], Q1le = buf[t.y >> 16];
+          const float Q2lt = buf[t.z >> 16], Q2le = buf[t.w & 0xFFFF];
+          const float win = Plt - Q1lt - Q2lt;
+          const float lose = (Tsum - Ple) - (M1 - Q1le) - (M2 - Q2le);
+          v = __fadd_rn(__fmul_rn(cw, win), __fmul_rn(cl, lose));
+        }
+        dst[h] = v;
+      }
+      continue;
+    }
+    if (!GEN && !SPLIT && op.term == TERM_FOLD) {  // folds in a loop of their own
+      const float cf = op.fold_pl != pay ? aw : al;
+#pragma unroll 2
+      for (int h = h0; h < hsp; h += hstep) {
+        float v = 0.f;
+        const uint4 t = tn;
+        tn = h + hstep < Hp ? thr[h + hstep] : make_uint4(THR_INVALID, 0, 0, 0);
+        if (t.x != THR_INVALID) {
+          const float M1 = buf[t.z & 0xFFFF], M2 = buf[t.w >> 16];
+          const uint32_t si = same[h];
+          const float rs = si != 0xFFFF ? rch[si] : 0.f;
+          const float adj = Tsum + rs - M1 - M2;
+          v = __fmul_rn(cf, adj);
         }
         dst[h] = v;
       }
@@ -1275,6 +1324,11 @@ struct FlowArgs {
   int node_parts;  // column blocks per node op (1 = whole ops)
 };
 
+// Publications of the CTA's lanes so far.  Items appear only when a step is
+// published, so a warp that found none at epoch e scans the claim words again
+// only once the epoch has moved: an idle poll is one shared load.
+__shared__ unsigned s_flow_epoch;
+
 // Publishes step L.step of the lane's current pass (finisher / binder only).
 __device__ void lane_publish_step(Lane& L, const SpotDev& sp, int node_parts) {
   const int p = lane_player(L.phase);
@@ -1299,6 +1353,8 @@ __device__ void lane_publish_step(Lane& L, const SpotDev& sp, int node_parts) {
     atomicExch(&L.wn, n);
     atomicExch(&L.wt, t);
   }
+  __threadfence_block();  // the claim words before the epoch that announces them
+  atomicAdd(&s_flow_epoch, 1u);
 }
 
 // The reference loop's decision after a completed exploitability check
@@ -1553,7 +1609,9 @@ __global__ void __launch_bounds__(kMaxFlowBlock, 1) k_flow(FlowArgs A, SmemPlan 
   if (threadIdx.x == 0) {
     s_retired = 0;
     s_progress = 0;
+    s_flow_epoch = 0;
   }
+  __syncthreads();
   if (warp < K) {
     Lane& L = lanes[warp];
     int bound = 0;
@@ -1569,20 +1627,26 @@ __global__ void __launch_bounds__(kMaxFlowBlock, 1) k_flow(FlowArgs A, SmemPlan 
   unsigned seen = 0;
   unsigned long long idle_since = global_ns();
   unsigned backoff = kFlowSleepMinNs, polls = 0;
+  unsigned empty_epoch = ~0u;  // lane 0: the epoch of this warp's last scan that found nothing
   int start = warp % K;
   for (;;) {
     int k = -1, idx = -1, term = 0;
     if (lane == 0) {
-      for (int r = 0; r < K && idx < 0; ++r) {
-        k = start + r < K ? start + r : start + r - K;
-        Lane& L = lanes[k];
-        if (buf) {
-          idx = try_claim(&L.wt);
-          term = idx >= 0;
+      const unsigned ep = *reinterpret_cast<volatile unsigned*>(&s_flow_epoch);
+      if (ep != empty_epoch) {
+        __threadfence_block();  // the claim words published up to epoch ep
+        for (int r = 0; r < K && idx < 0; ++r) {
+          k = start + r < K ? start + r : start + r - K;
+          Lane& L = lanes[k];
+          if (buf) {
+            idx = try_claim(&L.wt);
+            term = idx >= 0;
+          }
+          if (idx < 0) idx = try_claim(&L.wn);
         }
-        if (idx < 0) idx = try_claim(&L.wn);
+        if (idx < 0) empty_epoch = ep;
+        __threadfence_block();  // acquire: the claimed step's fields and inputs
       }
-      __threadfence_block();  // acquire: the claimed step's fields and inputs
     }
     idx = __shfl_sync(0xffffffffu, idx, 0);
     if (idx >= 0) {
