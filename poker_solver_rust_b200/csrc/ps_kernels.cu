@@ -1330,12 +1330,24 @@ struct FlowArgs {
 __shared__ unsigned s_flow_epoch;
 
 // Publishes step L.step of the lane's current pass (finisher / binder only).
-__device__ void lane_publish_step(Lane& L, const SpotDev& sp, int node_parts) {
+#ifndef PS_FLOW_ADAPT
+#define PS_FLOW_ADAPT 0
+#endif
+__device__ void lane_publish_step(Lane& L, const SpotDev& sp, int node_parts, int lanes) {
   const int p = lane_player(L.phase);
   const Step st = sp.steps[p][L.step];
   L.begin = st.begin;
   L.n_elem = st.n_elem;
   L.gbegin = st.gbegin;
+#if PS_FLOW_ADAPT
+  if (st.n_elem > 0) {
+    // thin steps: more column blocks, up to one per 32 columns of the wider player
+    const int target = (PS_FLOW_ADAPT * (int)(blockDim.x >> 5) + lanes - 1) / lanes;
+    const int cap = max(1, (max(sp.hs[0], sp.hs[1]) + 127) >> 7);
+    const int want = (target - st.n_groups + st.n_elem - 1) / st.n_elem;
+    node_parts = max(node_parts, min(cap, want));
+  }
+#endif
   L.parts = node_parts;
   L.total = st.n_groups + st.n_elem * node_parts;
   L.done = 0;
@@ -1489,7 +1501,7 @@ __device__ bool lane_move(Lane& L, const FlowArgs& A, const SmemPlan& plan) {
       __syncwarp();  // every lane has read the fields above before lane 0 publishes
       if (lane == 0) {
         L.step += 1;
-        lane_publish_step(L, sp, A.node_parts);
+        lane_publish_step(L, sp, A.node_parts, A.lanes);
       }
       return false;
     }
