@@ -298,11 +298,20 @@ int ps_batch_scan_buffers(ps_batch* b);
 /* the launch shape of the batch's solves: out[0] scheduler (PS_SCHED_STEP or
  * PS_SCHED_FLOW), [1] threads per CTA, [2] CTAs, [3] CTAs per SM, [4]
  * scan-buffer warps per CTA, [5] spots per CTA, [6] node-op parts, [7] 1 when
- * a single spot runs in grid mode (every SM on it) */
+ * a single spot runs in grid mode (every SM on it), 2 when it runs on the CTAs
+ * of one thread-block cluster */
 int ps_batch_schedule(ps_batch* b, int32_t out[8]);
+/* No counterpart in the reference.  The launch shape of a single game's
+ * solves, as ps_batch_schedule; in grid mode out[2] is the CTAs of the grid
+ * (or of the cluster).  PS_ERR_STATE before allocate_memory. */
+int ps_game_schedule(ps_game* g, int32_t out[8]);
 /* the trials of the last autotune: per trial 4 values (threads per CTA,
  * scan-buffer warps, spots per CTA, node-op parts; the last two 0 for a
- * step-synchronous trial) and its device ms; returns the count */
+ * step-synchronous trial) and its device ms; returns the count.  A dataflow
+ * autotune lists its sweep (every shape, one wave of sample spots) and then
+ * the refine runs of the shapes within 6% of the sweep's best on four times
+ * the spots; a shape's second entry is its refine run, and the fastest refine
+ * run is the choice. */
 int ps_batch_autotune_trials(ps_batch* b, int32_t* shape, float* trial_ms, int cap);
 /* bytes copied host->device by ps_batch_new and device->host by ps_batch_results */
 int ps_batch_io_bytes(ps_batch* b, uint64_t* h2d, uint64_t* d2h);

@@ -87,6 +87,7 @@ _sig("ps_discount_params", i32, u32, P(f32))
 _sig("ps_debug_grid_barrier_timeout", i32, i32, i32, i64, i32, P(i32), P(i32), P(f32))
 _sig("ps_game_program_info", i32, vp, P(i64))
 _sig("ps_game_set_terminals_first", i32, vp, i32)
+_sig("ps_game_schedule", i32, vp, P(i32))
 _sig("ps_eval_fixed_strategy_ex", i32, vp, vp, vp, vp, vp, i32)
 _sig("ps_eval_fixed_strategy_adjoint_ex", i32, vp, vp, vp, vp, vp, vp, vp, vp, i32)
 _sig("ps_set_boundary_cfvs_all", i32, vp, vp, i32)

@@ -290,6 +290,7 @@ struct Batch {
   // grid mode: a single large spot runs on every CTA of a cooperative launch
   bool grid_mode = false;
   int grid_blocks = 0;
+  int grid_cluster = 0;  // grid mode on the CTAs of one thread-block cluster (hardware barrier)
   unsigned* d_bar = nullptr;
   double* d_gred = nullptr;
   // dataflow scheduler (k_flow) for solve and run_iterations; the adjoint
@@ -585,6 +586,16 @@ struct Batch {
           grid_blocks = gc;
           CU(cudaMalloc(&d_bar, 64));
           CU(cudaMalloc(&d_gred, 64));
+          // PS_GRID_CLUSTER = C (2..16): the game runs on one cluster of C CTAs instead
+          const char* cl = std::getenv("PS_GRID_CLUSTER");
+          const int want = cl ? std::atoi(cl) : 0;
+          if (want >= 2) {
+            const int cc = grid_cluster_fits(std::min(want, 16), block, plan);
+            if (cc >= 2) {
+              grid_blocks = cc;
+              grid_cluster = 1;
+            }
+          }
         }
       }
     }
@@ -739,13 +750,22 @@ struct Batch {
       int occ, g;
       if (flow_shape(c.b, c.bufs, c.lanes, cap_ctas, n, pl, occ, g)) ns = std::max(ns, g * c.lanes);
     }
-    ns = std::min(n, ns);
+    // the sweep's sample fills every candidate's lanes once; the refine runs
+    // take kRefineWaves times as many spots, so lanes are rebound from the
+    // queue as in a whole batch
+    constexpr int kRefineWaves = 4;
+    const int ns_sweep = std::min(n, ns);
+    ns = std::min(n, kRefineWaves * ns);
     std::vector<SpotDev> sample(ns);
     std::vector<int> ids(ns);
     for (int i = 0; i < ns; ++i) {
       sample[i] = h_spots[order[(size_t)i * n / ns]];
       ids[i] = i;
     }
+    // the sweep's spots: every kRefineWaves-th of the refine sample, so they
+    // too are spread evenly over the cost order
+    std::vector<int> sweep_ids(ns_sweep);
+    for (int i = 0; i < ns_sweep; ++i) sweep_ids[i] = (int)((size_t)i * ns / ns_sweep);
     int rc = run_setup();
     if (rc) return rc;
     constexpr int kTrialIters = 6;
@@ -758,12 +778,13 @@ struct Batch {
         max_scr = std::max(max_scr, (size_t)g * c.lanes);
     }
     char* tmp = nullptr;
-    const size_t tb = align256(sizeof(SpotDev) * ns) + align256(16 * (size_t)ns) + 256;
+    const size_t tb = align256(sizeof(SpotDev) * ns) + align256(20 * (size_t)ns) + 256;
     CU(cudaMalloc(&tmp, tb));
     std::unique_ptr<char, decltype(&cudaFree)> k1(tmp, &cudaFree);
     SpotDev* d_sample = (SpotDev*)tmp;
-    int* d_ids = (int*)(tmp + align256(sizeof(SpotDev) * ns));
-    float* d_tz = (float*)(d_ids + ns);      // targets 0: every sampled spot runs all trial iterations
+    int* d_ids = (int*)(tmp + align256(sizeof(SpotDev) * ns));  // the refine runs' queue: 0 .. ns-1
+    int* d_sweep = d_ids + ns;                                   // the sweep's queue
+    float* d_tz = (float*)(d_sweep + ns);    // targets 0: every sampled spot runs all trial iterations
     float* d_te = d_tz + ns;
     int* d_ti = (int*)(d_te + ns);
     int* d_cnt = (int*)(tmp + tb - 256);
@@ -772,29 +793,61 @@ struct Batch {
     std::unique_ptr<float, decltype(&cudaFree)> k2(d_tscratch, &cudaFree);
     CU(cudaMemcpyAsync(d_sample, sample.data(), sizeof(SpotDev) * ns, cudaMemcpyHostToDevice, stream));
     CU(cudaMemcpyAsync(d_ids, ids.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, stream));
+    CU(cudaMemcpyAsync(d_sweep, sweep_ids.data(), sizeof(int) * ns_sweep, cudaMemcpyHostToDevice, stream));
     CU(cudaMemsetAsync(d_tz, 0, sizeof(float) * ns, stream));
     const SolveJob job{0, kTrialIters, 1, 0};
-    Cand best{flow_block, flow_plan.bufs, flow_lanes, flow_parts};
-    float best_ms = 0;
-    for (const auto& c : cands) {
+    // one trial: a warm-up run, then the timed run (device ms)
+    auto trial = [&](const Cand& c, const int* q, int nq, float* out_ms, int* out_bufs) -> cudaError_t {
       SmemPlan pl;
       int occ, g;
-      if (!flow_shape(c.b, c.bufs, c.lanes, cap_ctas, ns, pl, occ, g)) continue;
-      for (int rep = 0; rep < 2; ++rep) {  // the first run warms the shape up, the second is timed
-        CU(cudaMemsetAsync(d_cnt, 0, sizeof(int), stream));
-        CU(cudaEventRecord(ev[2], stream));
-        CU(launch_flow(d_sample, ns, d_ids, d_cnt, d_disc, job, d_tz, d_tscratch, scratch_floats, d_te, d_ti, d_err,
-                       g, c.b, c.lanes, c.parts, pl, stream));
-        CU(cudaEventRecord(ev[3], stream));
+      *out_ms = 0.f;
+      if (!flow_shape(c.b, c.bufs, c.lanes, cap_ctas, nq, pl, occ, g)) return cudaSuccess;
+      cudaError_t e = cudaSuccess;
+      for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {
+        e = cudaMemsetAsync(d_cnt, 0, sizeof(int), stream);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[2], stream);
+        if (e == cudaSuccess)
+          e = launch_flow(d_sample, nq, q, d_cnt, d_disc, job, d_tz, d_tscratch, scratch_floats, d_te, d_ti, d_err,
+                          g, c.b, c.lanes, c.parts, pl, stream);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[3], stream);
       }
-      CU(cudaStreamSynchronize(stream));
+      if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+      if (e == cudaSuccess) e = cudaEventElapsedTime(out_ms, ev[2], ev[3]);
+      *out_bufs = pl.bufs;
+      return e;
+    };
+    Cand best{flow_block, flow_plan.bufs, flow_lanes, flow_parts};
+    float best_ms = 0;
+    std::vector<std::pair<float, Cand>> swept;
+    for (const auto& c : cands) {
       float ms = 0;
-      CU(cudaEventElapsedTime(&ms, ev[2], ev[3]));
-      Trial t{c.b, pl.bufs, ms, c.lanes, c.parts};
-      tune_log.push_back(t);
+      int bufs = 0;
+      CU(trial(c, d_sweep, ns_sweep, &ms, &bufs));
+      if (ms <= 0.f) continue;
+      tune_log.push_back(Trial{c.b, bufs, ms, c.lanes, c.parts});
+      swept.push_back({ms, Cand{c.b, bufs, c.lanes, c.parts}});
       if (best_ms == 0 || ms < best_ms) {
         best_ms = ms;
-        best = {c.b, pl.bufs, c.lanes, c.parts};
+        best = {c.b, bufs, c.lanes, c.parts};
+      }
+    }
+    // refine: the shapes within 6% of the sweep's best (at most 6) run again on
+    // the larger sample, where each lane takes several spots in turn; the
+    // fastest of those runs is kept
+    if (ns > ns_sweep && !swept.empty()) {
+      std::stable_sort(swept.begin(), swept.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+      float best_refined = 0;
+      for (size_t i = 0; i < swept.size() && i < 6 && swept[i].first <= 1.06f * best_ms; ++i) {
+        const Cand& c = swept[i].second;
+        float ms = 0;
+        int bufs = 0;
+        CU(trial(c, d_ids, ns, &ms, &bufs));
+        if (ms <= 0.f) continue;
+        tune_log.push_back(Trial{c.b, bufs, ms, c.lanes, c.parts});
+        if (best_refined == 0 || ms < best_refined) {
+          best_refined = ms;
+          best = c;
+        }
       }
     }
     if ((rc = check_err())) return rc;
@@ -938,7 +991,7 @@ struct Batch {
   // One grid-mode launch of this batch's single spot.
   cudaError_t grid_launch(const GridJob& job) {
     return launch_grid(d_spots, job, d_disc, d_scratch, scratch_floats, d_expl, d_iters, d_bar, d_gred, d_err,
-                       grid_blocks, block, plan, stream);
+                       grid_blocks, block, plan, stream, grid_cluster);
   }
 
   // Average-strategy pass(es) of the single spot: on every SM in grid mode,
@@ -1001,7 +1054,7 @@ struct Batch {
       CU(cudaEventRecord(ev[2], stream));
       GridJob job{GRID_SOLVE, 0, (int)max_iter, target[0], 0, -1, nullptr, nullptr, nullptr};
       CU(launch_grid(d_spots, job, d_disc, d_scratch, scratch_floats, d_expl, d_iters, d_bar, d_gred, d_err,
-                     grid_blocks, block, plan, stream));
+                     grid_blocks, block, plan, stream, grid_cluster));
       CU(cudaEventRecord(ev[3], stream));
       h_expl.resize(1);
       h_iters.resize(1);
@@ -2608,9 +2661,7 @@ int ps_batch_config(ps_batch* pb, int32_t* block, int32_t* grid, int32_t* cps) {
   return PS_OK;
 }
 
-int ps_batch_schedule(ps_batch* pb, int32_t out[8]) {
-  if (!pb || !out) return fail(PS_ERR_INVALID, "null argument");
-  const Batch& B = *pb->b;
+static void schedule_of(const Batch& B, int32_t out[8]) {
   out[0] = B.flow ? PS_SCHED_FLOW : PS_SCHED_STEP;
   out[1] = B.flow ? B.flow_block : B.block;
   out[2] = B.flow ? B.flow_grid : B.grid;
@@ -2618,7 +2669,20 @@ int ps_batch_schedule(ps_batch* pb, int32_t out[8]) {
   out[4] = B.flow ? B.flow_plan.bufs : B.plan.bufs;
   out[5] = B.flow ? B.flow_lanes : B.inst_k;
   out[6] = B.flow ? B.flow_parts : 1;
-  out[7] = B.grid_mode ? 1 : 0;
+  out[7] = B.grid_mode ? (B.grid_cluster ? 2 : 1) : 0;
+}
+
+int ps_batch_schedule(ps_batch* pb, int32_t out[8]) {
+  if (!pb || !out) return fail(PS_ERR_INVALID, "null argument");
+  schedule_of(*pb->b, out);
+  return PS_OK;
+}
+
+int ps_game_schedule(ps_game* g, int32_t out[8]) {
+  if (!g || !out) return fail(PS_ERR_INVALID, "null argument");
+  if (g->state == GState::TreeBuilt) return fail(PS_ERR_STATE, "Memory is not allocated");
+  schedule_of(*g->b, out);
+  if (g->b->grid_mode) out[2] = g->b->grid_blocks;
   return PS_OK;
 }
 

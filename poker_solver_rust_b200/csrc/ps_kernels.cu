@@ -83,7 +83,8 @@ struct Ctx {
   float* slots;
   int vstride;
   const float* root_reach;
-  int grid;      // 1: every CTA of the launch works on this one spot (steps end in a grid barrier)
+  int grid;      // 1: every CTA of the launch works on this one spot (steps end in a grid barrier);
+                 // 2: the same on the CTAs of one cluster (steps end in the cluster barrier)
   unsigned* bar; // grid mode: barrier counter and generation
   double* gred;  // grid mode: root reductions shared by all CTAs
   int* err;
@@ -732,6 +733,14 @@ __device__ __forceinline__ unsigned long long global_ns() {
 }
 
 __device__ bool grid_barrier(const Ctx& c) {
+  if (c.grid == 2) {
+    // one cluster: the hardware barrier over every thread of its CTAs, with
+    // cluster-scope release / acquire (the spot's global-memory vectors and
+    // root values are written and read by those CTAs only).  Every CTA runs
+    // the same steps, so every thread arrives; nothing spins.
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+    return true;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     cuda::atomic_ref<unsigned, cuda::thread_scope_device> count(c.bar[0]), gen(c.bar[1]), abort_(c.bar[2]);
@@ -864,7 +873,10 @@ __device__ __noinline__ void run_pass_split(const Ctx& c, int p, const Discount 
     // run (CTAs 0 .. ng-1); otherwise split over the buffer warps a step
     // leaves idle (at most 8 parts a run, and at most half the warps when the
     // step has node ops to split as well)
-    const bool cta_runs = c.grid && !gen && ng > 0 && c.bufs == nw0 && 2 * ng <= (int)gridDim.x;
+    // (a cluster has few CTAs: there a step without node ops gives a CTA to
+    // each of up to gridDim.x runs)
+    const bool cta_runs = c.grid && !gen && ng > 0 && c.bufs == nw0 &&
+                          (2 * ng <= (int)gridDim.x || (c.grid == 2 && ne == 0 && ng <= (int)gridDim.x));
     const int TP = gen || ng == 0 ? 1 : max(1, min(8, min(nb, ne > 0 ? nw / 2 : nw) / ng));
     if (cta_runs) {
       for (int j = blockIdx.x; j < ng; j += gridDim.x) {
@@ -1732,7 +1744,7 @@ __global__ void PS_SOLVE_BOUNDS k_grid(const SpotDev* __restrict__ spot, const D
   Ctx c;
   const bool ok = bind_ctx(c, spot, scratch, scratch_floats, smem, plan, err);
   if (!ok) return;  // the check is the same on every CTA
-  c.grid = 1;
+  c.grid = job.cluster ? 2 : 1;
   c.bar = bar;
   c.gred = gred;
   c.wait_ns = job.wait_ns;
@@ -2137,19 +2149,63 @@ int grid_ctas(int block, const SmemPlan& plan) {
   return nsm * per_sm;
 }
 
+static cudaError_t grid_cluster_attrs() {
+  cudaError_t e = cudaFuncSetAttribute((const void*)k_grid, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  return e;
+}
+
+int grid_cluster_fits(int ctas, int block, const SmemPlan& plan) {
+  if (ctas < 2 || ctas > 16) return 0;
+  const size_t smem = plan.total();
+  if (set_smem((const void*)k_grid, smem) != cudaSuccess || grid_cluster_attrs() != cudaSuccess) return 0;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = ctas;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(ctas);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, (const void*)k_grid, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n > 0 ? ctas : 0;
+}
+
 cudaError_t launch_grid(const SpotDev* spot, const GridJob& job, const Discount* disc, float* scratch,
                         size_t scratch_floats, float* out_expl, int* out_iters, unsigned* bar, double* gred,
-                        int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s) {
+                        int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s, int cluster) {
   size_t smem = plan.total();
   cudaError_t e = set_smem((const void*)k_grid, smem);
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), s);  // count, generation, abort word
   if (e != cudaSuccess) return e;
   GridJob j = job;
+  j.cluster = cluster ? 1 : 0;
   SmemPlan pl = plan;
   void* args[] = {(void*)&spot, (void*)&disc, (void*)&scratch, (void*)&scratch_floats, (void*)&out_expl,
                   (void*)&out_iters, (void*)&bar, (void*)&gred, (void*)&j, (void*)&pl, (void*)&err};
-  return cudaLaunchCooperativeKernel((const void*)k_grid, dim3(grid), dim3(block), args, smem, s);
+  if (!cluster) return cudaLaunchCooperativeKernel((const void*)k_grid, dim3(grid), dim3(block), args, smem, s);
+  if (grid < 2 || grid > 16) return cudaErrorInvalidValue;
+  if ((e = grid_cluster_attrs()) != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = grid;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelExC(&cfg, (const void*)k_grid, args);
 }
 
 cudaError_t launch_iterate(const SpotDev* spots, int nspots, const Discount* disc, int t0, int t1, float* scratch,

@@ -58,6 +58,7 @@ struct GridJob {
   float* out;              // GRID_AVERAGE: root values [H_player]
   float* breach = nullptr; // GRID_AVERAGE: boundary reach buffer or null
   long long wait_ns = 1000000000LL;  // a grid barrier's wait limit before the launch aborts with ERR_WAIT
+  int cluster = 0;                   // set by launch_grid: the CTAs form one cluster (hardware barrier)
 };
 int grid_ctas(int block, const SmemPlan& plan);
 // Reach-weighted 48-river average of boundary-network outputs (ps_datagen.cu):
@@ -128,9 +129,14 @@ struct SamplerParams {
 // rejection exhausted); all device pointers.
 cudaError_t launch_sample_situations(const SamplerParams& P, int n, uint8_t* boards, int32_t* pots, int32_t* stacks,
                                      float* ranges, int* err, cudaStream_t s);
+// cluster = 0: a cooperative launch of `grid` CTAs whose steps end in the
+// software grid barrier; cluster = 1: one thread-block cluster of `grid` CTAs
+// (at most 16) whose steps end in the hardware cluster barrier.
 cudaError_t launch_grid(const SpotDev* spot, const GridJob& job, const Discount* disc, float* scratch,
                         size_t scratch_floats, float* out_expl, int* out_iters, unsigned* bar, double* gred,
-                        int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s);
+                        int* err, int grid, int block, const SmemPlan& plan, cudaStream_t s, int cluster = 0);
+// CTAs of one cluster launch of k_grid that fit the device at once (0 = none)
+int grid_cluster_fits(int ctas, int block, const SmemPlan& plan);
 cudaError_t launch_setup(const SpotDev* spots, const int2* work, int nwork, const int32_t* table, int* err,
                          int grid, cudaStream_t s);
 // Work of one persistent batched-solve launch.

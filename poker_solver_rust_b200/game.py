@@ -192,6 +192,15 @@ class PostFlopGame:
                 "node_ops": [int(v[4]), int(v[5])], "terminal_ops": [int(v[6]), int(v[7])],
                 "terminal_runs": [int(v[8]), int(v[9])], "S": int(v[10]), "boards": int(v[11])}
 
+    def schedule(self) -> dict:
+        """The launch shape of the game's solves (ps_game_schedule): grid mode
+        runs the game on every SM (cooperative grid, "grid") or on the CTAs of
+        one thread-block cluster ("cluster")."""
+        v = (C.c_int32 * 8)()
+        N.check(N.lib().ps_game_schedule(self._h, v))
+        return {"block_threads": int(v[1]), "ctas": int(v[2]),
+                "mode": {0: "one CTA", 1: "grid", 2: "cluster"}[int(v[7])]}
+
     def allocate_memory(self, enable_compression: bool = False) -> None:
         N.check(N.lib().ps_game_allocate_memory(self._h, int(enable_compression)))
 
@@ -614,14 +623,25 @@ class BatchSolver:
     def autotune_trials(self):
         """Every trial of the last autotune: dicts of threads per CTA,
         scan-buffer warps, spots per CTA and node-op parts (0 for a
-        step-synchronous trial) and the trial's device ms."""
+        step-synchronous trial), the trial's device ms and its stage: "sweep"
+        for the trials of every shape on one wave of spots, "refine" for the
+        re-runs of the leading shapes on a larger sample (the library lists
+        them after the sweep, so a shape's second entry is its refine run);
+        the choice is the fastest refine run, or the fastest sweep trial
+        when there was none."""
         cap = 256
         shape = (C.c_int32 * (4 * cap))()
         t = (C.c_float * cap)()
         n = min(N.check(N.lib().ps_batch_autotune_trials(self._h, shape, t, cap)), cap)
-        return [{"block_threads": int(shape[4 * i]), "scan_buffers": int(shape[4 * i + 1]),
-                 "spots_per_cta": int(shape[4 * i + 2]), "node_parts": int(shape[4 * i + 3]),
-                 "trial_ms": float(t[i])} for i in range(n)]
+        out, seen, stage = [], set(), "sweep"
+        for i in range(n):
+            k = tuple(int(shape[4 * i + j]) for j in range(4))
+            if k in seen:
+                stage = "refine"
+            seen.add(k)
+            out.append({"block_threads": k[0], "scan_buffers": k[1], "spots_per_cta": k[2], "node_parts": k[3],
+                        "trial_ms": float(t[i]), "stage": stage})
+        return out
 
     def config(self):
         """The launch shape of the batch's solves (ps_batch_schedule)."""

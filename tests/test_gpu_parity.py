@@ -475,6 +475,39 @@ def test_grid_mode_matches_single_cta(monkeypatch):
     assert e1 == e2 and grid.last_iterations == one.last_iterations
 
 
+@pytest.mark.parametrize("ctas", ["8", "16"])
+def test_cluster_mode_matches_grid_mode(monkeypatch, ctas):
+    """A single game on the CTAs of one thread-block cluster (hardware
+    cluster barrier between steps) against the cooperative grid: the items'
+    arithmetic is the same wherever they run, so every query matches bit for
+    bit - the solve loop with its checks, single steps, finalize, root values
+    and the expected values."""
+    r, b, t = spots.river_spot(1)
+    monkeypatch.setenv("PS_GRID_CLUSTER", "0")
+    grid = spots.product_game(r, b, t)
+    monkeypatch.setenv("PS_GRID_CLUSTER", ctas)
+    clu = spots.product_game(r, b, t)
+    assert grid.schedule()["mode"] == "grid"
+    assert clu.schedule()["mode"] == "cluster" and clu.schedule()["ctas"] == int(ctas)
+    for it in range(3):
+        ps.solve_step(grid, it)
+        ps.solve_step(clu, it)
+    assert ps.compute_exploitability(grid) == ps.compute_exploitability(clu)
+    for i in _decision_nodes(grid):
+        assert np.array_equal(grid.node_storage(i, 2), clu.node_storage(i, 2))
+        assert np.array_equal(grid.node_storage(i, 1), clu.node_storage(i, 1))
+    e1 = ps.solve(grid, 60, 0.0)
+    e2 = ps.solve(clu, 60, 0.0)
+    assert e1 == e2 and grid.last_iterations == clu.last_iterations
+    for p in range(2):  # solve() ended with finalize, as the reference's does
+        assert np.array_equal(ps.root_cfvalues(grid, p), ps.root_cfvalues(clu, p))
+    assert np.array_equal(grid.strategy_at_index(0), clu.strategy_at_index(0))
+    for g in (grid, clu):
+        g.cache_normalized_weights()
+    for p in range(2):
+        assert np.array_equal(grid.expected_values(p), clu.expected_values(p))
+
+
 @pytest.mark.parametrize("case", [0, 1, 2])
 def test_regret_matching_known_answers(case):
     """solver.rs:724-750 on the device: one iteration at t = 0 (gamma_0 = 0)
