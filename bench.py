@@ -181,9 +181,10 @@ def turn_game_measure(ps, spots, iters: int, cpu_iters: int):
 def river_game_measure(ps, spots, iters: int, cpu_iters: int):
     """One plain river subgame (5-card board, U[0,1] ranges masked by the
     board, pot 100, stack 200, bets 50% / 100% / all-in, raise 100%) solved
-    for `iters` iterations through ps.solve in grid mode (one cooperative
-    launch over every SM; a single river game is latency-bound, so the line
-    gives iterations/s and the exploitability reached), beside the oracle on
+    for `iters` iterations through ps.solve (one launch on a 16-CTA
+    thread-block cluster, whose hardware barrier ends each step; a single
+    river game is latency-bound, so the line gives iterations/s and the
+    exploitability reached), beside the oracle on
     one host thread (river nodes never parallelise in the reference,
     node.rs:347-349), timed through the same solve loop (checks every 5
     iterations, finalize).  The tree has no bet cap: the reference's tree
@@ -203,7 +204,7 @@ def river_game_measure(ps, spots, iters: int, cpu_iters: int):
            "nodes": g.num_nodes(), "hands": [H0, g.num_private_hands(1)],
            "iterations": iters, "gpu_iterations_per_s": iters / dt, "gpu_ms_per_iteration": dt / iters * 1e3,
            "gpu_note": "ps.solve from host: iterations, exploitability every 5, finalize",
-           "exploitability_pct_pot": 100.0 * e / t.starting_pot,
+           "exploitability_pct_pot": 100.0 * e / t.starting_pot, "launch": g.schedule(),
            "root_action_frequencies": [float(x) for x in root.mean(axis=1)]}
     if cpu_iters > 0:
         o = spots.oracle_game(r, b, t)
@@ -562,8 +563,8 @@ def main():
             ps.solve(g, MAX_ITER, TARGET_FRAC * t.starting_pot)
         plain_s = time.perf_counter() - t0
         plain = {"value": len(sample) / plain_s, "unit": UNIT, "sample": f"first {len(sample)} spots, one "
-                 "game per spot through the single-game API (grid mode: one cooperative solve launch over every "
-                 "SM per spot), host-synchronised"}
+                 "game per spot through the single-game API (one solve launch per spot: on one 16-CTA "
+                 "thread-block cluster for these small trees, on every SM for wide ones), host-synchronised"}
 
     # ---- single turn game (config 2 of the spec), grid mode ----
     turn = None

@@ -51,7 +51,17 @@ struct DeviceConsts {
   unsigned long long ctx = 0;
   int32_t* table = nullptr;
   int nsm = 0;
+  // The library's stream-ordered memory pool of the device: a batch's device
+  // buffers come from it on the batch's stream and go back to it when the
+  // batch ends, so building one batch while another solves neither waits for
+  // the running kernels (as cudaMalloc / cudaFree do) nor maps memory anew.
+  // Up to kPoolKeepBytes of freed memory stay in the pool for the next batch.
+  cudaMemPool_t mpool = nullptr;
 };
+constexpr uint64_t kPoolKeepBytes = 8ull << 30;
+// single games with at most this many acting hand-edges (sum over decision
+// edges of the actor's hands) run on one thread-block cluster (Batch::build)
+constexpr int64_t kClusterMaxEdgeHands = 131072;
 std::mutex g_dev_mu;
 std::mutex g_tune_mu;
 
@@ -190,6 +200,14 @@ int device_consts(DeviceConsts** out) {
     if (n != kHandTableSize) return fail(PS_ERR_INVALID, "hand table size mismatch");
     CU(cudaMalloc(&d.table, sizeof(int32_t) * kHandTableSize));
     CU(cudaMemcpy(d.table, t.data(), sizeof(int32_t) * kHandTableSize, cudaMemcpyHostToDevice));
+    cudaMemPoolProps pp = {};
+    pp.allocType = cudaMemAllocationTypePinned;
+    pp.handleTypes = cudaMemHandleTypeNone;
+    pp.location.type = cudaMemLocationTypeDevice;
+    pp.location.id = dev;
+    CU(cudaMemPoolCreate(&d.mpool, &pp));
+    uint64_t keep = kPoolKeepBytes;
+    CU(cudaMemPoolSetAttribute(d.mpool, cudaMemPoolAttrReleaseThreshold, &keep));
     d.nsm = prop.multiProcessorCount;
     d.device = dev;
     d.ctx = ctx;
@@ -309,26 +327,40 @@ struct Batch {
   std::vector<float> h_expl;
   std::vector<int> h_iters;
 
+  // device buffers of the batch: from the device's pool, ordered on the
+  // batch's stream (DeviceConsts::mpool)
+  template <class T>
+  cudaError_t dalloc(T** p, size_t bytes) {
+    return cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), std::max<size_t>(bytes, 1), dc->mpool, stream);
+  }
+  template <class T>
+  void dfree(T*& p) {
+    if (p) cudaFreeAsync(p, stream);
+    p = nullptr;
+  }
+
   ~Batch() {
     if (stream) cudaStreamSynchronize(stream);
-    cudaFree(pool);
     if (h_static) g_pinned.release(h_static, h_static_cap, h_static_tag);
-    cudaFree(d_spots);
-    cudaFree(d_work);
-    cudaFree(d_items);
-    cudaFree(adj_pool);
-    cudaFree(rec_pool);
-    cudaFree(d_scratch);
-    cudaFree(d_disc);
-    cudaFree(d_target);
-    cudaFree(d_expl);
-    cudaFree(d_bar);
-    cudaFree(d_gred);
-    cudaFree(d_iters);
-    cudaFree(d_counter);
-    cudaFree(d_err);
-    cudaFree(d_order);
-    cudaFree(d_inst);
+    if (stream) {  // the buffers go back to the pool behind the batch's last work
+      dfree(pool);
+      dfree(d_spots);
+      dfree(d_work);
+      dfree(d_items);
+      dfree(adj_pool);
+      dfree(rec_pool);
+      dfree(d_scratch);
+      dfree(d_disc);
+      dfree(d_target);
+      dfree(d_expl);
+      dfree(d_bar);
+      dfree(d_gred);
+      dfree(d_iters);
+      dfree(d_counter);
+      dfree(d_err);
+      dfree(d_order);
+      dfree(d_inst);
+    }
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
@@ -397,7 +429,7 @@ struct Batch {
     setup_bytes = su;
     state_bytes = st;
     bnd_bytes = sb;
-    CU(cudaMalloc(&pool, static_bytes + setup_bytes + state_bytes + bnd_bytes));
+    CU(dalloc(&pool, static_bytes + setup_bytes + state_bytes + bnd_bytes));
     CU(cudaMemsetAsync(pool + static_bytes + setup_bytes + state_bytes, 0, bnd_bytes, stream));
     h_static_cap = std::max<size_t>(static_bytes, 16);
     CU(g_pinned.acquire(h_static_cap, &h_static, &h_static_tag));
@@ -521,15 +553,15 @@ struct Batch {
     nwork = (int)work.size();
     for (int i = 0; i < n; ++i)
       for (int k = 0; k < games[i]->num_boundary; ++k) items.push_back(make_int2(i, k));
-    if (!items.empty()) CU(cudaMalloc(&d_items, sizeof(int2) * items.size()));
-    CU(cudaMalloc(&d_spots, sizeof(SpotDev) * n));
-    CU(cudaMalloc(&d_work, sizeof(int2) * std::max(1, nwork)));
-    CU(cudaMalloc(&d_target, sizeof(float) * n));
-    CU(cudaMalloc(&d_expl, sizeof(float) * n));
-    CU(cudaMalloc(&d_iters, sizeof(int) * n));
-    CU(cudaMalloc(&d_counter, sizeof(int)));
-    CU(cudaMalloc(&d_err, sizeof(int)));
-    CU(cudaMalloc(&d_order, sizeof(int) * n));
+    if (!items.empty()) CU(dalloc(&d_items, sizeof(int2) * items.size()));
+    CU(dalloc(&d_spots, sizeof(SpotDev) * n));
+    CU(dalloc(&d_work, sizeof(int2) * std::max(1, nwork)));
+    CU(dalloc(&d_target, sizeof(float) * n));
+    CU(dalloc(&d_expl, sizeof(float) * n));
+    CU(dalloc(&d_iters, sizeof(int) * n));
+    CU(dalloc(&d_counter, sizeof(int)));
+    CU(dalloc(&d_err, sizeof(int)));
+    CU(dalloc(&d_order, sizeof(int) * n));
     // launch configuration: warps per CTA (one op per warp at a time) and
     // whether single-board spots stage their board tables in shared memory
     int hs_max = 4;
@@ -572,7 +604,7 @@ struct Batch {
       }
     }
     scratch_ctas = std::max(grid * inst_k, flow ? flow_grid * flow_lanes : 0);
-    CU(cudaMalloc(&d_scratch, sizeof(float) * scratch_floats * scratch_ctas));
+    CU(dalloc(&d_scratch, sizeof(float) * scratch_floats * scratch_ctas));
     // a single tree of at least PS_GRID_NODES nodes (default 16; 0 = never)
     // is solved by all SMs at once: a lone game is latency-bound, and even a
     // 33-node river tree iterates 1.5x faster on every SM than on one
@@ -584,11 +616,21 @@ struct Batch {
         if (gc >= 2) {
           grid_mode = true;
           grid_blocks = gc;
-          CU(cudaMalloc(&d_bar, 64));
-          CU(cudaMalloc(&d_gred, 64));
-          // PS_GRID_CLUSTER = C (2..16): the game runs on one cluster of C CTAs instead
+          CU(dalloc(&d_bar, 64));
+          CU(dalloc(&d_gred, 64));
+          // A small tree runs on one cluster of 16 CTAs instead, its steps
+          // ended by the hardware cluster barrier: a river game of 33 nodes
+          // iterates 1.24x faster so, and datagen spots of 21-129 nodes solve
+          // 1.21-1.41x faster; from about 150k acting hand-edges per iteration
+          // the wider steps need the whole grid (a 141-node river tree with
+          // 1081 hands ran 3% slower on the cluster, a 357-node one 24%).
+          // PS_GRID_CLUSTER = C overrides: 0 = never, 2..16 = always, on C CTAs.
+          const Game& g0 = *games[0];
+          int64_t S = 0;
+          for (const auto& nd : g0.arena)
+            if (!nd.terminal() && !nd.chance()) S += (int64_t)nd.nch * g0.H[nd.player];
           const char* cl = std::getenv("PS_GRID_CLUSTER");
-          const int want = cl ? std::atoi(cl) : 0;
+          const int want = cl ? std::atoi(cl) : (S <= kClusterMaxEdgeHands ? 16 : 0);
           if (want >= 2) {
             const int cc = grid_cluster_fits(std::min(want, 16), block, plan);
             if (cc >= 2) {
@@ -651,7 +693,7 @@ struct Batch {
       ninst = (int)insts.size();
       inst.clear();
       for (auto& it : insts) inst.insert(inst.end(), it.second.begin(), it.second.end());
-      CU(cudaMalloc(&d_inst, sizeof(int) * std::max<size_t>(1, inst.size())));
+      CU(dalloc(&d_inst, sizeof(int) * std::max<size_t>(1, inst.size())));
     }
     // ---- upload ----
     CU(cudaMemcpyAsync(pool, h_static, static_bytes, cudaMemcpyHostToDevice, stream));
@@ -690,9 +732,8 @@ struct Batch {
       return fail(PS_ERR_INVALID, "dataflow launch shape does not fit: " + std::to_string(b) + " threads, " +
                                       std::to_string(bufs) + " scan buffers, " + std::to_string(lanes) + " spots");
     if (d_scratch && (size_t)g * lanes > (size_t)scratch_ctas) {
-      cudaFree(d_scratch);
-      d_scratch = nullptr;
-      CU(cudaMalloc(&d_scratch, sizeof(float) * scratch_floats * g * lanes));
+      dfree(d_scratch);
+      CU(dalloc(&d_scratch, sizeof(float) * scratch_floats * g * lanes));
       scratch_ctas = g * lanes;
     }
     flow_block = b;
@@ -769,7 +810,10 @@ struct Batch {
     int rc = run_setup();
     if (rc) return rc;
     constexpr int kTrialIters = 6;
-    if ((rc = ensure_disc(kTrialIters + 1))) return rc;
+    // refine runs: 20 iterations, checks before the first and after every
+    // fifth, as the solve loop does (the sweep's 6 iterations carry 3 checks)
+    constexpr int kRefineIters = 20;
+    if ((rc = ensure_disc(kRefineIters + 1))) return rc;
     size_t max_scr = 0;
     for (const auto& c : cands) {
       SmemPlan pl;
@@ -795,9 +839,10 @@ struct Batch {
     CU(cudaMemcpyAsync(d_ids, ids.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, stream));
     CU(cudaMemcpyAsync(d_sweep, sweep_ids.data(), sizeof(int) * ns_sweep, cudaMemcpyHostToDevice, stream));
     CU(cudaMemsetAsync(d_tz, 0, sizeof(float) * ns, stream));
-    const SolveJob job{0, kTrialIters, 1, 0};
+    const SolveJob job{0, kTrialIters, 1, 0}, job_refine{0, kRefineIters, 1, 0};
     // one trial: a warm-up run, then the timed run (device ms)
-    auto trial = [&](const Cand& c, const int* q, int nq, float* out_ms, int* out_bufs) -> cudaError_t {
+    auto trial = [&](const Cand& c, const SolveJob& jb, const int* q, int nq, float* out_ms,
+                     int* out_bufs) -> cudaError_t {
       SmemPlan pl;
       int occ, g;
       *out_ms = 0.f;
@@ -807,7 +852,7 @@ struct Batch {
         e = cudaMemsetAsync(d_cnt, 0, sizeof(int), stream);
         if (e == cudaSuccess) e = cudaEventRecord(ev[2], stream);
         if (e == cudaSuccess)
-          e = launch_flow(d_sample, nq, q, d_cnt, d_disc, job, d_tz, d_tscratch, scratch_floats, d_te, d_ti, d_err,
+          e = launch_flow(d_sample, nq, q, d_cnt, d_disc, jb, d_tz, d_tscratch, scratch_floats, d_te, d_ti, d_err,
                           g, c.b, c.lanes, c.parts, pl, stream);
         if (e == cudaSuccess) e = cudaEventRecord(ev[3], stream);
       }
@@ -822,7 +867,7 @@ struct Batch {
     for (const auto& c : cands) {
       float ms = 0;
       int bufs = 0;
-      CU(trial(c, d_sweep, ns_sweep, &ms, &bufs));
+      CU(trial(c, job, d_sweep, ns_sweep, &ms, &bufs));
       if (ms <= 0.f) continue;
       tune_log.push_back(Trial{c.b, bufs, ms, c.lanes, c.parts});
       swept.push_back({ms, Cand{c.b, bufs, c.lanes, c.parts}});
@@ -832,8 +877,8 @@ struct Batch {
       }
     }
     // refine: the shapes within 6% of the sweep's best (at most 6) run again on
-    // the larger sample, where each lane takes several spots in turn; the
-    // fastest of those runs is kept
+    // the larger sample, where each lane takes several spots in turn, for
+    // kRefineIters iterations; the fastest of those runs is kept
     if (ns > ns_sweep && !swept.empty()) {
       std::stable_sort(swept.begin(), swept.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
       float best_refined = 0;
@@ -841,7 +886,7 @@ struct Batch {
         const Cand& c = swept[i].second;
         float ms = 0;
         int bufs = 0;
-        CU(trial(c, d_ids, ns, &ms, &bufs));
+        CU(trial(c, job_refine, d_ids, ns, &ms, &bufs));
         if (ms <= 0.f) continue;
         tune_log.push_back(Trial{c.b, bufs, ms, c.lanes, c.parts});
         if (best_refined == 0 || ms < best_refined) {
@@ -975,9 +1020,8 @@ struct Batch {
     int occ, g;
     shape_for(b, bufs, cap_ctas, n, pl, occ, g);
     if (g * inst_k > scratch_ctas) {
-      cudaFree(d_scratch);
-      d_scratch = nullptr;
-      CU(cudaMalloc(&d_scratch, sizeof(float) * scratch_floats * g * inst_k));
+      dfree(d_scratch);
+      CU(dalloc(&d_scratch, sizeof(float) * scratch_floats * g * inst_k));
       scratch_ctas = g * inst_k;
     }
     block = b;
@@ -1034,10 +1078,10 @@ struct Batch {
     int cap = std::max<int>(upto, std::max(1024, 2 * disc_cap));
     std::vector<Discount> h(cap);
     for (int t = 0; t < cap; ++t) h[t] = discount_params((uint32_t)t);
-    cudaFree(d_disc);
-    d_disc = nullptr;
-    CU(cudaMalloc(&d_disc, sizeof(Discount) * cap));
-    CU(cudaMemcpy(d_disc, h.data(), sizeof(Discount) * cap, cudaMemcpyHostToDevice));
+    dfree(d_disc);
+    CU(dalloc(&d_disc, sizeof(Discount) * cap));
+    CU(cudaMemcpyAsync(d_disc, h.data(), sizeof(Discount) * cap, cudaMemcpyHostToDevice, stream));
+    CU(cudaStreamSynchronize(stream));  // h is released on return
     disc_cap = cap;
     return PS_OK;
   }
@@ -1120,7 +1164,7 @@ struct Batch {
         x.board_size = (uint8_t)(g.turn == NOT_DEALT ? 3 : g.river == NOT_DEALT ? 4 : 5);
         std::memcpy(x.board, bd, x.board_size);
       }
-      CU(cudaMalloc(&rec_pool, rb + sizeof(RecordMeta) * n));
+      CU(dalloc(&rec_pool, rb + sizeof(RecordMeta) * n));
       CU(cudaMemcpyAsync(rec_pool, r.data(), 4 * r.size(), cudaMemcpyHostToDevice, stream));
       CU(cudaMemcpyAsync(rec_pool + rb, m.data(), sizeof(RecordMeta) * n, cudaMemcpyHostToDevice, stream));
     }
@@ -1147,7 +1191,7 @@ struct Batch {
       off += align256((size_t)games[i]->num_boundary * 2 * games[i]->vstride * 4);
     }
     adj_bytes = std::max<size_t>(off, 256);
-    CU(cudaMalloc(&adj_pool, adj_bytes));
+    CU(dalloc(&adj_pool, adj_bytes));
     for (int i = 0; i < n; ++i) {
       SpotDev& s = h_spots[i];
       float* v = (float*)(adj_pool + o[i]);

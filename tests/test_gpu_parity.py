@@ -461,6 +461,7 @@ def test_grid_mode_matches_single_cta(monkeypatch):
     r, b, t = spots.turn_spot(8, weights=_sparse)
     grid = spots.product_game(r, b, t)            # default: grid mode for single trees >= 16 nodes
     assert grid.num_nodes() >= 2000
+    assert grid.schedule()["mode"] == "grid"      # too wide for one cluster
     monkeypatch.setenv("PS_GRID_NODES", "0")
     one = spots.product_game(r, b, t)
     for it in range(4):
@@ -483,6 +484,9 @@ def test_cluster_mode_matches_grid_mode(monkeypatch, ctas):
     bit - the solve loop with its checks, single steps, finalize, root values
     and the expected values."""
     r, b, t = spots.river_spot(1)
+    monkeypatch.delenv("PS_GRID_CLUSTER", raising=False)
+    dflt = spots.product_game(r, b, t).schedule()  # a 33-node river game: one cluster by default
+    assert dflt["mode"] == "cluster" and dflt["ctas"] == 16
     monkeypatch.setenv("PS_GRID_CLUSTER", "0")
     grid = spots.product_game(r, b, t)
     monkeypatch.setenv("PS_GRID_CLUSTER", ctas)
