@@ -118,6 +118,60 @@ struct PinnedPool {
 };
 PinnedPool g_pinned;
 
+// Streams and their four timing events, kept for reuse by the next batch:
+// creating a stream or an event waits while a kernel of another batch runs
+// (measured: 430 ms, the rest of a 600 ms solve), which would hold up
+// building the next batch of a datagen job.  Reused only in the context that
+// made them; at most kKeepStreams wait in the pool.
+struct StreamPool {
+  struct Entry {
+    cudaStream_t s;
+    cudaEvent_t ev[4];
+    CtxTag tag;
+  };
+  static constexpr size_t kKeepStreams = 8;
+  std::mutex mu;
+  std::vector<Entry> free_;
+  cudaError_t acquire(cudaStream_t* s, cudaEvent_t ev[4]) {
+    CtxTag tag;
+    cudaError_t e = current_tag(&tag);
+    if (e != cudaSuccess) return e;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      // entries of an ended context of this device are gone with it
+      free_.erase(std::remove_if(free_.begin(), free_.end(),
+                                 [&](const Entry& x) { return x.tag.dev == tag.dev && x.tag.ctx != tag.ctx; }),
+                  free_.end());
+      for (size_t i = 0; i < free_.size(); ++i)
+        if (free_[i].tag.dev == tag.dev && free_[i].tag.ctx == tag.ctx) {
+          *s = free_[i].s;
+          for (int k = 0; k < 4; ++k) ev[k] = free_[i].ev[k];
+          free_.erase(free_.begin() + (long)i);
+          return cudaSuccess;
+        }
+    }
+    e = cudaStreamCreateWithFlags(s, cudaStreamNonBlocking);
+    for (int k = 0; k < 4 && e == cudaSuccess; ++k) e = cudaEventCreate(&ev[k]);
+    return e;
+  }
+  // the stream's queued work (a batch's buffer frees) still runs in order
+  void release(cudaStream_t s, cudaEvent_t ev[4]) {
+    CtxTag tag;
+    if (current_tag(&tag) == cudaSuccess) {
+      std::lock_guard<std::mutex> lk(mu);
+      if (free_.size() < kKeepStreams && ev[0] && ev[1] && ev[2] && ev[3]) {
+        Entry x{s, {ev[0], ev[1], ev[2], ev[3]}, tag};
+        free_.push_back(x);
+        return;
+      }
+    }
+    for (int k = 0; k < 4; ++k)
+      if (ev[k]) cudaEventDestroy(ev[k]);
+    if (s) cudaStreamDestroy(s);
+  }
+};
+StreamPool g_streams;
+
 // Device staging for the per-call metadata of the datagen entry points
 // (boards, pots, stacks, an error word): one buffer per device that only
 // grows.  A call holds it, under the lock, until its stream work is done, so
@@ -322,6 +376,12 @@ struct Batch {
     int lanes = 0, parts = 0;  // dataflow trials: spots per CTA and node-op parts (0 = step-synchronous)
   };
   std::vector<Trial> tune_log;  // trials of the last autotune
+  // dataflow shapes the sweep left within 6% of its best, re-timed by the
+  // first fresh solve (refine_flow); empty when the choice is made
+  std::vector<std::array<int, 4>> refine_cands;
+  long refine_key = 0;
+  int refine_cap = 0;
+  std::vector<int> refine_order;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   float last_solve_ms = 0, last_setup_ms = 0;
   std::vector<float> h_expl;
@@ -361,16 +421,13 @@ struct Batch {
       dfree(d_order);
       dfree(d_inst);
     }
-    for (auto& e : ev)
-      if (e) cudaEventDestroy(e);
-    if (stream) cudaStreamDestroy(stream);
+    if (stream) g_streams.release(stream, ev);
   }
 
   int build(const ps_batch_opts* opts) {
     int rc = device_consts(&dc);
     if (rc) return rc;
-    CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    for (auto& e : ev) CU(cudaEventCreate(&e));
+    CU(g_streams.acquire(&stream, ev));
     const int n = (int)games.size();
     // a single game large enough for grid mode (below) evaluates all of a
     // pass's terminals in one step unless its caller chose the program
@@ -810,10 +867,7 @@ struct Batch {
     int rc = run_setup();
     if (rc) return rc;
     constexpr int kTrialIters = 6;
-    // refine runs: 20 iterations, checks before the first and after every
-    // fifth, as the solve loop does (the sweep's 6 iterations carry 3 checks)
-    constexpr int kRefineIters = 20;
-    if ((rc = ensure_disc(kRefineIters + 1))) return rc;
+    if ((rc = ensure_disc(kTrialIters + 1))) return rc;
     size_t max_scr = 0;
     for (const auto& c : cands) {
       SmemPlan pl;
@@ -839,7 +893,7 @@ struct Batch {
     CU(cudaMemcpyAsync(d_ids, ids.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, stream));
     CU(cudaMemcpyAsync(d_sweep, sweep_ids.data(), sizeof(int) * ns_sweep, cudaMemcpyHostToDevice, stream));
     CU(cudaMemsetAsync(d_tz, 0, sizeof(float) * ns, stream));
-    const SolveJob job{0, kTrialIters, 1, 0}, job_refine{0, kRefineIters, 1, 0};
+    const SolveJob job{0, kTrialIters, 1, 0};
     // one trial: a warm-up run, then the timed run (device ms)
     auto trial = [&](const Cand& c, const SolveJob& jb, const int* q, int nq, float* out_ms,
                      int* out_bufs) -> cudaError_t {
@@ -876,29 +930,26 @@ struct Batch {
         best = {c.b, bufs, c.lanes, c.parts};
       }
     }
-    // refine: the shapes within 6% of the sweep's best (at most 6) run again on
-    // the larger sample, where each lane takes several spots in turn, for
-    // kRefineIters iterations; the fastest of those runs is kept
+    // refine: the shapes within 6% of the sweep's best (at most 6) run again at
+    // the batch's first solve, on a larger sample with the solve's own targets
+    // and iteration limit (refine_flow); until then the sweep's best stands
+    refine_cands.clear();
     if (ns > ns_sweep && !swept.empty()) {
       std::stable_sort(swept.begin(), swept.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
-      float best_refined = 0;
       for (size_t i = 0; i < swept.size() && i < 6 && swept[i].first <= 1.06f * best_ms; ++i) {
         const Cand& c = swept[i].second;
-        float ms = 0;
-        int bufs = 0;
-        CU(trial(c, job_refine, d_ids, ns, &ms, &bufs));
-        if (ms <= 0.f) continue;
-        tune_log.push_back(Trial{c.b, bufs, ms, c.lanes, c.parts});
-        if (best_refined == 0 || ms < best_refined) {
-          best_refined = ms;
-          best = c;
-        }
+        refine_cands.push_back({c.b, c.bufs, c.lanes, c.parts});
       }
+      if (refine_cands.size() < 2) refine_cands.clear();
     }
     if ((rc = check_err())) return rc;
-    {
+    if (refine_cands.empty()) {
       std::lock_guard<std::mutex> lk(g_tune_mu);
       g_flow_tune[key] = {best.b, best.bufs, best.lanes, best.parts};
+    } else {
+      refine_key = key;
+      refine_cap = cap_ctas;
+      refine_order = order;
     }
     CU(cudaMemsetAsync(pool + static_bytes + setup_bytes, 0, state_bytes, stream));
     ready = true;  // the trials' state is cleared and the board tables stay built
@@ -906,6 +957,92 @@ struct Batch {
     if (rc) return rc;
     CU(cudaStreamSynchronize(stream));
     return PS_OK;
+  }
+
+  // The autotuner's refine stage, run by the batch's first fresh solve: each
+  // shape the sweep left within 6% of its best solves a sample of the batch
+  // (four waves of spots, evenly along the cost order) from zero state with
+  // the solve's own targets and iteration limit, as the whole batch will, so
+  // the spots' spread of iteration counts and the lanes' rebinding count in
+  // the timing.  The fastest is adopted and cached; the trials are logged
+  // after the sweep's.  The state is zeroed again afterwards.
+  int refine_flow(uint32_t max_iter, const float* target) {
+    const int n = (int)games.size();
+    int ns = 1;
+    for (const auto& c : refine_cands) {
+      SmemPlan pl;
+      int occ, g;
+      if (flow_shape(c[0], c[1], c[2], refine_cap, n, pl, occ, g)) ns = std::max(ns, g * c[2]);
+    }
+    size_t max_scr = (size_t)ns;
+    ns = std::min(n, 4 * ns);
+    std::vector<SpotDev> sample(ns);
+    std::vector<int> ids(ns);
+    std::vector<float> tg(ns);
+    for (int i = 0; i < ns; ++i) {
+      const int k = refine_order[(size_t)i * n / ns];
+      sample[i] = h_spots[k];
+      ids[i] = i;
+      tg[i] = target[k];
+    }
+    char* tmp = nullptr;
+    const size_t tb = align256(sizeof(SpotDev) * ns) + align256(16 * (size_t)ns) + 256;
+    CU(cudaMalloc(&tmp, tb));
+    std::unique_ptr<char, decltype(&cudaFree)> k1(tmp, &cudaFree);
+    SpotDev* d_sample = (SpotDev*)tmp;
+    int* d_ids = (int*)(tmp + align256(sizeof(SpotDev) * ns));
+    float* d_tg = (float*)(d_ids + ns);
+    float* d_te = d_tg + ns;
+    int* d_ti = (int*)(d_te + ns);
+    int* d_cnt = (int*)(tmp + tb - 256);
+    float* d_tscratch = nullptr;
+    CU(cudaMalloc(&d_tscratch, sizeof(float) * scratch_floats * max_scr));
+    std::unique_ptr<float, decltype(&cudaFree)> k2(d_tscratch, &cudaFree);
+    CU(cudaMemcpyAsync(d_sample, sample.data(), sizeof(SpotDev) * ns, cudaMemcpyHostToDevice, stream));
+    CU(cudaMemcpyAsync(d_ids, ids.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, stream));
+    CU(cudaMemcpyAsync(d_tg, tg.data(), sizeof(float) * ns, cudaMemcpyHostToDevice, stream));
+    const SolveJob job{0, (int)max_iter, 1, 0};
+    std::array<int, 4> best = refine_cands[0];
+    float best_ms = 0;
+    for (const auto& c : refine_cands) {
+      SmemPlan pl;
+      int occ, g;
+      if (!flow_shape(c[0], c[1], c[2], refine_cap, ns, pl, occ, g)) continue;
+      CU(cudaMemsetAsync(pool + static_bytes + setup_bytes, 0, state_bytes, stream));
+      CU(cudaMemsetAsync(d_cnt, 0, sizeof(int), stream));
+      CU(cudaEventRecord(ev[2], stream));
+      CU(launch_flow(d_sample, ns, d_ids, d_cnt, d_disc, job, d_tg, d_tscratch, scratch_floats, d_te, d_ti, d_err, g,
+                     c[0], c[2], c[3], pl, stream));
+      CU(cudaEventRecord(ev[3], stream));
+      CU(cudaStreamSynchronize(stream));
+      float ms = 0;
+      CU(cudaEventElapsedTime(&ms, ev[2], ev[3]));
+      tune_log.push_back(Trial{c[0], pl.bufs, ms, c[2], c[3]});
+      if (best_ms == 0 || ms < best_ms) {
+        best_ms = ms;
+        best = {c[0], pl.bufs, c[2], c[3]};
+      }
+    }
+    int rc = check_err();
+    if (rc) return rc;
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      g_flow_tune[refine_key] = best;
+    }
+    refine_cands.clear();
+    refine_order.clear();
+    CU(cudaMemsetAsync(pool + static_bytes + setup_bytes, 0, state_bytes, stream));
+    return adopt_flow(best[0], best[1], best[2], best[3], refine_cap);
+  }
+
+  // A first call other than a fresh solve keeps the sweep's choice: it is
+  // cached as it stands, so the next batch of the class does not sweep again.
+  void settle_tune() {
+    if (refine_cands.empty()) return;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_flow_tune[refine_key] = {flow_block, flow_plan.bufs, flow_lanes, flow_parts};
+    refine_cands.clear();
+    refine_order.clear();
   }
 
   // The batch's solve-type job (iterations, checks, epilogue) on every spot,
@@ -1109,6 +1246,8 @@ struct Batch {
       last_setup_ms = 0;
       return check_err();
     }
+    if (fresh && flow && !refine_cands.empty() && (rc = refine_flow(max_iter, target))) return rc;
+    settle_tune();
     CU(cudaMemcpyAsync(d_target, target, sizeof(float) * n, cudaMemcpyHostToDevice, stream));
     CU(cudaMemsetAsync(d_counter, 0, sizeof(int), stream));
     CU(cudaEventRecord(ev[1], stream));
@@ -1244,6 +1383,7 @@ struct Batch {
   // with iterations = t1).  The first call after construction or a reset
   // zeroes the state and builds the board tables.
   int run_iterations(uint32_t t0, uint32_t t1, int epilogue) {
+    settle_tune();
     const int n = (int)games.size();
     int rc = ensure_disc(t1 + 1);
     if (rc) return rc;
