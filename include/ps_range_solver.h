@@ -308,10 +308,11 @@ int ps_game_schedule(ps_game* g, int32_t out[8]);
 /* the trials of the last autotune: per trial 4 values (threads per CTA,
  * scan-buffer warps, spots per CTA, node-op parts; the last two 0 for a
  * step-synchronous trial) and its device ms; returns the count.  A dataflow
- * autotune lists its sweep (every shape, one wave of sample spots) and then
- * the refine runs of the shapes within 6% of the sweep's best on four times
- * the spots; a shape's second entry is its refine run, and the fastest refine
- * run is the choice. */
+ * autotune lists its sweep (every shape, 6 iterations on one wave of sample
+ * spots) and, once the batch's first fresh ps_batch_solve has run, the refine
+ * runs of the shapes within 6% of the sweep's best (that solve's targets and
+ * iteration limit on four waves of spots); a shape's second entry is its
+ * refine run, and the fastest refine run is the choice. */
 int ps_batch_autotune_trials(ps_batch* b, int32_t* shape, float* trial_ms, int cap);
 /* bytes copied host->device by ps_batch_new and device->host by ps_batch_results */
 int ps_batch_io_bytes(ps_batch* b, uint64_t* h2d, uint64_t* d2h);

@@ -625,10 +625,10 @@ class BatchSolver:
         scan-buffer warps, spots per CTA and node-op parts (0 for a
         step-synchronous trial), the trial's device ms and its stage: "sweep"
         for the trials of every shape on one wave of spots, "refine" for the
-        re-runs of the leading shapes on a larger sample (the library lists
-        them after the sweep, so a shape's second entry is its refine run);
-        the choice is the fastest refine run, or the fastest sweep trial
-        when there was none."""
+        re-runs of the leading shapes that the first fresh solve makes on a
+        larger sample with its own targets (the library lists them after the
+        sweep, so a shape's second entry is its refine run); the choice is the
+        fastest refine run, or the fastest sweep trial when there was none."""
         cap = 256
         shape = (C.c_int32 * (4 * cap))()
         t = (C.c_float * cap)()
