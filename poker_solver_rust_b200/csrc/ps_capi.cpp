@@ -59,6 +59,7 @@ struct DeviceConsts {
   cudaMemPool_t mpool = nullptr;
 };
 constexpr uint64_t kPoolKeepBytes = 8ull << 30;
+constexpr int kMaxInstances = 4;  // spots per CTA in lockstep (ps_batch_opts.instances_per_cta) at most
 // single games with at most this many acting hand-edges (sum over decision
 // edges of the actor's hands) run on one thread-block cluster (Batch::build)
 constexpr int64_t kClusterMaxEdgeHands = 131072;
@@ -171,6 +172,7 @@ struct StreamPool {
   }
 };
 StreamPool g_streams;
+
 
 // Device staging for the per-call metadata of the datagen entry points
 // (boards, pots, stacks, an error word): one buffer per device that only
@@ -487,8 +489,24 @@ struct Batch {
     state_bytes = st;
     bnd_bytes = sb;
     CU(dalloc(&pool, static_bytes + setup_bytes + state_bytes + bnd_bytes));
-    CU(cudaMemsetAsync(pool + static_bytes + setup_bytes + state_bytes, 0, bnd_bytes, stream));
-    h_static_cap = std::max<size_t>(static_bytes, 16);
+    // boundary values and reach start at zero.  Only batches with depth
+    // boundaries clear them: the clear is a kernel, which cannot start while
+    // another batch's solve holds every SM (measured: it held a datagen job's
+    // next batch back by 430 ms of a 600 ms solve)
+    bool any_boundary = false;
+    for (const auto& gp : games) any_boundary = any_boundary || gp->num_boundary > 0;
+    if (any_boundary) CU(cudaMemsetAsync(pool + static_bytes + setup_bytes + state_bytes, 0, bnd_bytes, stream));
+    // the pinned staging buffer carries the static region and, after it, the
+    // spot descriptors and the work, order, instance and boundary-item lists:
+    // every upload then comes from pinned memory and is one asynchronous copy
+    size_t nb_all = 0, bnd_all = 0;
+    for (const auto& gp : games) {
+      nb_all += gp->boards.size();
+      bnd_all += (size_t)gp->num_boundary;
+    }
+    const size_t extra = align256(sizeof(SpotDev) * n) + align256(sizeof(int2) * nb_all) + align256(sizeof(int) * n) +
+                         align256(sizeof(int) * (size_t)n * kMaxInstances) + align256(sizeof(int2) * bnd_all);
+    h_static_cap = align256(std::max<size_t>(static_bytes, 16)) + extra;
     CU(g_pinned.acquire(h_static_cap, &h_static, &h_static_tag));
     // ---- fill static ----
     h_spots.resize(n);
@@ -628,7 +646,7 @@ struct Batch {
       single_board &= gp->boards.size() == 1;
     }
     const bool tune = opts && opts->block_threads < 0;
-    inst_k = opts && opts->instances_per_cta > 0 ? std::min(opts->instances_per_cta, 4) : 1;
+    inst_k = opts && opts->instances_per_cta > 0 ? std::min(opts->instances_per_cta, kMaxInstances) : 1;
     req_bufs = opts ? opts->scan_buffers : 0;
     block = opts && opts->block_threads > 0 ? opts->block_threads : 256;
     block = std::max(64, std::min(256, (block / 32) * 32));
@@ -752,14 +770,22 @@ struct Batch {
       for (auto& it : insts) inst.insert(inst.end(), it.second.begin(), it.second.end());
       CU(dalloc(&d_inst, sizeof(int) * std::max<size_t>(1, inst.size())));
     }
-    // ---- upload ----
+    // ---- upload (every source in the pinned staging buffer) ----
+    if (inst.size() > (size_t)n * kMaxInstances) return fail(PS_ERR_INVALID, "instance list too long");
+    char* hx = h_static + align256(std::max<size_t>(static_bytes, 16));
+    auto put = [&](void* dst, const void* src, size_t bytes) -> cudaError_t {
+      if (bytes == 0) return cudaSuccess;
+      std::memcpy(hx, src, bytes);
+      cudaError_t e = cudaMemcpyAsync(dst, hx, bytes, cudaMemcpyHostToDevice, stream);
+      hx += align256(bytes);
+      return e;
+    };
     CU(cudaMemcpyAsync(pool, h_static, static_bytes, cudaMemcpyHostToDevice, stream));
-    CU(cudaMemcpyAsync(d_spots, h_spots.data(), sizeof(SpotDev) * n, cudaMemcpyHostToDevice, stream));
-    CU(cudaMemcpyAsync(d_work, work.data(), sizeof(int2) * nwork, cudaMemcpyHostToDevice, stream));
-    CU(cudaMemcpyAsync(d_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
-    CU(cudaMemcpyAsync(d_inst, inst.data(), sizeof(int) * inst.size(), cudaMemcpyHostToDevice, stream));
-    if (!items.empty())
-      CU(cudaMemcpyAsync(d_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, stream));
+    CU(put(d_spots, h_spots.data(), sizeof(SpotDev) * n));
+    CU(put(d_work, work.data(), sizeof(int2) * nwork));
+    CU(put(d_order, order.data(), sizeof(int) * n));
+    CU(put(d_inst, inst.data(), sizeof(int) * inst.size()));
+    CU(put(d_items, items.data(), sizeof(int2) * items.size()));
     CU(cudaStreamSynchronize(stream));
     g_pinned.release(h_static, h_static_cap, h_static_tag);  // uploaded: the staging buffer goes back to the pool
     h_static = nullptr;

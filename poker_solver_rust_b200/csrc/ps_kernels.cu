@@ -24,6 +24,7 @@
 #include <stdint.h>
 
 #include <mutex>
+#include <vector>
 
 #include "ps_device.hpp"
 #include "ps_handeval.hpp"
@@ -2079,8 +2080,48 @@ __global__ void k_setup(const SpotDev* __restrict__ spots, const int2* __restric
 // ---------------------------------------------------------------------------
 // Host-side launch wrappers
 // ---------------------------------------------------------------------------
+// The dynamic shared memory a kernel may use is set only when it differs from
+// the value set last (per device and context).  Setting it while the kernel
+// runs for another batch waits for that launch to end (measured: 440 ms of a
+// 600 ms solve, when a datagen job builds its next batch), and back-to-back
+// batches of one shape ask for the same value.  It is set exactly, not only
+// raised: a larger limit than the launch needs cost the one-game-at-a-time
+// path 14% (45.8 -> 39.4 spots/s), as games of different sizes then ran with
+// less L1.  The calling thread's last error is cleared on every return, so
+// the launch after it reports its own error; a failure is still returned.
+struct SmemLimit {
+  const void* fn;
+  int dev;
+  unsigned long long ctx;
+  size_t bytes;
+};
+static std::mutex g_smem_mu;
+static std::vector<SmemLimit> g_smem_limits;
+
 static cudaError_t set_smem(const void* fn, size_t bytes) {
-  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  int dev = 0;
+  unsigned long long ctx = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = current_context_id(&ctx);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return e;
+  }
+  std::lock_guard<std::mutex> lk(g_smem_mu);
+  SmemLimit* l = nullptr;
+  for (auto& x : g_smem_limits)
+    if (x.fn == fn && x.dev == dev && x.ctx == ctx) l = &x;
+  if (!l || l->bytes != bytes) {
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) {
+      if (l)
+        l->bytes = bytes;
+      else
+        g_smem_limits.push_back(SmemLimit{fn, dev, ctx, bytes});
+    }
+  }
+  cudaGetLastError();
+  return e;
 }
 
 size_t setup_smem_bytes() { return sizeof(SetupSmem); }
