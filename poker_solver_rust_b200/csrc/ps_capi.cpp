@@ -133,8 +133,8 @@ struct StreamPool {
   static constexpr size_t kKeepStreams = 8;
   std::mutex mu;
   std::vector<Entry> free_;
-  cudaError_t acquire(cudaStream_t* s, cudaEvent_t ev[4]) {
-    CtxTag tag;
+  cudaError_t acquire(cudaStream_t* s, cudaEvent_t ev[4], CtxTag* made_in) {
+    CtxTag& tag = *made_in;
     cudaError_t e = current_tag(&tag);
     if (e != cudaSuccess) return e;
     {
@@ -155,10 +155,15 @@ struct StreamPool {
     for (int k = 0; k < 4 && e == cudaSuccess; ++k) e = cudaEventCreate(&ev[k]);
     return e;
   }
-  // the stream's queued work (a batch's buffer frees) still runs in order
-  void release(cudaStream_t s, cudaEvent_t ev[4]) {
+  // the stream's queued work (a batch's buffer frees) still runs in order.
+  // made_in: the context acquire() found; a stream of a context that has
+  // ended since (a device reset) is gone with it and is neither kept nor
+  // destroyed
+  void release(cudaStream_t s, cudaEvent_t ev[4], const CtxTag& made_in) {
     CtxTag tag;
-    if (current_tag(&tag) == cudaSuccess) {
+    if (current_tag(&tag) != cudaSuccess) return;
+    if (tag.dev != made_in.dev || tag.ctx != made_in.ctx) return;
+    {
       std::lock_guard<std::mutex> lk(mu);
       if (free_.size() < kKeepStreams && ev[0] && ev[1] && ev[2] && ev[3]) {
         Entry x{s, {ev[0], ev[1], ev[2], ev[3]}, tag};
@@ -385,6 +390,7 @@ struct Batch {
   int refine_cap = 0;
   std::vector<int> refine_order;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  CtxTag stream_tag;  // the context the stream and events were made in
   float last_solve_ms = 0, last_setup_ms = 0;
   std::vector<float> h_expl;
   std::vector<int> h_iters;
@@ -423,13 +429,13 @@ struct Batch {
       dfree(d_order);
       dfree(d_inst);
     }
-    if (stream) g_streams.release(stream, ev);
+    if (stream) g_streams.release(stream, ev, stream_tag);
   }
 
   int build(const ps_batch_opts* opts) {
     int rc = device_consts(&dc);
     if (rc) return rc;
-    CU(g_streams.acquire(&stream, ev));
+    CU(g_streams.acquire(&stream, ev, &stream_tag));
     const int n = (int)games.size();
     // a single game large enough for grid mode (below) evaluates all of a
     // pass's terminals in one step unless its caller chose the program
