@@ -25,7 +25,7 @@ extern "C" {
 #define PS_ERR_INVALID (-1)     /* invalid configuration or argument */
 #define PS_ERR_STATE (-2)       /* call not allowed in the game's state */
 #define PS_ERR_CUDA (-3)        /* CUDA runtime error or no usable GPU */
-#define PS_ERR_UNSUPPORTED (-4) /* feature outside this build */
+#define PS_ERR_UNSUPPORTED (-4) /* feature the library does not support */
 #define PS_ERR_DEVICE (-5)      /* a kernel reported an error flag */
 
 /* action_tree.rs:130-192 TreeConfig; bet sizes are the reference's strings

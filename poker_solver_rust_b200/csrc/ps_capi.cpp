@@ -254,7 +254,7 @@ int device_consts(DeviceConsts** out) {
   if (!d.table) {
     cudaDeviceProp prop;
     CU(cudaGetDeviceProperties(&prop, dev));
-    if (prop.major != 10) return fail(PS_ERR_CUDA, "this build targets sm_100a (B200); found sm_" +
+    if (prop.major != 10) return fail(PS_ERR_CUDA, "the library is compiled for sm_100a (B200); found sm_" +
                                                        std::to_string(prop.major) + std::to_string(prop.minor));
     std::vector<int32_t> t(kHandTableSize + 64);
     int n = build_hand_table(t.data(), (int)t.size());
