@@ -535,6 +535,21 @@ def _is_cuda_tensor(x) -> bool:
     return type(x).__module__.startswith("torch") and getattr(x, "is_cuda", False)
 
 
+def autotune_stages(shapes, trial_ms):
+    """Trial records of an autotune log (ps_batch_autotune_trials): shapes are
+    (threads per CTA, scan-buffer warps, spots per CTA, node-op parts).  The
+    log lists the sweep (every shape once) and then the refine runs, so the
+    first shape that repeats starts the refine stage."""
+    out, seen, stage = [], set(), "sweep"
+    for k, ms in zip(shapes, trial_ms):
+        if k in seen:
+            stage = "refine"
+        seen.add(k)
+        out.append({"block_threads": k[0], "scan_buffers": k[1], "spots_per_cta": k[2], "node_parts": k[3],
+                    "trial_ms": ms, "stage": stage})
+    return out
+
+
 class BatchSolver:
     """Thousands of independent subgames solved by one persistent launch
     (replaces the per-spot GpuBatchSolver launches of the reference's GPU
@@ -633,15 +648,8 @@ class BatchSolver:
         shape = (C.c_int32 * (4 * cap))()
         t = (C.c_float * cap)()
         n = min(N.check(N.lib().ps_batch_autotune_trials(self._h, shape, t, cap)), cap)
-        out, seen, stage = [], set(), "sweep"
-        for i in range(n):
-            k = tuple(int(shape[4 * i + j]) for j in range(4))
-            if k in seen:
-                stage = "refine"
-            seen.add(k)
-            out.append({"block_threads": k[0], "scan_buffers": k[1], "spots_per_cta": k[2], "node_parts": k[3],
-                        "trial_ms": float(t[i]), "stage": stage})
-        return out
+        return autotune_stages([tuple(int(shape[4 * i + j]) for j in range(4)) for i in range(n)],
+                               [float(t[i]) for i in range(n)])
 
     def config(self):
         """The launch shape of the batch's solves (ps_batch_schedule)."""

@@ -205,3 +205,18 @@ def test_program_forms_pass_slot_replay():
         assert tf["terminal_runs"] == base["terminal_runs"]
         g.set_terminals_first(False)
         assert g.program_info() == base
+
+
+def test_autotune_log_stages():
+    """The autotune log lists the sweep (each shape once), then the refine
+    runs of the leading shapes: the first repeated shape starts the refine
+    stage, and the choice is the fastest refine run."""
+    from poker_solver_rust_b200.game import autotune_stages
+
+    shapes = [(256, 4, 1, 1), (512, 8, 2, 3), (1024, 16, 3, 3), (512, 8, 2, 3), (1024, 16, 3, 3)]
+    ms = [30.0, 20.2, 21.0, 510.0, 505.0]
+    log = autotune_stages(shapes, ms)
+    assert [r["stage"] for r in log] == ["sweep"] * 3 + ["refine"] * 2
+    best = min((r for r in log if r["stage"] == "refine"), key=lambda r: r["trial_ms"])
+    assert (best["block_threads"], best["spots_per_cta"], best["node_parts"]) == (1024, 3, 3)
+    assert [r["stage"] for r in autotune_stages(shapes[:3], ms[:3])] == ["sweep"] * 3
